@@ -1,0 +1,274 @@
+/*
+ * nemo_b200.h -- C ABI of the B200 (sm_100a) NeMo simulation backend.
+ *
+ * Part 1 is a drop-in for the reference C API (src/nemo.h).  Every function
+ * keeps the reference's name, signature, argument meaning, status codes
+ * (src/nemo/types.h:31-61) and error reporting (status return plus the
+ * process-global message of nemo_strerror, src/nemo/nemo_c.cpp:21-65).
+ * The comment above each declaration cites the reference declaration it
+ * replaces.  Handles are opaque pointers; there are no C++ or torch types.
+ *
+ * Part 2 replaces the backend plugin ABI that libnemo dlopens for the CUDA
+ * backend (src/nemo/cuda/devices.hpp:21-52,
+ * src/nemo/cuda/create_simulation.hpp:16-20).  The two functions whose
+ * reference signatures carry only C types are exported under their reference
+ * names.  The two that take reference C++ objects
+ * (cuda_simulation(const network::Generator*, const ConfigurationImpl*) and
+ * cuda_set_configuration(ConfigurationImpl*, int)) are bound through the
+ * adapter shown in INTEGRATION.md, which forwards to Part 1.
+ *
+ * Part 3 is extensions with no counterpart in the reference: bulk
+ * construction, device-resident multi-step runs and bulk read-back.
+ */
+#ifndef NEMO_B200_H
+#define NEMO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define NEMO_B200_API __attribute__((visibility("default")))
+#else
+#define NEMO_B200_API
+#endif
+
+/* src/nemo/types.h:31-61 */
+#define NEMO_OK 0
+#define NEMO_CUDA_INVOCATION_ERROR 1
+#define NEMO_CUDA_ASSERTION_FAILURE 2
+#define NEMO_CUDA_MEMORY_ERROR 3
+#define NEMO_CUDA_ERROR 4
+#define NEMO_API_UNSUPPORTED 5
+#define NEMO_INVALID_INPUT 6
+#define NEMO_BUFFER_OVERFLOW 7
+#define NEMO_BUFFER_UNDERFLOW 8
+#define NEMO_LOGIC_ERROR 9
+#define NEMO_ALLOCATION_ERROR 10
+#define NEMO_MPI_ERROR 11
+#define NEMO_DL_ERROR 12
+#define NEMO_IO_ERROR 13
+#define NEMO_UNKNOWN_ERROR 14
+
+/* src/nemo/types.h:63-66 */
+enum { NEMO_BACKEND_CUDA = 0, NEMO_BACKEND_CPU = 1 };
+typedef unsigned backend_t;
+typedef uint64_t synapse_id;
+
+/* src/nemo.h:42-52 */
+struct nemo_network_class;
+struct nemo_simulation_class;
+struct nemo_configuration_class;
+typedef struct nemo_network_class* nemo_network_t;
+typedef struct nemo_simulation_class* nemo_simulation_t;
+typedef struct nemo_configuration_class* nemo_configuration_t;
+typedef int nemo_status_t;
+
+/* ===================================================================== */
+/* Part 1: the reference C API (src/nemo.h)                              */
+/* ===================================================================== */
+
+/* src/nemo.h:56-57 */
+NEMO_B200_API const char* nemo_version(void);
+/* src/nemo.h:72-74.  The four in-scope neuron types are linked in; a
+ * directory that exists is accepted and recorded. */
+NEMO_B200_API nemo_status_t nemo_add_plugin_path(const char* dir);
+/* src/nemo.h:88-90 */
+NEMO_B200_API nemo_status_t nemo_cuda_device_count(unsigned* count);
+/* src/nemo.h:93-95 */
+NEMO_B200_API nemo_status_t nemo_cuda_device_description(unsigned device, const char** descr);
+
+/* --- configuration, src/nemo.h:104-191 --- */
+/* src/nemo.h:105-106 */
+NEMO_B200_API nemo_configuration_t nemo_new_configuration(void);
+/* src/nemo.h:109-110 */
+NEMO_B200_API void nemo_delete_configuration(nemo_configuration_t);
+/* src/nemo.h:114-115 */
+NEMO_B200_API nemo_status_t nemo_log_stdout(nemo_configuration_t);
+/* src/nemo.h:148-157 */
+NEMO_B200_API nemo_status_t nemo_set_stdp_function(nemo_configuration_t,
+		float prefire_fn[], size_t prefire_len,
+		float postfire_fn[], size_t postfire_len,
+		float min_excitatory_weight, float max_excitatory_weight,
+		float min_inhibitory_weight, float max_inhibitory_weight);
+/* src/nemo.h:160-162.  Recorded; creating a simulation with it fails with
+ * NEMO_API_UNSUPPORTED because this library has no CPU backend. */
+NEMO_B200_API nemo_status_t nemo_set_cpu_backend(nemo_configuration_t);
+/* src/nemo.h:166-168 */
+NEMO_B200_API nemo_status_t nemo_set_cuda_backend(nemo_configuration_t conf, int dev);
+/* src/nemo.h:171-173 */
+NEMO_B200_API nemo_status_t nemo_cuda_device(nemo_configuration_t conf, int* dev);
+/* src/nemo.h:177-179 */
+NEMO_B200_API nemo_status_t nemo_backend(nemo_configuration_t conf, backend_t* backend);
+/* src/nemo.h:183-185 */
+NEMO_B200_API nemo_status_t nemo_backend_description(nemo_configuration_t conf, const char** descr);
+/* src/nemo.h:189-191 */
+NEMO_B200_API nemo_status_t nemo_set_write_only_synapses(nemo_configuration_t conf);
+
+/* --- construction, src/nemo.h:199-292 --- */
+/* src/nemo.h:215-216 */
+NEMO_B200_API nemo_network_t nemo_new_network(void);
+/* src/nemo.h:220-221 */
+NEMO_B200_API void nemo_delete_network(nemo_network_t);
+/* src/nemo.h:235-239 */
+NEMO_B200_API nemo_status_t nemo_add_neuron_type(nemo_network_t, const char* name, unsigned* neuron_type);
+/* src/nemo.h:245-250 */
+NEMO_B200_API nemo_status_t nemo_add_neuron_iz(nemo_network_t, unsigned idx,
+		float a, float b, float c, float d, float u, float v, float sigma);
+/* src/nemo.h:265-268 */
+NEMO_B200_API nemo_status_t nemo_add_neuron(nemo_network_t, unsigned type, unsigned idx,
+		unsigned nargs, float args[]);
+/* src/nemo.h:278-286 */
+NEMO_B200_API nemo_status_t nemo_add_synapse(nemo_network_t, unsigned source, unsigned target,
+		unsigned delay, float weight, unsigned char is_plastic, synapse_id* id);
+/* src/nemo.h:290-292 */
+NEMO_B200_API nemo_status_t nemo_neuron_count(nemo_network_t net, unsigned* ncount);
+
+/* --- simulation, src/nemo.h:307-762 --- */
+/* src/nemo.h:311-312 */
+NEMO_B200_API nemo_simulation_t nemo_new_simulation(nemo_network_t, nemo_configuration_t);
+/* src/nemo.h:316-317 */
+NEMO_B200_API void nemo_delete_simulation(nemo_simulation_t);
+/* src/nemo.h:347-352.  *fired points into a buffer owned by the simulation,
+ * valid until the next step (src/nemo/nemo_c.cpp:454-460). */
+NEMO_B200_API nemo_status_t nemo_step(nemo_simulation_t,
+		unsigned fstim_nidx[], size_t fstim_count,
+		unsigned istim_nidx[], float istim_current[], size_t istim_count,
+		unsigned* fired[], size_t* fired_count);
+/* src/nemo.h:356-358 */
+NEMO_B200_API nemo_status_t nemo_apply_stdp(nemo_simulation_t, float reward);
+/* src/nemo.h:380-382 */
+NEMO_B200_API nemo_status_t nemo_get_membrane_potential(nemo_simulation_t sim, unsigned neuron, float* v);
+/* src/nemo.h:399-401 */
+NEMO_B200_API nemo_status_t nemo_get_neuron_state_n(nemo_network_t net, unsigned neuron, unsigned var, float* val);
+/* src/nemo.h:418-420 */
+NEMO_B200_API nemo_status_t nemo_get_neuron_parameter_n(nemo_network_t net, unsigned neuron, unsigned param, float* val);
+/* src/nemo.h:437-439 */
+NEMO_B200_API nemo_status_t nemo_get_neuron_state_s(nemo_simulation_t sim, unsigned neuron, unsigned var, float* val);
+/* src/nemo.h:456-458 */
+NEMO_B200_API nemo_status_t nemo_get_neuron_parameter_s(nemo_simulation_t sim, unsigned neuron, unsigned param, float* val);
+/* src/nemo.h:467-469 */
+NEMO_B200_API nemo_status_t nemo_get_synapse_source_n(nemo_network_t, synapse_id synapse, unsigned* source);
+/* src/nemo.h:478-480 */
+NEMO_B200_API nemo_status_t nemo_get_synapse_source_s(nemo_simulation_t, synapse_id synapse, unsigned* source);
+/* src/nemo.h:489-491 */
+NEMO_B200_API nemo_status_t nemo_get_synapse_target_n(nemo_network_t, synapse_id synapse, unsigned* target);
+/* src/nemo.h:499-501 */
+NEMO_B200_API nemo_status_t nemo_get_synapse_target_s(nemo_simulation_t, synapse_id synapse, unsigned* target);
+/* src/nemo.h:509-511 */
+NEMO_B200_API nemo_status_t nemo_get_synapse_delay_n(nemo_network_t, synapse_id synapse, unsigned* delay);
+/* src/nemo.h:519-521 */
+NEMO_B200_API nemo_status_t nemo_get_synapse_delay_s(nemo_simulation_t, synapse_id synapse, unsigned* delay);
+/* src/nemo.h:529-531 */
+NEMO_B200_API nemo_status_t nemo_get_synapse_weight_n(nemo_network_t, synapse_id synapse, float* weight);
+/* src/nemo.h:539-541 */
+NEMO_B200_API nemo_status_t nemo_get_synapse_weight_s(nemo_simulation_t, synapse_id synapse, float* weight);
+/* src/nemo.h:549-551 */
+NEMO_B200_API nemo_status_t nemo_get_synapse_plastic_n(nemo_network_t, synapse_id synapse, unsigned char* plastic);
+/* src/nemo.h:559-561 */
+NEMO_B200_API nemo_status_t nemo_get_synapse_plastic_s(nemo_simulation_t, synapse_id synapse, unsigned char* plastic);
+/* src/nemo.h:565-567.  *synapses points into a buffer owned by the network,
+ * valid until the next query. */
+NEMO_B200_API nemo_status_t nemo_get_synapses_from_n(nemo_network_t, unsigned source, synapse_id* synapses[], size_t* len);
+/* src/nemo.h:579-581 */
+NEMO_B200_API nemo_status_t nemo_get_synapses_from_s(nemo_simulation_t, unsigned source, synapse_id* synapses[], size_t* len);
+/* src/nemo.h:613-615 */
+NEMO_B200_API nemo_status_t nemo_set_neuron_n(nemo_network_t, unsigned idx, unsigned nargs, float args[]);
+/* src/nemo.h:627-629 */
+NEMO_B200_API nemo_status_t nemo_set_neuron_s(nemo_simulation_t, unsigned idx, unsigned nargs, float args[]);
+/* src/nemo.h:639-645 */
+NEMO_B200_API nemo_status_t nemo_set_neuron_iz_n(nemo_network_t net, unsigned idx,
+		float a, float b, float c, float d, float u, float v, float sigma);
+/* src/nemo.h:654-660 */
+NEMO_B200_API nemo_status_t nemo_set_neuron_iz_s(nemo_simulation_t sim, unsigned idx,
+		float a, float b, float c, float d, float u, float v, float sigma);
+/* src/nemo.h:675-677 */
+NEMO_B200_API nemo_status_t nemo_set_neuron_state_n(nemo_network_t net, unsigned neuron, unsigned var, float val);
+/* src/nemo.h:693-695 */
+NEMO_B200_API nemo_status_t nemo_set_neuron_parameter_n(nemo_network_t net, unsigned neuron, unsigned param, float val);
+/* src/nemo.h:711-713 */
+NEMO_B200_API nemo_status_t nemo_set_neuron_state_s(nemo_simulation_t sim, unsigned neuron, unsigned var, float val);
+/* src/nemo.h:729-731 */
+NEMO_B200_API nemo_status_t nemo_set_neuron_parameter_s(nemo_simulation_t sim, unsigned neuron, unsigned param, float val);
+/* src/nemo.h:753-754 */
+NEMO_B200_API nemo_status_t nemo_elapsed_wallclock(nemo_simulation_t, unsigned long*);
+/* src/nemo.h:757-758 */
+NEMO_B200_API nemo_status_t nemo_elapsed_simulation(nemo_simulation_t, unsigned long*);
+/* src/nemo.h:761-762 */
+NEMO_B200_API nemo_status_t nemo_reset_timer(nemo_simulation_t);
+/* src/nemo.h:786-787 */
+NEMO_B200_API const char* nemo_strerror(void);
+
+/* ===================================================================== */
+/* Part 2: backend plugin ABI                                             */
+/* ===================================================================== */
+
+/* src/nemo/cuda/devices.hpp:21-52 (exported at src/nemo/cuda/devices.cpp:282-300) */
+NEMO_B200_API unsigned cuda_device_count(void);
+NEMO_B200_API const char* cuda_device_description(unsigned device);
+
+/* ===================================================================== */
+/* Part 3: extensions (no counterpart in the reference)                   */
+/* ===================================================================== */
+
+/* Bulk form of nemo_add_neuron: n neurons of one type, args row-major
+ * (n x nargs). */
+NEMO_B200_API nemo_status_t nemo_b200_add_neurons(nemo_network_t, unsigned type, size_t n,
+		const unsigned idx[], unsigned nargs, const float args[]);
+/* Bulk form of nemo_add_synapse.  ids may be NULL. */
+NEMO_B200_API nemo_status_t nemo_b200_add_synapses(nemo_network_t, size_t n,
+		const unsigned source[], const unsigned target[], const unsigned delay[],
+		const float weight[], const unsigned char plastic[], synapse_id ids[]);
+/* The reference's example network random::construct
+ * (src/examples/random.cpp:63-88), generated in native code. */
+NEMO_B200_API nemo_status_t nemo_b200_example_random(nemo_network_t* net,
+		unsigned ncount, unsigned scount, unsigned dmax, int stdp);
+
+/* Run `steps` unstimulated steps on the device without returning to the
+ * host in between.  If stdp_period != 0, applyStdp(reward) is applied after
+ * every step whose 1-based index is a multiple of stdp_period.  Per-step
+ * fired counts and synaptic events (sum of the out-degrees of the neurons
+ * that fired) are written to fired_counts/events when non-NULL; fired ids of
+ * each step, in the order nemo_step returns them, are appended to fired_ids
+ * (capacity fired_cap, total in *fired_len) when fired_ids is non-NULL. */
+NEMO_B200_API nemo_status_t nemo_b200_run(nemo_simulation_t, unsigned steps,
+		unsigned stdp_period, float reward,
+		unsigned fired_counts[], uint64_t events[],
+		unsigned fired_ids[], size_t fired_cap, size_t* fired_len);
+
+/* Read every synapse weight (raw Q11.20) in network iteration order: source
+ * neurons ascending, each source's synapses in insertion order. */
+NEMO_B200_API nemo_status_t nemo_b200_get_weights_fx(nemo_simulation_t, int32_t out[], size_t cap, size_t* len);
+/* Read all state variables of the neurons of network type `type`, as
+ * [var][neuron] in insertion order. */
+NEMO_B200_API nemo_status_t nemo_b200_get_type_state(nemo_simulation_t, unsigned type,
+		float out[], size_t cap, size_t* len);
+/* Number of synapses in the simulation and the out-degree of each neuron in
+ * the order of nemo_b200_get_type_state's neurons (type order, then
+ * insertion order). */
+NEMO_B200_API nemo_status_t nemo_b200_synapse_count(nemo_simulation_t, uint64_t* count);
+/* Device time (ms, CUDA events) of the last nemo_b200_run, and the summed
+ * time of its dominant kernel (the per-step update/scatter kernel) with its
+ * launch count. */
+NEMO_B200_API nemo_status_t nemo_b200_last_run_timing(nemo_simulation_t, float* run_ms,
+		float* step_kernel_ms, unsigned* step_kernel_launches);
+/* Names of the compiled-in neuron types, one per call (index < count). */
+NEMO_B200_API unsigned nemo_b200_neuron_type_count(void);
+NEMO_B200_API const char* nemo_b200_neuron_type_name(unsigned i);
+/* The host-libm calibration used to reproduce glibc logf/sinf bit for bit on
+ * the device: the number of inputs at which the device's own double-precision
+ * evaluation rounds differently from the host libm, for logf and sinf. */
+NEMO_B200_API nemo_status_t nemo_b200_libm_calibration(uint64_t* log_flips, uint64_t* sin_flips,
+		uint64_t* exceptions);
+/* Host build of the device's glibc-exact nrand (for tests): advances the
+ * xorshift state in place and returns the normal deviate. */
+NEMO_B200_API float nemo_b200_host_nrand(unsigned state[4]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,355 @@
+"""nemosim_b200 -- a B200 (sm_100a) simulation backend for the NeMo spiking
+neural network simulator.
+
+The native library (``lib/libnemo_b200.so``, C ABI in ``include/nemo_b200.h``)
+is a drop-in for the reference C API (src/nemo.h).  This module binds it with
+ctypes behind the interface of the reference's Python binding
+(src/api/python/nemo_py.cpp:729-816 and src/api/python/__init__.py.in):
+``Network``, ``Configuration`` and ``Simulation`` with the same method names,
+argument meaning and errors (a ``NemoError`` carrying the reference status
+code).  Vector arguments are accepted wherever the reference binding accepts
+lists.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import lib, library_path  # noqa: F401
+
+NEMO_OK = 0
+NEMO_INVALID_INPUT = 6
+NEMO_BACKEND_CUDA = 0
+NEMO_BACKEND_CPU = 1
+
+
+class NemoError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _check(code: int):
+    if code != NEMO_OK:
+        raise NemoError(code, lib().nemo_strerror().decode())
+
+
+def _u32(x):
+    return np.ascontiguousarray(np.atleast_1d(np.asarray(x, dtype=np.uint32)))
+
+
+def _f32(x):
+    return np.ascontiguousarray(np.atleast_1d(np.asarray(x, dtype=np.float32)))
+
+
+_EMPTY_U32 = np.zeros(1, np.uint32)
+_EMPTY_F32 = np.zeros(1, np.float32)
+
+
+def version() -> str:
+    return lib().nemo_version().decode()
+
+
+def cuda_device_count() -> int:
+    n = C.c_uint()
+    _check(lib().nemo_cuda_device_count(C.byref(n)))
+    return n.value
+
+
+class Configuration:
+    """nemo::Configuration (src/nemo/Configuration.hpp)."""
+
+    def __init__(self):
+        self._h = lib().nemo_new_configuration()
+        if not self._h:
+            raise NemoError(10, lib().nemo_strerror().decode())
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().nemo_delete_configuration(self._h)
+            self._h = None
+
+    def set_stdp_function(self, prefire, postfire, *limits):
+        """(pre, post, min_weight, max_weight) or (pre, post, minE, maxE, minI, maxI):
+        the two overloads of Configuration::setStdpFunction
+        (src/nemo/Configuration.cpp:80-100)."""
+        if len(limits) == 2:
+            min_w, max_w = limits
+            limits = (0.0, max_w, 0.0, min_w)
+        if len(limits) != 4:
+            raise TypeError("set_stdp_function takes 2 or 4 weight limits")
+        pre, post = _f32(prefire), _f32(postfire)
+        _check(lib().nemo_set_stdp_function(self._h, pre, len(pre), post, len(post),
+                                            *[float(v) for v in limits]))
+
+    def set_cuda_backend(self, device: int = -1):
+        _check(lib().nemo_set_cuda_backend(self._h, int(device)))
+
+    def set_cpu_backend(self):
+        _check(lib().nemo_set_cpu_backend(self._h))
+
+    def set_write_only_synapses(self):
+        _check(lib().nemo_set_write_only_synapses(self._h))
+
+    def backend_description(self) -> str:
+        d = C.c_char_p()
+        _check(lib().nemo_backend_description(self._h, C.byref(d)))
+        return d.value.decode()
+
+
+class Network:
+    """nemo::Network (src/nemo/Network.hpp)."""
+
+    def __init__(self, _handle=None):
+        self._h = _handle if _handle is not None else lib().nemo_new_network()
+        if not self._h:
+            raise NemoError(10, lib().nemo_strerror().decode())
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().nemo_delete_network(self._h)
+            self._h = None
+
+    def add_neuron_type(self, name: str) -> int:
+        t = C.c_uint()
+        _check(lib().nemo_add_neuron_type(self._h, name.encode(), C.byref(t)))
+        return t.value
+
+    def add_neuron(self, ntype: int, idx, *args):
+        """add_neuron(type, idx, p0, ..., s0, ...); idx and each argument may
+        be a scalar or a vector (src/api/python/nemo_py.cpp add_neuron_va)."""
+        idx = _u32(idx)
+        n = len(idx)
+        cols = [np.broadcast_to(_f32(a), (n,)) for a in args]
+        mat = np.ascontiguousarray(np.stack(cols, axis=1), dtype=np.float32).reshape(-1) if cols else _EMPTY_F32
+        _check(lib().nemo_b200_add_neurons(self._h, ntype, n, idx, len(args), mat))
+
+    def add_synapse(self, source, target, delay, weight, plastic):
+        """Returns the synapse id (or a vector of ids for vector arguments)."""
+        src, tgt, dly = _u32(source), _u32(target), _u32(delay)
+        w = _f32(weight)
+        pl = np.ascontiguousarray(np.atleast_1d(np.asarray(plastic, dtype=np.uint8)))
+        n = max(len(src), len(tgt), len(dly), len(w), len(pl))
+        src, tgt, dly, w, pl = (np.ascontiguousarray(np.broadcast_to(a, (n,))) for a in (src, tgt, dly, w, pl))
+        ids = np.zeros(max(n, 1), np.uint64)
+        _check(lib().nemo_b200_add_synapses(self._h, n, src, tgt, dly, w, pl, ids))
+        scalar = all(np.ndim(a) == 0 for a in (source, target, delay, weight, plastic))
+        return int(ids[0]) if scalar else ids[:n]
+
+    def neuron_count(self) -> int:
+        c = C.c_uint()
+        _check(lib().nemo_neuron_count(self._h, C.byref(c)))
+        return c.value
+
+    def _getf(self, fn, *args):
+        v = C.c_float()
+        _check(fn(self._h, *args, C.byref(v)))
+        return v.value
+
+    def get_neuron_state(self, idx, var):
+        return self._getf(lib().nemo_get_neuron_state_n, idx, var)
+
+    def get_neuron_parameter(self, idx, p):
+        return self._getf(lib().nemo_get_neuron_parameter_n, idx, p)
+
+    def set_neuron(self, idx, *args):
+        a = _f32(args)
+        _check(lib().nemo_set_neuron_n(self._h, idx, len(a), a))
+
+    def set_neuron_state(self, idx, var, val):
+        _check(lib().nemo_set_neuron_state_n(self._h, idx, var, float(val)))
+
+    def set_neuron_parameter(self, idx, p, val):
+        _check(lib().nemo_set_neuron_parameter_n(self._h, idx, p, float(val)))
+
+    def get_synapses_from(self, source):
+        p = C.POINTER(C.c_uint64)()
+        n = C.c_size_t()
+        _check(lib().nemo_get_synapses_from_n(self._h, source, C.byref(p), C.byref(n)))
+        return [p[i] for i in range(n.value)]
+
+    def _getu(self, fn, sid):
+        v = C.c_uint()
+        _check(fn(self._h, C.c_uint64(sid), C.byref(v)))
+        return v.value
+
+    def get_synapse_source(self, sid):
+        return self._getu(lib().nemo_get_synapse_source_n, sid)
+
+    def get_synapse_target(self, sid):
+        return self._getu(lib().nemo_get_synapse_target_n, sid)
+
+    def get_synapse_delay(self, sid):
+        return self._getu(lib().nemo_get_synapse_delay_n, sid)
+
+    def get_synapse_weight(self, sid):
+        return self._getf(lib().nemo_get_synapse_weight_n, C.c_uint64(sid))
+
+    def get_synapse_plastic(self, sid):
+        v = C.c_ubyte()
+        _check(lib().nemo_get_synapse_plastic_n(self._h, C.c_uint64(sid), C.byref(v)))
+        return bool(v.value)
+
+
+def example_random(ncount: int, scount: int, dmax: int, stdp: bool) -> Network:
+    """The reference's example network random::construct
+    (src/examples/random.cpp:63-88)."""
+    h = C.c_void_p()
+    _check(lib().nemo_b200_example_random(C.byref(h), ncount, scount, dmax, int(stdp)))
+    return Network(h.value)
+
+
+class Simulation:
+    """nemo::Simulation on the B200 backend."""
+
+    def __init__(self, net: Network, conf: Configuration):
+        h = lib().nemo_new_simulation(net._h, conf._h)
+        if not h:
+            raise NemoError(NEMO_INVALID_INPUT, lib().nemo_strerror().decode())
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().nemo_delete_simulation(self._h)
+            self._h = None
+
+    def step(self, fstim=None, istim=None):
+        """One 1 ms cycle; returns the fired neuron ids (src/api/python/__init__.py.in step)."""
+        f = _u32(fstim) if fstim is not None and len(fstim) else None
+        if istim:
+            inid = _u32([p[0] for p in istim])
+            icur = _f32([p[1] for p in istim])
+        else:
+            inid = icur = None
+        fired = C.POINTER(C.c_uint)()
+        n = C.c_size_t()
+        _check(lib().nemo_step(self._h, f if f is not None else _EMPTY_U32, 0 if f is None else len(f),
+                               inid if inid is not None else _EMPTY_U32,
+                               icur if icur is not None else _EMPTY_F32, 0 if inid is None else len(inid),
+                               C.byref(fired), C.byref(n)))
+        if n.value == 0:
+            return []
+        return np.ctypeslib.as_array(fired, shape=(n.value,)).tolist()
+
+    def run(self, steps: int, stdp_period: int = 0, reward: float = 1.0, ids: bool = True,
+            max_ids: int | None = None):
+        """Device-resident run of `steps` unstimulated steps (an extension):
+        returns (fired counts, synaptic events, fired ids or None)."""
+        counts = np.zeros(max(steps, 1), np.uint32)
+        events = np.zeros(max(steps, 1), np.uint64)
+        cap = max_ids if max_ids is not None else steps * 4096
+        buf = np.zeros(max(cap, 1), np.uint32) if ids else None
+        ln = C.c_size_t()
+
+        def ptr(a):
+            return None if a is None else a.ctypes.data_as(C.c_void_p)
+        _check(lib().nemo_b200_run(self._h, steps, stdp_period, reward, ptr(counts), ptr(events), ptr(buf),
+                                   cap if buf is not None else 0, C.byref(ln)))
+        if buf is None:
+            return counts[:steps], events[:steps], None
+        return counts[:steps], events[:steps], buf[: ln.value].copy()
+
+    def apply_stdp(self, reward: float):
+        _check(lib().nemo_apply_stdp(self._h, float(reward)))
+
+    def _getf(self, fn, *args):
+        v = C.c_float()
+        _check(fn(self._h, *args, C.byref(v)))
+        return v.value
+
+    def get_neuron_state(self, idx, var):
+        return self._getf(lib().nemo_get_neuron_state_s, idx, var)
+
+    def get_neuron_parameter(self, idx, p):
+        return self._getf(lib().nemo_get_neuron_parameter_s, idx, p)
+
+    def get_membrane_potential(self, idx):
+        return self._getf(lib().nemo_get_membrane_potential, idx)
+
+    def set_neuron(self, idx, *args):
+        a = _f32(args)
+        _check(lib().nemo_set_neuron_s(self._h, idx, len(a), a))
+
+    def set_neuron_state(self, idx, var, val):
+        _check(lib().nemo_set_neuron_state_s(self._h, idx, var, float(val)))
+
+    def set_neuron_parameter(self, idx, p, val):
+        _check(lib().nemo_set_neuron_parameter_s(self._h, idx, p, float(val)))
+
+    def get_synapses_from(self, source):
+        p = C.POINTER(C.c_uint64)()
+        n = C.c_size_t()
+        _check(lib().nemo_get_synapses_from_s(self._h, source, C.byref(p), C.byref(n)))
+        return [p[i] for i in range(n.value)]
+
+    def _getu(self, fn, sid):
+        v = C.c_uint()
+        _check(fn(self._h, C.c_uint64(sid), C.byref(v)))
+        return v.value
+
+    def get_synapse_source(self, sid):
+        return self._getu(lib().nemo_get_synapse_source_s, sid)
+
+    def get_synapse_target(self, sid):
+        return self._getu(lib().nemo_get_synapse_target_s, sid)
+
+    def get_synapse_delay(self, sid):
+        return self._getu(lib().nemo_get_synapse_delay_s, sid)
+
+    def get_synapse_weight(self, sid):
+        return self._getf(lib().nemo_get_synapse_weight_s, C.c_uint64(sid))
+
+    def get_synapse_plastic(self, sid):
+        v = C.c_ubyte()
+        _check(lib().nemo_get_synapse_plastic_s(self._h, C.c_uint64(sid), C.byref(v)))
+        return bool(v.value)
+
+    def weights_fx(self, nsyn: int | None = None) -> np.ndarray:
+        """All weights (raw Q11.20) in network iteration order (an extension)."""
+        if nsyn is None:
+            nsyn = self.synapse_count()
+        out = np.zeros(max(nsyn, 1), np.int32)
+        ln = C.c_size_t()
+        _check(lib().nemo_b200_get_weights_fx(self._h, out, len(out), C.byref(ln)))
+        return out[: ln.value]
+
+    def type_state(self, ntype: int, nstate: int, n: int) -> np.ndarray:
+        out = np.zeros(max(nstate * n, 1), np.float32)
+        ln = C.c_size_t()
+        _check(lib().nemo_b200_get_type_state(self._h, ntype, out, len(out), C.byref(ln)))
+        return out[: ln.value].reshape(nstate, n) if ln.value else np.zeros((nstate, 0), np.float32)
+
+    def synapse_count(self) -> int:
+        v = C.c_uint64()
+        _check(lib().nemo_b200_synapse_count(self._h, C.byref(v)))
+        return v.value
+
+    def last_run_timing(self):
+        a, b, c = C.c_float(), C.c_float(), C.c_uint()
+        _check(lib().nemo_b200_last_run_timing(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def elapsed_wallclock(self):
+        v = C.c_ulong()
+        _check(lib().nemo_elapsed_wallclock(self._h, C.byref(v)))
+        return v.value
+
+    def elapsed_simulation(self):
+        v = C.c_ulong()
+        _check(lib().nemo_elapsed_simulation(self._h, C.byref(v)))
+        return v.value
+
+    def reset_timer(self):
+        _check(lib().nemo_reset_timer(self._h))
+
+
+def host_nrand(state: np.ndarray) -> float:
+    """Host build of the device's glibc-exact nrand (advances `state`)."""
+    return lib().nemo_b200_host_nrand(state)
+
+
+def libm_calibration():
+    a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    _check(lib().nemo_b200_libm_calibration(C.byref(a), C.byref(b), C.byref(c)))
+    return a.value, b.value, c.value

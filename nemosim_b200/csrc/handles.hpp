@@ -1,0 +1,11 @@
+// handles.hpp -- the objects behind the C ABI's opaque handles.
+#pragma once
+
+#include <memory>
+
+#include "network.hpp"
+#include "simulation.hpp"
+
+struct nemo_network_class { nemo_b200::Network net; };
+struct nemo_configuration_class { nemo_b200::Configuration conf; };
+struct nemo_simulation_class { std::unique_ptr<nemo_b200::Simulation> sim; };

@@ -1,0 +1,112 @@
+// libm_calib.cpp -- host calibration of the device's logf/sinf against the
+// host C library (see nemo_libm.cuh for the method).
+//
+// The reference CPU backend takes its input noise from the host libm
+// (src/nemo/RNG.cpp:30-32), so the calibration is made against the libm of
+// the process that runs the simulation: every reachable argument is
+// evaluated with both the libm and the device's own double-precision
+// routine, once per process, on all host threads (about a second).
+#include "libm_calib.hpp"
+
+#include <math.h>
+
+#include <algorithm>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+namespace nemo_b200 {
+
+namespace {
+
+struct Exc { uint32_t key, val; };
+
+void calibrate_range(bool isLog, uint32_t wbegin, uint32_t wend, uint32_t count,
+		std::vector<uint32_t>& bits, uint64_t& flips, std::vector<Exc>& exc)
+{
+	for(uint32_t w = wbegin; w < wend; ++w) {
+		uint32_t word = 0;
+		for(uint32_t b = 0; b < 32; ++b) {
+			uint32_t idx = w * 32 + b;
+			if(idx >= count) break;
+			float libm, mine;
+			double d;
+			if(isLog) {
+				float x = (float) idx * 0x1p-24f;
+				if(x == 0.0f) continue; // special-cased on the device
+				libm = logf(x);
+				d = nb_log_d((double) x);
+			} else {
+				float fu = nb_sin_value(idx);
+				float a = fu * NB_NRAND_A;
+				libm = sinf(a);
+				d = nb_sin_d((double) a);
+			}
+			mine = (float) d;
+			if(nb_fbits(libm) != nb_fbits(mine)) {
+				word |= 1u << b;
+				flips++;
+				float stepped = nb_step_toward(mine, d);
+				if(nb_fbits(stepped) != nb_fbits(libm)) {
+					exc.push_back(Exc{ (isLog ? 0u : (1u << 31)) | idx, nb_fbits(libm) });
+				}
+			}
+		}
+		bits[w] = word;
+	}
+}
+
+void calibrate(bool isLog, uint32_t count, std::vector<uint32_t>& bits, uint64_t& flips,
+		std::vector<Exc>& exc)
+{
+	uint32_t nwords = (count + 31) / 32;
+	bits.assign(nwords, 0);
+	unsigned nt = std::max(1u, std::thread::hardware_concurrency());
+	std::vector<std::thread> threads;
+	std::vector<uint64_t> tflips(nt, 0);
+	std::vector<std::vector<Exc>> texc(nt);
+	uint32_t chunk = (nwords + nt - 1) / nt;
+	for(unsigned t = 0; t < nt; ++t) {
+		uint32_t b = std::min(nwords, t * chunk), e = std::min(nwords, (t + 1) * chunk);
+		threads.emplace_back([&, t, b, e] { calibrate_range(isLog, b, e, count, bits, tflips[t], texc[t]); });
+	}
+	for(auto& th : threads) th.join();
+	flips = 0;
+	for(unsigned t = 0; t < nt; ++t) {
+		flips += tflips[t];
+		exc.insert(exc.end(), texc[t].begin(), texc[t].end());
+	}
+}
+
+} // namespace
+
+const CalibTables& libm_calibration()
+{
+	static CalibTables tables;
+	static std::once_flag once;
+	std::call_once(once, [] {
+		std::vector<Exc> exc;
+		calibrate(true, NB_LOG_COUNT, tables.logFlip, tables.logFlips, exc);
+		calibrate(false, NB_SIN_COUNT, tables.sinFlip, tables.sinFlips, exc);
+		std::sort(exc.begin(), exc.end(), [](const Exc& a, const Exc& b) { return a.key < b.key; });
+		for(const Exc& e : exc) {
+			tables.excKey.push_back(e.key);
+			tables.excVal.push_back(e.val);
+		}
+	});
+	return tables;
+}
+
+LibmCalib host_calib_view()
+{
+	const CalibTables& t = libm_calibration();
+	LibmCalib c;
+	c.logFlip = t.logFlip.data();
+	c.sinFlip = t.sinFlip.data();
+	c.excKey = t.excKey.data();
+	c.excVal = t.excVal.data();
+	c.nexc = (uint32_t) t.excKey.size();
+	return c;
+}
+
+} // namespace nemo_b200

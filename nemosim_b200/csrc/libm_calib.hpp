@@ -1,0 +1,25 @@
+// libm_calib.hpp -- calibration tables that let the device reproduce the
+// host libm's logf/sinf at every argument nrand can produce.
+#pragma once
+
+#include <stdint.h>
+
+#include <vector>
+
+#include "nemo_libm.cuh"
+
+namespace nemo_b200 {
+
+struct CalibTables {
+	std::vector<uint32_t> logFlip, sinFlip;  // one bit per reachable argument
+	std::vector<uint32_t> excKey, excVal;    // arguments a one-ulp step cannot fix
+	uint64_t logFlips = 0, sinFlips = 0;
+};
+
+// Computed once per process against the host libm (thread-safe).
+const CalibTables& libm_calibration();
+
+// A LibmCalib whose pointers refer to the host tables.
+LibmCalib host_calib_view();
+
+} // namespace nemo_b200

@@ -1,0 +1,578 @@
+// nemo_c.cpp -- the C ABI (include/nemo_b200.h).
+//
+// Exceptions never cross the ABI: every call catches them and converts them
+// to a status code plus a process-global message, as the reference C API
+// does (src/nemo/nemo_c.cpp:21-65).  Like the reference, the message is not
+// thread-safe.
+#include <cuda_runtime.h>
+#include <string.h>
+#include <sys/stat.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/nemo_b200.h"
+#include "libm_calib.hpp"
+#include "handles.hpp"
+#include "network.hpp"
+#include "simulation.hpp"
+
+using namespace nemo_b200;
+
+
+static std::string g_lastError;
+static nemo_status_t g_lastStatus = NEMO_OK;
+
+static void setResult(const char* msg, nemo_status_t status)
+{
+	g_lastError = msg;
+	g_lastStatus = status;
+}
+
+#define CALL(...)                                                               \
+	do {                                                                        \
+		g_lastStatus = NEMO_OK;                                                 \
+		try {                                                                   \
+			__VA_ARGS__;                                                             \
+		} catch(const Error& e) {                                               \
+			setResult(e.what(), e.code());                                      \
+		} catch(const std::bad_alloc&) {                                        \
+			setResult("host memory allocation failed", NEMO_ALLOCATION_ERROR);  \
+		} catch(const std::exception& e) {                                      \
+			setResult(e.what(), NEMO_UNKNOWN_ERROR);                            \
+		} catch(...) {                                                          \
+			setResult("unknown exception", NEMO_UNKNOWN_ERROR);                 \
+		}                                                                       \
+		return g_lastStatus;                                                    \
+	} while(0)
+
+#define NULLCHECK(p)                                                            \
+	do {                                                                        \
+		if(!(p)) {                                                              \
+			setResult("NULL handle or output pointer", NEMO_INVALID_INPUT);     \
+			return NEMO_INVALID_INPUT;                                          \
+		}                                                                       \
+	} while(0)
+
+static Simulation& S(nemo_simulation_t s) { return *s->sim; }
+
+extern "C" {
+
+const char* nemo_version(void) { return "0.7.2-b200"; }
+
+const char* nemo_strerror(void) { return g_lastError.c_str(); }
+
+nemo_status_t nemo_add_plugin_path(const char* dir)
+{
+	NULLCHECK(dir);
+	CALL({
+		struct stat st;
+		if(stat(dir, &st) != 0 || !S_ISDIR(st.st_mode)) {
+			NB_THROW(NEMO_INVALID_INPUT, "%s is not a directory", dir);
+		}
+	});
+}
+
+nemo_status_t nemo_cuda_device_count(unsigned* count)
+{
+	NULLCHECK(count);
+	*count = 0;
+	CALL({
+		int n = 0;
+		cudaError_t e = cudaGetDeviceCount(&n);
+		if(e != cudaSuccess) NB_THROW(NEMO_CUDA_ERROR, "%s", cudaGetErrorString(e));
+		*count = (unsigned) n;
+	});
+}
+
+static std::vector<std::string> g_descr;
+
+nemo_status_t nemo_cuda_device_description(unsigned device, const char** descr)
+{
+	NULLCHECK(descr);
+	CALL({
+		cudaDeviceProp p;
+		cudaError_t e = cudaGetDeviceProperties(&p, (int) device);
+		if(e != cudaSuccess) NB_THROW(NEMO_CUDA_ERROR, "%s", cudaGetErrorString(e));
+		if(g_descr.size() <= device) g_descr.resize(device + 1);
+		g_descr[device] = format("%s (sm_%d%d, %d SMs, %.0f GB)", p.name, p.major, p.minor,
+				p.multiProcessorCount, p.totalGlobalMem / 1e9);
+		*descr = g_descr[device].c_str();
+	});
+}
+
+unsigned cuda_device_count(void)
+{
+	unsigned n = 0;
+	return nemo_cuda_device_count(&n) == NEMO_OK ? n : 0;
+}
+
+const char* cuda_device_description(unsigned device)
+{
+	const char* d = nullptr;
+	return nemo_cuda_device_description(device, &d) == NEMO_OK ? d : "";
+}
+
+/* --- configuration --- */
+
+nemo_configuration_t nemo_new_configuration(void)
+{
+	try {
+		auto* c = new nemo_configuration_class();
+		c->conf.description = "B200 (sm_100a) backend";
+		return c;
+	} catch(...) {
+		setResult("failed to allocate configuration", NEMO_ALLOCATION_ERROR);
+		return nullptr;
+	}
+}
+
+void nemo_delete_configuration(nemo_configuration_t c) { delete c; }
+
+nemo_status_t nemo_log_stdout(nemo_configuration_t c)
+{
+	NULLCHECK(c);
+	CALL(c->conf.logging = true);
+}
+
+nemo_status_t nemo_set_stdp_function(nemo_configuration_t c, float pre[], size_t npre,
+		float post[], size_t npost, float minE, float maxE, float minI, float maxI)
+{
+	NULLCHECK(c);
+	CALL(c->conf.setStdpFunction(pre, npre, post, npost, minE, maxE, minI, maxI));
+}
+
+nemo_status_t nemo_set_cpu_backend(nemo_configuration_t c)
+{
+	NULLCHECK(c);
+	CALL({
+		c->conf.backend = NEMO_BACKEND_CPU;
+		c->conf.description = "CPU backend (not provided by this library)";
+	});
+}
+
+nemo_status_t nemo_set_cuda_backend(nemo_configuration_t c, int dev)
+{
+	NULLCHECK(c);
+	CALL({
+		int n = 0;
+		cudaError_t e = cudaGetDeviceCount(&n);
+		if(e != cudaSuccess || n == 0) NB_THROW(NEMO_CUDA_ERROR, "No CUDA device available");
+		if(dev >= n) NB_THROW(NEMO_INVALID_INPUT, "Invalid CUDA device %d", dev);
+		c->conf.backend = NEMO_BACKEND_CUDA;
+		c->conf.device = dev;
+		c->conf.description = "B200 (sm_100a) backend";
+	});
+}
+
+nemo_status_t nemo_cuda_device(nemo_configuration_t c, int* dev)
+{
+	NULLCHECK(c);
+	NULLCHECK(dev);
+	CALL(*dev = c->conf.device);
+}
+
+nemo_status_t nemo_backend(nemo_configuration_t c, backend_t* b)
+{
+	NULLCHECK(c);
+	NULLCHECK(b);
+	CALL(*b = c->conf.backend);
+}
+
+nemo_status_t nemo_backend_description(nemo_configuration_t c, const char** d)
+{
+	NULLCHECK(c);
+	NULLCHECK(d);
+	CALL(*d = c->conf.description.c_str());
+}
+
+nemo_status_t nemo_set_write_only_synapses(nemo_configuration_t c)
+{
+	NULLCHECK(c);
+	CALL(c->conf.writeOnlySynapses = true);
+}
+
+/* --- network --- */
+
+nemo_network_t nemo_new_network(void)
+{
+	try {
+		return new nemo_network_class();
+	} catch(...) {
+		setResult("failed to allocate network", NEMO_ALLOCATION_ERROR);
+		return nullptr;
+	}
+}
+
+void nemo_delete_network(nemo_network_t n) { delete n; }
+
+nemo_status_t nemo_add_neuron_type(nemo_network_t n, const char* name, unsigned* type)
+{
+	NULLCHECK(n);
+	NULLCHECK(name);
+	NULLCHECK(type);
+	CALL(*type = n->net.addNeuronType(name));
+}
+
+/* Network::addNeuron(idx, a, b, c, d, u, v, sigma) (src/nemo/Network.cpp:45-55) */
+nemo_status_t nemo_add_neuron_iz(nemo_network_t n, unsigned idx, float a, float b, float c,
+		float d, float u, float v, float sigma)
+{
+	NULLCHECK(n);
+	CALL({
+		unsigned t = n->net.addNeuronType("Izhikevich");
+		float args[7] = { a, b, c, d, sigma, u, v };
+		n->net.addNeurons(t, 1, &idx, 7, args);
+	});
+}
+
+nemo_status_t nemo_add_neuron(nemo_network_t n, unsigned type, unsigned idx, unsigned nargs, float args[])
+{
+	NULLCHECK(n);
+	CALL(n->net.addNeurons(type, 1, &idx, nargs, args));
+}
+
+nemo_status_t nemo_b200_add_neurons(nemo_network_t n, unsigned type, size_t count,
+		const unsigned idx[], unsigned nargs, const float args[])
+{
+	NULLCHECK(n);
+	CALL(n->net.addNeurons(type, count, idx, nargs, args));
+}
+
+nemo_status_t nemo_add_synapse(nemo_network_t n, unsigned source, unsigned target, unsigned delay,
+		float weight, unsigned char plastic, synapse_id* id)
+{
+	NULLCHECK(n);
+	CALL(n->net.addSynapses(1, &source, &target, &delay, &weight, &plastic, id));
+}
+
+nemo_status_t nemo_b200_add_synapses(nemo_network_t n, size_t count, const unsigned source[],
+		const unsigned target[], const unsigned delay[], const float weight[],
+		const unsigned char plastic[], synapse_id ids[])
+{
+	NULLCHECK(n);
+	CALL(n->net.addSynapses(count, source, target, delay, weight, plastic, ids));
+}
+
+nemo_status_t nemo_neuron_count(nemo_network_t n, unsigned* count)
+{
+	NULLCHECK(n);
+	NULLCHECK(count);
+	CALL(*count = n->net.neuronCount());
+}
+
+nemo_status_t nemo_get_neuron_state_n(nemo_network_t n, unsigned neuron, unsigned var, float* val)
+{
+	NULLCHECK(n);
+	NULLCHECK(val);
+	CALL(*val = n->net.getNeuronState(neuron, var));
+}
+
+nemo_status_t nemo_get_neuron_parameter_n(nemo_network_t n, unsigned neuron, unsigned param, float* val)
+{
+	NULLCHECK(n);
+	NULLCHECK(val);
+	CALL(*val = n->net.getNeuronParameter(neuron, param));
+}
+
+nemo_status_t nemo_set_neuron_n(nemo_network_t n, unsigned idx, unsigned nargs, float args[])
+{
+	NULLCHECK(n);
+	CALL(n->net.setNeuron(idx, nargs, args));
+}
+
+nemo_status_t nemo_set_neuron_iz_n(nemo_network_t n, unsigned idx, float a, float b, float c,
+		float d, float u, float v, float sigma)
+{
+	NULLCHECK(n);
+	float args[7] = { a, b, c, d, sigma, u, v };
+	CALL(n->net.setNeuron(idx, 7, args));
+}
+
+nemo_status_t nemo_set_neuron_state_n(nemo_network_t n, unsigned neuron, unsigned var, float val)
+{
+	NULLCHECK(n);
+	CALL(n->net.setNeuronState(neuron, var, val));
+}
+
+nemo_status_t nemo_set_neuron_parameter_n(nemo_network_t n, unsigned neuron, unsigned param, float val)
+{
+	NULLCHECK(n);
+	CALL(n->net.setNeuronParameter(neuron, param, val));
+}
+
+nemo_status_t nemo_get_synapse_source_n(nemo_network_t n, synapse_id s, unsigned* source)
+{
+	NULLCHECK(n);
+	NULLCHECK(source);
+	CALL({
+		(void) n->net.getSynapseTarget(s); // validates the id
+		*source = (unsigned) (s >> 32);
+	});
+}
+
+nemo_status_t nemo_get_synapse_target_n(nemo_network_t n, synapse_id s, unsigned* target)
+{
+	NULLCHECK(n);
+	NULLCHECK(target);
+	CALL(*target = n->net.getSynapseTarget(s));
+}
+
+nemo_status_t nemo_get_synapse_delay_n(nemo_network_t n, synapse_id s, unsigned* delay)
+{
+	NULLCHECK(n);
+	NULLCHECK(delay);
+	CALL(*delay = n->net.getSynapseDelay(s));
+}
+
+nemo_status_t nemo_get_synapse_weight_n(nemo_network_t n, synapse_id s, float* weight)
+{
+	NULLCHECK(n);
+	NULLCHECK(weight);
+	CALL(*weight = n->net.getSynapseWeight(s));
+}
+
+nemo_status_t nemo_get_synapse_plastic_n(nemo_network_t n, synapse_id s, unsigned char* plastic)
+{
+	NULLCHECK(n);
+	NULLCHECK(plastic);
+	CALL(*plastic = n->net.getSynapsePlastic(s));
+}
+
+nemo_status_t nemo_get_synapses_from_n(nemo_network_t n, unsigned source, synapse_id* synapses[], size_t* len)
+{
+	NULLCHECK(n);
+	NULLCHECK(synapses);
+	NULLCHECK(len);
+	CALL({
+		const std::vector<uint64_t>& ids = n->net.getSynapsesFrom(source);
+		*synapses = ids.empty() ? nullptr : const_cast<synapse_id*>(ids.data());
+		*len = ids.size();
+	});
+}
+
+/* --- simulation --- */
+
+nemo_simulation_t nemo_new_simulation(nemo_network_t n, nemo_configuration_t c)
+{
+	if(!n || !c) {
+		setResult("NULL network or configuration", NEMO_INVALID_INPUT);
+		return nullptr;
+	}
+	g_lastStatus = NEMO_OK;
+	try {
+		auto* s = new nemo_simulation_class();
+		try {
+			s->sim.reset(new Simulation(n->net, c->conf));
+		} catch(...) {
+			delete s;
+			throw;
+		}
+		return s;
+	} catch(const Error& e) {
+		setResult(e.what(), e.code());
+	} catch(const std::bad_alloc&) {
+		setResult("host memory allocation failed", NEMO_ALLOCATION_ERROR);
+	} catch(const std::exception& e) {
+		setResult(e.what(), NEMO_UNKNOWN_ERROR);
+	}
+	return nullptr;
+}
+
+void nemo_delete_simulation(nemo_simulation_t s) { delete s; }
+
+/* nemo_c.cpp:440-477 */
+nemo_status_t nemo_step(nemo_simulation_t s, unsigned fstim[], size_t nf, unsigned inidx[],
+		float icur[], size_t ni, unsigned* fired[], size_t* nfired)
+{
+	NULLCHECK(s);
+	CALL({
+		const std::vector<unsigned>& f = S(s).step(fstim, nf, inidx, icur, ni);
+		if(fired) *fired = f.empty() ? nullptr : const_cast<unsigned*>(f.data());
+		if(nfired) *nfired = f.size();
+	});
+}
+
+nemo_status_t nemo_apply_stdp(nemo_simulation_t s, float reward)
+{
+	NULLCHECK(s);
+	CALL(S(s).applyStdp(reward));
+}
+
+nemo_status_t nemo_b200_run(nemo_simulation_t s, unsigned steps, unsigned stdpPeriod, float reward,
+		unsigned counts[], uint64_t events[], unsigned ids[], size_t cap, size_t* len)
+{
+	NULLCHECK(s);
+	CALL(S(s).run(steps, stdpPeriod, reward, counts, events, ids, cap, len));
+}
+
+nemo_status_t nemo_get_membrane_potential(nemo_simulation_t s, unsigned neuron, float* v)
+{
+	NULLCHECK(s);
+	NULLCHECK(v);
+	CALL(*v = S(s).getMembranePotential(neuron));
+}
+
+nemo_status_t nemo_get_neuron_state_s(nemo_simulation_t s, unsigned neuron, unsigned var, float* val)
+{
+	NULLCHECK(s);
+	NULLCHECK(val);
+	CALL(*val = S(s).getNeuronState(neuron, var));
+}
+
+nemo_status_t nemo_get_neuron_parameter_s(nemo_simulation_t s, unsigned neuron, unsigned p, float* val)
+{
+	NULLCHECK(s);
+	NULLCHECK(val);
+	CALL(*val = S(s).getNeuronParameter(neuron, p));
+}
+
+nemo_status_t nemo_set_neuron_s(nemo_simulation_t s, unsigned idx, unsigned nargs, float args[])
+{
+	NULLCHECK(s);
+	CALL(S(s).setNeuron(idx, nargs, args));
+}
+
+nemo_status_t nemo_set_neuron_iz_s(nemo_simulation_t s, unsigned idx, float a, float b, float c,
+		float d, float u, float v, float sigma)
+{
+	NULLCHECK(s);
+	float args[7] = { a, b, c, d, sigma, u, v };
+	CALL(S(s).setNeuron(idx, 7, args));
+}
+
+nemo_status_t nemo_set_neuron_state_s(nemo_simulation_t s, unsigned neuron, unsigned var, float val)
+{
+	NULLCHECK(s);
+	CALL(S(s).setNeuronState(neuron, var, val));
+}
+
+nemo_status_t nemo_set_neuron_parameter_s(nemo_simulation_t s, unsigned neuron, unsigned p, float val)
+{
+	NULLCHECK(s);
+	CALL(S(s).setNeuronParameter(neuron, p, val));
+}
+
+nemo_status_t nemo_get_synapse_source_s(nemo_simulation_t s, synapse_id id, unsigned* source)
+{
+	NULLCHECK(s);
+	NULLCHECK(source);
+	CALL({
+		(void) S(s).getSynapseTarget(id);
+		*source = (unsigned) (id >> 32);
+	});
+}
+
+nemo_status_t nemo_get_synapse_target_s(nemo_simulation_t s, synapse_id id, unsigned* target)
+{
+	NULLCHECK(s);
+	NULLCHECK(target);
+	CALL(*target = S(s).getSynapseTarget(id));
+}
+
+nemo_status_t nemo_get_synapse_delay_s(nemo_simulation_t s, synapse_id id, unsigned* delay)
+{
+	NULLCHECK(s);
+	NULLCHECK(delay);
+	CALL(*delay = S(s).getSynapseDelay(id));
+}
+
+nemo_status_t nemo_get_synapse_weight_s(nemo_simulation_t s, synapse_id id, float* weight)
+{
+	NULLCHECK(s);
+	NULLCHECK(weight);
+	CALL(*weight = S(s).getSynapseWeight(id));
+}
+
+nemo_status_t nemo_get_synapse_plastic_s(nemo_simulation_t s, synapse_id id, unsigned char* plastic)
+{
+	NULLCHECK(s);
+	NULLCHECK(plastic);
+	CALL(*plastic = S(s).getSynapsePlastic(id));
+}
+
+nemo_status_t nemo_get_synapses_from_s(nemo_simulation_t s, unsigned source, synapse_id* synapses[], size_t* len)
+{
+	NULLCHECK(s);
+	NULLCHECK(synapses);
+	NULLCHECK(len);
+	CALL({
+		const std::vector<uint64_t>& ids = S(s).getSynapsesFrom(source);
+		*synapses = ids.empty() ? nullptr : const_cast<synapse_id*>(ids.data());
+		*len = ids.size();
+	});
+}
+
+nemo_status_t nemo_elapsed_wallclock(nemo_simulation_t s, unsigned long* ms)
+{
+	NULLCHECK(s);
+	NULLCHECK(ms);
+	CALL(*ms = S(s).elapsedWallclock());
+}
+
+nemo_status_t nemo_elapsed_simulation(nemo_simulation_t s, unsigned long* ms)
+{
+	NULLCHECK(s);
+	NULLCHECK(ms);
+	CALL(*ms = S(s).elapsedSimulation());
+}
+
+nemo_status_t nemo_reset_timer(nemo_simulation_t s)
+{
+	NULLCHECK(s);
+	CALL(S(s).resetTimer());
+}
+
+nemo_status_t nemo_b200_get_weights_fx(nemo_simulation_t s, int32_t out[], size_t cap, size_t* len)
+{
+	NULLCHECK(s);
+	NULLCHECK(len);
+	CALL(S(s).getWeightsFx(out, cap, len));
+}
+
+nemo_status_t nemo_b200_get_type_state(nemo_simulation_t s, unsigned type, float out[], size_t cap, size_t* len)
+{
+	NULLCHECK(s);
+	NULLCHECK(len);
+	CALL(S(s).getTypeState(type, out, cap, len));
+}
+
+nemo_status_t nemo_b200_synapse_count(nemo_simulation_t s, uint64_t* count)
+{
+	NULLCHECK(s);
+	NULLCHECK(count);
+	CALL(*count = S(s).synapseCount());
+}
+
+nemo_status_t nemo_b200_last_run_timing(nemo_simulation_t s, float* runMs, float* kernelMs, unsigned* launches)
+{
+	NULLCHECK(s);
+	CALL({
+		if(runMs) *runMs = S(s).lastRunMs;
+		if(kernelMs) *kernelMs = S(s).lastStepKernelMs;
+		if(launches) *launches = S(s).lastStepLaunches;
+	});
+}
+
+unsigned nemo_b200_neuron_type_count(void) { return 4; }
+
+const char* nemo_b200_neuron_type_name(unsigned i) { return i < 4 ? NEURON_TYPES[i].name : ""; }
+
+nemo_status_t nemo_b200_libm_calibration(uint64_t* logFlips, uint64_t* sinFlips, uint64_t* exceptions)
+{
+	CALL({
+		const CalibTables& t = libm_calibration();
+		if(logFlips) *logFlips = t.logFlips;
+		if(sinFlips) *sinFlips = t.sinFlips;
+		if(exceptions) *exceptions = t.excKey.size();
+	});
+}
+
+float nemo_b200_host_nrand(unsigned state[4])
+{
+	LibmCalib c = host_calib_view();
+	return nb_nrand(c, state[0], state[1], state[2], state[3]);
+}
+
+} // extern "C"

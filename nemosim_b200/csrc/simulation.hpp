@@ -1,0 +1,163 @@
+// simulation.hpp -- the B200 simulation backend (replaces the reference's
+// cuda::Simulation, src/nemo/cuda/Simulation.cpp, and reproduces the
+// results of its CPU backend, src/nemo/cpu/Simulation.cpp, bit for bit).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <chrono>
+#include <unordered_map>
+#include <vector>
+
+#include "network.hpp"
+#include "nemo_libm.cuh"
+
+namespace nemo_b200 {
+
+constexpr unsigned MAX_TYPES = 8;
+constexpr unsigned STEP_THREADS = 256;
+
+struct TypeRange {
+	int kind;
+	uint32_t base, n;
+	const float* param;  // [nparam][n]
+	float* state;        // [nstate][n]
+};
+
+// STDP process in fixed point (src/nemo/StdpProcess.cpp:20-46)
+struct StdpParams {
+	int32_t fnPre[MAX_HISTORY];
+	int32_t fnPost[MAX_HISTORY];
+	uint64_t potBits, depBits, prePostBits, postPreBits, postFireMask;
+	uint32_t npre, npost;
+	int32_t minE, maxE, minI, maxI;
+};
+
+// Everything a kernel needs, passed by value.  Neuron arrays use the
+// backend-local index: type order, then insertion order
+// (src/nemo/cpu/Simulation.cpp:58-73).
+struct DevSim {
+	uint32_t N;       // neurons
+	uint32_t W;       // 32-bit words per neuron bit-vector
+	uint32_t ntypes;
+	uint32_t D;       // accumulator slots (max delay + 1); 0 = nothing is ever delivered
+	uint32_t R;       // firing ring length (steps)
+	TypeRange types[MAX_TYPES];
+	uint32_t* rng;            // [4][N] xorshift words
+	uint64_t* hist;           // [2][N] firing history, double-buffered by step parity
+	uint32_t* fstim;          // [W] pending firing stimulus
+	float* curExt;            // [N] pending current stimulus
+	longlong2* slots;         // [D][N] (E, I) fixed-point sums per delivery step
+	const unsigned long long* outPtr; // [N+1] outgoing synapses per source
+	uint2* syn;               // [S] {target | (delay - 1) << 26, weight}
+	uint32_t* firedRing;      // [R][W] fired bit-vector per step
+	uint32_t* firedCount;     // [R]
+	unsigned long long* eventCount; // [R] synaptic events (out-degree of fired neurons)
+	int stdp;
+	const unsigned long long* rcmPtr; // [N+1] incoming plastic synapses per target
+	const uint32_t* rcmSrc;   // source | (delay - 1) << 26
+	const uint32_t* rcmFwd;   // index into syn
+	int32_t* rcmAcc;          // STDP accumulator per incoming plastic synapse
+	StdpParams sp;
+	LibmCalib calib;
+};
+
+class Simulation {
+public:
+	Simulation(const Network& net, const Configuration& conf);
+	~Simulation();
+
+	const std::vector<unsigned>& step(const unsigned* fstim, size_t nf,
+			const unsigned* inidx, const float* icur, size_t ni);
+	void applyStdp(float reward);
+	void run(unsigned steps, unsigned stdpPeriod, float reward, unsigned* counts,
+			uint64_t* events, unsigned* ids, size_t cap, size_t* len);
+
+	float getNeuronState(unsigned g, unsigned var);
+	float getNeuronParameter(unsigned g, unsigned p);
+	float getMembranePotential(unsigned g);
+	void setNeuron(unsigned g, unsigned nargs, const float* args);
+	void setNeuronState(unsigned g, unsigned var, float v);
+	void setNeuronParameter(unsigned g, unsigned p, float v);
+
+	const std::vector<uint64_t>& getSynapsesFrom(unsigned source);
+	unsigned getSynapseTarget(uint64_t id);
+	unsigned getSynapseDelay(uint64_t id);
+	float getSynapseWeight(uint64_t id);
+	unsigned char getSynapsePlastic(uint64_t id);
+
+	void getWeightsFx(int32_t* out, size_t cap, size_t* len);
+	void getTypeState(unsigned netType, float* out, size_t cap, size_t* len);
+	uint64_t synapseCount() const { return m_nsyn; }
+
+	unsigned long elapsedWallclock() const;
+	unsigned long elapsedSimulation() const { return m_timerSteps; }
+	void resetTimer();
+
+	float lastRunMs = 0, lastStepKernelMs = 0;
+	unsigned lastStepLaunches = 0;
+
+private:
+	struct HostType {
+		const NeuronTypeDesc* desc;
+		unsigned netType;
+		unsigned base, n;
+		float* dParam = nullptr;
+		float* dState = nullptr;
+	};
+
+	unsigned localIdx(unsigned g) const;
+	void locate(unsigned g, const HostType** t, unsigned* i) const;
+	size_t synapseKey(uint64_t id) const;
+	void launchStep(bool fullRecord);
+	void flushStdp();
+	void applyStdpDevice(int32_t fxReward);
+	void sync();
+
+	int m_device = 0;
+	cudaStream_t m_stream = nullptr;
+	DevSim m_dev;
+	unsigned m_N = 0;
+	uint64_t m_nsyn = 0;
+	unsigned m_maxDelay = 0;
+	std::vector<HostType> m_types;
+	std::vector<unsigned> m_l2g;
+	std::vector<uint8_t> m_ltype;
+	std::unordered_map<unsigned, unsigned> m_g2l;
+
+	// synapse bookkeeping for queries: for local source l, the synapse with
+	// per-source index i is m_srcOrder[m_srcStart[l] + i] (an insertion-order
+	// position k); its device slot is m_pos[k]
+	bool m_writeOnly = false;
+	std::vector<uint64_t> m_srcStart;
+	std::vector<uint64_t> m_srcOrder;
+	std::vector<uint64_t> m_pos;
+	std::vector<unsigned> m_synDelay;  // by insertion order
+	std::vector<uint8_t> m_synPlastic; // by insertion order
+	std::vector<unsigned> m_synTarget; // global target, by insertion order
+	std::vector<uint64_t> m_queried;
+
+	// step state
+	uint64_t m_cycle = 0;        // steps since creation (never reset)
+	bool m_stdpPending = false;  // STDP accumulation of step m_cycle-1 not yet run
+	unsigned long m_timerSteps = 0;
+	std::chrono::steady_clock::time_point m_timerStart;
+
+	// host staging
+	uint32_t* m_hFired = nullptr;  // pinned, [R][W]
+	uint32_t* m_hStim = nullptr;   // pinned stimulus staging
+	uint32_t* m_dStim = nullptr;
+	size_t m_stimCap = 0;
+	std::vector<unsigned> m_fired;
+
+	cudaEvent_t m_ev0 = nullptr, m_ev1 = nullptr;
+	std::vector<void*> m_allocs;
+	template<typename T> T* dalloc(size_t n);
+};
+
+// Device copies of the libm calibration tables (one per device, kept for
+// the life of the process).
+LibmCalib device_calibration(int device);
+
+} // namespace nemo_b200
