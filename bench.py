@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""bench.py -- throughput of the NeMo simulation step on the B200 backend.
+
+Workload: the reference's random Izhikevich network (src/examples/random.cpp,
+synthetic and seeded) at 100,000 neurons x 1000 outgoing synapses (100M
+synapses; 80/20 excitatory/inhibitory; excitatory delays uniform 1-44 ms,
+inhibitory 1 ms; Gaussian input noise sigma 5/2) with STDP on the excitatory
+synapses (20 + 20 ms exponential window, A+ = 0.1, A- = -0.12, tau = 20 ms,
+weights in [0, 10]) and applyStdp(1.0) every 100 ms.  The maximum delay is 44
+rather than 64 because the reference rejects max delay + postfire window > 64
+(src/nemo/StdpFunction.cpp:51-60).
+
+One bench "step" is one STDP period: 100 simulated milliseconds followed by
+applyStdp(1.0).  The metric is synaptic events per second (spike arrivals:
+the sum of the out-degrees of the neurons that fired, as the reference's
+benchmark counts them, src/examples/common.cpp:94-99) and simulated ms per
+wall second.
+
+  value    device-resident run through the native run loop (CUDA events)
+  e2e      the reference-facing C ABI, nemo_step once per ms with host
+           buffers: a one-neuron firing stimulus goes host->device and the
+           fired bit-vector comes back every step (src/examples/common.cpp
+           --fstim), plus nemo_apply_stdp every 100 ms
+  roofline the step kernel's algorithmic bytes per launch / its measured
+           average duration, against the measured HBM copy bandwidth
+  --impl reference  the CPU oracle (a restatement of the reference CPU
+           backend; the reference itself cannot be built here) on the host
+
+Multi-GPU: independent replicas, one per GPU (the path does not shard);
+value = events of all ranks / max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NEURONS = 100_000
+SYNAPSES = 1000
+DMAX = 44
+WINDOW_MS = 100
+METRIC = "synaptic events/s (100k x 1k Izhikevich, STDP)"
+UNIT = "events/s"
+
+# algorithmic bytes (per neuron-step, per fired neuron, per event, per STDP
+# entry) of the step kernel
+B_NEURON = 60 + 16   # Izhikevich u,v r/w, a,b,sigma, RNG r/w + history r/w
+B_FIRED = 8          # c, d on a spike
+B_EVENT = 8          # {target, weight} per delivered synapse
+B_STDP = 12          # {source,delay} + accumulator r/w per walked entry
+B_APPLY = 20         # per plastic synapse per applyStdp
+
+
+def config(args) -> dict:
+    return {
+        "workload": "izhikevich-100k-x1000-stdp",
+        "neurons": args.neurons,
+        "synapses_per_neuron": SYNAPSES,
+        "synapses": args.neurons * SYNAPSES,
+        "max_delay_ms": DMAX,
+        "stdp": "20+20 ms exponential window, A+=0.1, A-=-0.12, weights [0,10], applyStdp(1.0) every 100 ms",
+        "step": f"{WINDOW_MS} simulated ms + applyStdp",
+        "generator": "random::construct (src/examples/random.cpp), mt19937 seed 5489",
+        "cache": "inputs larger than L2: 0.8 GB forward matrix + 1 GB reverse matrix streamed per period",
+        "parallelism": f"replicas x{args.gpus}",
+    }
+
+
+def stdp_conf(mod):
+    conf = mod.Configuration()
+    dt = np.arange(1, 21, dtype=np.float32)
+    pre = (np.float32(0.1) * np.exp(-dt / np.float32(20.0))).astype(np.float32)
+    post = (np.float32(-0.12) * np.exp(-dt / np.float32(20.0))).astype(np.float32)
+    conf.set_stdp_function(pre, post, -10.0, 10.0)
+    return conf
+
+
+def measured_peak_gbs():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["not sampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_sample(neurons: int, warm_ms: int, ms: int, stdp_period: int = WINDOW_MS) -> dict:
+    """Time the oracle (the reference CPU backend restated, OpenMP on the
+    neuron update as in the reference) on the same network."""
+    import oracle as O
+    t0 = time.perf_counter()
+    net = O.example_random(neurons, SYNAPSES, DMAX, True)
+    sim = O.Simulation(net, stdp_conf(O))
+    build_s = time.perf_counter() - t0
+    sim.run(warm_ms, stdp_period, 1.0, max_ids=warm_ms * neurons)
+    t0 = time.perf_counter()
+    counts, _ = sim.run(ms, stdp_period, 1.0, max_ids=ms * neurons)
+    el = time.perf_counter() - t0
+    events = float(counts.sum()) * SYNAPSES
+    return {"events_per_s": events / el, "sim_ms_per_s": ms / el, "seconds": el, "build_s": build_s,
+            "fired": int(counts.sum())}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the oracle on the host cores, same metric/config."""
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    # each bench step is a bounded sample of the 100 ms period so that the
+    # whole run stays within a few minutes
+    per_ms = 0.03 * args.neurons / 100_000  # ~30 ms per simulated ms at 100k on one socket
+    budget = 150.0
+    window = max(5, min(WINDOW_MS, int(budget / max(1, args.steps + args.warmup) / per_ms)))
+    import oracle as O
+    t0 = time.perf_counter()
+    net = O.example_random(args.neurons, SYNAPSES, DMAX, True)
+    sim = O.Simulation(net, stdp_conf(O))
+    build_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        sim.run(window, window, 1.0, max_ids=window * args.neurons)
+    t0 = time.perf_counter()
+    fired = 0
+    for _ in range(args.steps):
+        counts, _ = sim.run(window, window, 1.0, max_ids=window * args.neurons)
+        fired += int(counts.sum())
+    el = time.perf_counter() - t0
+    value = fired * SYNAPSES / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32+f64+int64", "data": "synthetic",
+        "config": config(args),
+        "sim_ms_per_s": args.steps * window / el,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} steps of {window} simulated ms (+applyStdp) after "
+                                   f"{args.warmup} warm-up steps; network build {build_s:.1f} s untimed"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, rank, world, local):
+    import nemosim_b200 as nb
+
+    t0 = time.perf_counter()
+    net = nb.example_random(args.neurons, SYNAPSES, DMAX, True)
+    conf = stdp_conf(nb)
+    conf.set_cuda_backend(local)
+    sim = nb.Simulation(net, conf)
+    del net
+    build_s = time.perf_counter() - t0
+    W = args.window
+
+    # warm-up
+    sim.run(W * args.warmup, W, 1.0, ids=False)
+
+    # timed: K periods, device-resident, CUDA events inside the run loop
+    barrier(world)
+    with ClockSampler(local) as clk:
+        sim.run(W * args.steps, W, 1.0, ids=False)
+    st = sim.run_stats()
+    barrier(world)
+    run_ms = dist_max(st["run_ms"], world)
+    events = dist_sum(float(st["events"]), world)
+    value = events / (run_ms / 1e3)
+    sim_ms_per_s = args.steps * W / (run_ms / 1e3)
+
+    # profiled pass: per-kernel CUDA events for the roofline
+    sim.set_profiling(True)
+    kp = max(1, min(args.steps, 5))
+    sim.run(W * kp, W, 1.0, ids=False)
+    sim.set_profiling(False)
+    ps = sim.run_stats()
+    launches = ps["kernel_launches"]["step"]
+    step_ms = ps["kernel_ms"]["step"] / max(1, launches)
+    alg_bytes = (args.neurons * B_NEURON * launches + ps["fired"] * B_FIRED + ps["events"] * B_EVENT
+                 + ps["stdp_entries"] * B_STDP) / max(1, launches)
+    achieved = alg_bytes / (step_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_gbs()
+    apply_ms = ps["kernel_ms"]["apply"] / max(1, ps["kernel_launches"]["apply"])
+    apply_gbs = ps["plastic_synapses"] * B_APPLY / (apply_ms / 1e3) / 1e9 if apply_ms else None
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            tj = json.load(f)
+        # scale the captured bytes per launch to this run's per-launch work
+        if tj.get("alg_bytes_per_launch"):
+            traffic = tj["dram_bytes_per_launch"] * alg_bytes / tj["alg_bytes_per_launch"]
+
+    # e2e through the C ABI with host buffers
+    rng = np.random.default_rng(rank)
+    ke = max(1, min(args.steps, args.e2e_steps))
+    ev0 = sim.step_events()
+    stim = rng.integers(0, args.neurons, size=ke * W).tolist()
+    barrier(world)
+    t0 = time.perf_counter()
+    k = 0
+    for _ in range(ke):
+        for _ in range(W):
+            sim.step([stim[k]])
+            k += 1
+        sim.apply_stdp(1.0)
+    e2e_s = time.perf_counter() - t0
+    barrier(world)
+    e2e_s = dist_max(e2e_s, world)
+    e2e_events = dist_sum(float(sim.step_events() - ev0), world)
+    words = (args.neurons + 31) // 32
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        c = cpu_sample(args.neurons, args.cpu_warm_ms, args.cpu_ms)
+        cpu = {"value": c["events_per_s"], "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{args.cpu_ms} simulated ms (after {args.cpu_warm_ms} warm-up ms) of the same "
+                         f"network on the oracle; build {c['build_s']:.0f} s untimed",
+               "sim_ms_per_s": c["sim_ms_per_s"]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": run_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32+f64+int64", "data": "synthetic",
+            "config": config(args),
+            "sim_ms_per_s": sim_ms_per_s,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "step_kernel", "alg_bytes_per_launch": alg_bytes,
+                         "avg_launch_us": step_ms * 1e3,
+                         "apply_stdp_kernel": {"avg_launch_us": apply_ms * 1e3, "achieved_gbs": apply_gbs}},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_events / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 4 * W,
+                    "d2h_bytes_per_step": 4 * words * W, "api": "nemo_step + nemo_apply_stdp (C ABI)",
+                    "sim_ms_per_s": ke * W / e2e_s},
+            "gpu_launches": args.steps * (W + 2),
+            "clocks": clk.summary(),
+            "build_s": build_s,
+            "spikes_per_neuron_s": st["fired"] / args.neurons / (args.steps * W / 1e3),
+        }
+        print(json.dumps(line), flush=True)
+    del sim
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--neurons", type=int, default=NEURONS)
+    ap.add_argument("--window", type=int, default=WINDOW_MS, help=argparse.SUPPRESS)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--cpu-ms", type=int, default=200)
+    ap.add_argument("--cpu-warm-ms", type=int, default=50)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("at least 3 warm-up steps")
+    if args.impl == "reference":
+        # the CPU reference needs no process group: rank 0 runs, the others exit
+        rank = int(os.environ.get("RANK", 0))
+        args.gpus = int(os.environ.get("WORLD_SIZE", args.gpus))
+        run_reference(args, rank, 1)
+        return
+    rank, world, local = dist_setup(args)
+    args.gpus = world if world > 1 else args.gpus
+    run_b200(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

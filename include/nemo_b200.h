@@ -250,11 +250,20 @@ NEMO_B200_API nemo_status_t nemo_b200_get_type_state(nemo_simulation_t, unsigned
  * the order of nemo_b200_get_type_state's neurons (type order, then
  * insertion order). */
 NEMO_B200_API nemo_status_t nemo_b200_synapse_count(nemo_simulation_t, uint64_t* count);
-/* Device time (ms, CUDA events) of the last nemo_b200_run, and the summed
- * time of its dominant kernel (the per-step update/scatter kernel) with its
- * launch count. */
-NEMO_B200_API nemo_status_t nemo_b200_last_run_timing(nemo_simulation_t, float* run_ms,
-		float* step_kernel_ms, unsigned* step_kernel_launches);
+/* Turn per-launch CUDA-event timing of nemo_b200_run's kernels on or off. */
+NEMO_B200_API nemo_status_t nemo_b200_set_profiling(nemo_simulation_t, int on);
+/* Statistics of the last nemo_b200_run: its device time in ms (CUDA events
+ * on the simulation's stream), and per kernel kind (0 = step kernel,
+ * 1 = pending STDP accumulation, 2 = applyStdp) the summed device time and
+ * launch count when profiling is on; the spikes, synaptic events and STDP
+ * reverse-matrix entries walked in the run; and the number of plastic
+ * synapses.  Any output pointer may be NULL. */
+NEMO_B200_API nemo_status_t nemo_b200_run_stats(nemo_simulation_t, float* run_ms,
+		float kernel_ms[3], unsigned kernel_launches[3],
+		uint64_t* fired, uint64_t* events, uint64_t* stdp_entries, uint64_t* plastic_synapses);
+/* Synaptic events (sum of the out-degrees of the fired neurons) of all
+ * nemo_step calls on this simulation so far. */
+NEMO_B200_API nemo_status_t nemo_b200_step_events(nemo_simulation_t, uint64_t* events);
 /* Names of the compiled-in neuron types, one per call (index < count). */
 NEMO_B200_API unsigned nemo_b200_neuron_type_count(void);
 NEMO_B200_API const char* nemo_b200_neuron_type_name(unsigned i);
@@ -263,6 +272,10 @@ NEMO_B200_API const char* nemo_b200_neuron_type_name(unsigned i);
  * evaluation rounds differently from the host libm, for logf and sinf. */
 NEMO_B200_API nemo_status_t nemo_b200_libm_calibration(uint64_t* log_flips, uint64_t* sin_flips,
 		uint64_t* exceptions);
+/* Status of the most recent call, including the constructors
+ * (nemo_new_simulation and the like) that report failure only by returning
+ * NULL. */
+NEMO_B200_API nemo_status_t nemo_b200_last_status(void);
 /* Host build of the device's glibc-exact nrand (for tests): advances the
  * xorshift state in place and returns the normal deviate. */
 NEMO_B200_API float nemo_b200_host_nrand(unsigned state[4]);

@@ -206,7 +206,7 @@ class Simulation:
     def __init__(self, net: Network, conf: Configuration):
         h = lib().nemo_new_simulation(net._h, conf._h)
         if not h:
-            raise NemoError(NEMO_INVALID_INPUT, lib().nemo_strerror().decode())
+            raise NemoError(lib().nemo_b200_last_status(), lib().nemo_strerror().decode())
         self._h = h
 
     def __del__(self):
@@ -325,10 +325,30 @@ class Simulation:
         _check(lib().nemo_b200_synapse_count(self._h, C.byref(v)))
         return v.value
 
-    def last_run_timing(self):
-        a, b, c = C.c_float(), C.c_float(), C.c_uint()
-        _check(lib().nemo_b200_last_run_timing(self._h, C.byref(a), C.byref(b), C.byref(c)))
-        return a.value, b.value, c.value
+    def set_profiling(self, on: bool = True):
+        _check(lib().nemo_b200_set_profiling(self._h, int(on)))
+
+    def run_stats(self) -> dict:
+        """Statistics of the last run() (an extension): device ms, per-kernel
+        ms and launches (when profiling), spikes, events, STDP entries walked
+        and the number of plastic synapses."""
+        run_ms = C.c_float()
+        kms = (C.c_float * 3)()
+        kl = (C.c_uint * 3)()
+        vals = [C.c_uint64() for _ in range(4)]
+        _check(lib().nemo_b200_run_stats(self._h, C.byref(run_ms), kms, kl, *[C.byref(v) for v in vals]))
+        names = ("step", "stdp", "apply")
+        return {"run_ms": run_ms.value,
+                "kernel_ms": {n: kms[i] for i, n in enumerate(names)},
+                "kernel_launches": {n: kl[i] for i, n in enumerate(names)},
+                "fired": vals[0].value, "events": vals[1].value,
+                "stdp_entries": vals[2].value, "plastic_synapses": vals[3].value}
+
+    def step_events(self) -> int:
+        """Synaptic events of all step() calls so far (an extension)."""
+        v = C.c_uint64()
+        _check(lib().nemo_b200_step_events(self._h, C.byref(v)))
+        return v.value
 
     def elapsed_wallclock(self):
         v = C.c_ulong()

@@ -91,10 +91,13 @@ SIGNATURES = {
     "nemo_b200_get_weights_fx": (st, [vp, i32p, sz, C.POINTER(sz)]),
     "nemo_b200_get_type_state": (st, [vp, C.c_uint, f32p, sz, C.POINTER(sz)]),
     "nemo_b200_synapse_count": (st, [vp, C.POINTER(C.c_uint64)]),
-    "nemo_b200_last_run_timing": (st, [vp, PF, PF, PU]),
+    "nemo_b200_set_profiling": (st, [vp, C.c_int]),
+    "nemo_b200_run_stats": (st, [vp, PF, PF, PU] + [C.POINTER(C.c_uint64)] * 4),
+    "nemo_b200_step_events": (st, [vp, C.POINTER(C.c_uint64)]),
     "nemo_b200_neuron_type_count": (C.c_uint, []),
     "nemo_b200_neuron_type_name": (C.c_char_p, [C.c_uint]),
     "nemo_b200_libm_calibration": (st, [C.POINTER(C.c_uint64)] * 3),
+    "nemo_b200_last_status": (st, []),
     "nemo_b200_host_nrand": (C.c_float, [u32p]),
 }
 

@@ -28,19 +28,24 @@ struct Mt19937 {
 		idx = 624;
 	}
 	uint32_t operator()() {
-		if(idx >= 624) {
-			for(int k = 0; k < 624; ++k) {
-				uint32_t y = (mt[k] & 0x80000000u) | (mt[(k + 1) % 624] & 0x7fffffffu);
-				mt[k] = mt[(k + 397) % 624] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
-			}
-			idx = 0;
-		}
+		if(idx >= 624) twist();
 		uint32_t y = mt[idx++];
 		y ^= (y >> 11);
 		y ^= (y << 7) & 0x9d2c5680u;
 		y ^= (y << 15) & 0xefc60000u;
 		y ^= (y >> 18);
 		return y;
+	}
+	void twist() {
+		auto mix = [](uint32_t a, uint32_t b, uint32_t c) {
+			uint32_t y = (a & 0x80000000u) | (b & 0x7fffffffu);
+			return c ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+		};
+		int k = 0;
+		for(; k < 624 - 397; ++k) mt[k] = mix(mt[k], mt[k + 1], mt[k + 397]);
+		for(; k < 623; ++k) mt[k] = mix(mt[k], mt[k + 1], mt[k + 397 - 624]);
+		mt[623] = mix(mt[623], mt[0], mt[396]);
+		idx = 0;
 	}
 };
 
@@ -73,12 +78,13 @@ extern "C" nemo_status_t nemo_b200_example_random(nemo_network_t* out, unsigned 
 	std::vector<unsigned> src(scount), tgt(scount), dly(scount);
 	std::vector<float> w(scount);
 	std::vector<unsigned char> pl(scount);
-	net->net.src.reserve((size_t) ncount * scount);
-	net->net.tgt.reserve((size_t) ncount * scount);
-	net->net.delay.reserve((size_t) ncount * scount);
-	net->net.weight.reserve((size_t) ncount * scount);
-	net->net.plastic.reserve((size_t) ncount * scount);
-	net->net.sid.reserve((size_t) ncount * scount);
+	const size_t total = (size_t) ncount * scount;
+	net->net.src.reserve(total);
+	net->net.tgt.reserve(total);
+	net->net.delay.reserve(total);
+	net->net.weight.reserve(total);
+	net->net.plastic.reserve(total);
+	net->net.sid.reserve(total);
 	for(unsigned nidx = 0; nidx < ncount && r == NEMO_OK; ++nidx) {
 		const float v = -65.0f;
 		const bool exc = nidx < (ncount * 4) / 5;

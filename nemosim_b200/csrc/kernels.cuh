@@ -174,7 +174,8 @@ __device__ __forceinline__ bool update_poisson(const DevSim& S, const TypeRange&
 // Walk the incoming plastic synapses of `tgt` and accumulate their STDP
 // weight change (ConnectivityMatrix::accumulateStdp,
 // src/nemo/ConnectivityMatrix.cpp:193-227).  Called by a whole warp.
-__device__ __forceinline__ void stdp_accumulate_target(const DevSim& S, uint32_t tgt, const uint64_t* histPrev, uint32_t lane)
+__device__ __forceinline__ unsigned long long stdp_accumulate_target(const DevSim& S, uint32_t tgt,
+		const uint64_t* histPrev, uint32_t lane)
 {
 	unsigned long long b = S.rcmPtr[tgt], e = S.rcmPtr[tgt + 1];
 	for(unsigned long long p = b + lane; p < e; p += 32) {
@@ -185,6 +186,7 @@ __device__ __forceinline__ void stdp_accumulate_target(const DevSim& S, uint32_t
 		int32_t dw = stdp_weight_change(S.sp, pre);
 		if(dw != 0) S.rcmAcc[p] = (int32_t) ((uint32_t) S.rcmAcc[p] + (uint32_t) dw);
 	}
+	return e - b;
 }
 
 } // namespace nemo_b200

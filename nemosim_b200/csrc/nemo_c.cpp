@@ -545,14 +545,35 @@ nemo_status_t nemo_b200_synapse_count(nemo_simulation_t s, uint64_t* count)
 	CALL(*count = S(s).synapseCount());
 }
 
-nemo_status_t nemo_b200_last_run_timing(nemo_simulation_t s, float* runMs, float* kernelMs, unsigned* launches)
+nemo_status_t nemo_b200_set_profiling(nemo_simulation_t s, int on)
+{
+	NULLCHECK(s);
+	CALL(S(s).profiling = on != 0);
+}
+
+nemo_status_t nemo_b200_run_stats(nemo_simulation_t s, float* runMs, float kernelMs[3], unsigned launches[3],
+		uint64_t* fired, uint64_t* events, uint64_t* stdpEntries, uint64_t* plastic)
 {
 	NULLCHECK(s);
 	CALL({
-		if(runMs) *runMs = S(s).lastRunMs;
-		if(kernelMs) *kernelMs = S(s).lastStepKernelMs;
-		if(launches) *launches = S(s).lastStepLaunches;
+		Simulation& sim = S(s);
+		if(runMs) *runMs = sim.lastRunMs;
+		for(int k = 0; k < 3; ++k) {
+			if(kernelMs) kernelMs[k] = sim.kernelMs[k];
+			if(launches) launches[k] = sim.kernelLaunches[k];
+		}
+		if(fired) *fired = sim.lastFired;
+		if(events) *events = sim.lastEvents;
+		if(stdpEntries) *stdpEntries = sim.lastStdpEntries;
+		if(plastic) *plastic = sim.lastPlastic;
 	});
+}
+
+nemo_status_t nemo_b200_step_events(nemo_simulation_t s, uint64_t* events)
+{
+	NULLCHECK(s);
+	NULLCHECK(events);
+	CALL(*events = S(s).stepEvents);
 }
 
 unsigned nemo_b200_neuron_type_count(void) { return 4; }
@@ -568,6 +589,8 @@ nemo_status_t nemo_b200_libm_calibration(uint64_t* logFlips, uint64_t* sinFlips,
 		if(exceptions) *exceptions = t.excKey.size();
 	});
 }
+
+nemo_status_t nemo_b200_last_status(void) { return g_lastStatus; }
 
 float nemo_b200_host_nrand(unsigned state[4])
 {

@@ -5,6 +5,8 @@
 #include <stdio.h>
 #include <stdlib.h>
 
+#include <algorithm>
+
 namespace nemo_b200 {
 
 std::string format(const char* fmt, ...)
@@ -72,8 +74,10 @@ void Network::addNeurons(unsigned type, size_t n, const unsigned* idx, unsigned 
 		NB_THROW(NEMO_INVALID_INPUT,
 				"Unexpected number of parameters/state variables when adding neuron. Expected %u, found %u", na, nargs);
 	}
-	c.gidx.reserve(c.gidx.size() + n);
-	c.args.reserve(c.args.size() + n * na);
+	if(c.gidx.size() + n > c.gidx.capacity()) {
+		c.gidx.reserve(std::max(c.gidx.size() + n, 2 * c.gidx.capacity()));
+		c.args.reserve(std::max(c.args.size() + n * na, 2 * c.args.capacity()));
+	}
 	for(size_t i = 0; i < n; ++i) {
 		c.gidx.push_back(idx[i]);
 		c.args.insert(c.args.end(), args + i * na, args + (i + 1) * na);
@@ -91,10 +95,23 @@ void Network::addSynapses(size_t n, const unsigned* s, const unsigned* t, const 
 		const float* w, const unsigned char* p, uint64_t* ids)
 {
 	m_synIndexValid = false;
+	const size_t base = src.size();
+	const size_t need = base + n;
+	if(need > src.capacity()) {
+		size_t cap = std::max(need, src.capacity() * 2);
+		src.reserve(cap); tgt.reserve(cap); delay.reserve(cap);
+		weight.reserve(cap); plastic.reserve(cap); sid.reserve(cap);
+	}
+	src.resize(need); tgt.resize(need); delay.resize(need);
+	weight.resize(need); plastic.resize(need); sid.resize(need);
 	unsigned lastSrc = 0;
 	uint32_t* lastCount = nullptr;
 	for(size_t i = 0; i < n; ++i) {
 		if(d[i] < 1) {
+			// roll back this call's partial additions
+			for(size_t j = 0; j < i; ++j) axonCount[s[j]]--;
+			src.resize(base); tgt.resize(base); delay.resize(base);
+			weight.resize(base); plastic.resize(base); sid.resize(base);
 			NB_THROW(NEMO_INVALID_INPUT, "Invalid delay (%u) for synapse between %u and %u", d[i], s[i], t[i]);
 		}
 		if(!lastCount || s[i] != lastSrc) {
@@ -102,12 +119,13 @@ void Network::addSynapses(size_t n, const unsigned* s, const unsigned* t, const 
 			lastCount = &axonCount[s[i]];
 		}
 		uint32_t id = (*lastCount)++;
-		src.push_back(s[i]);
-		tgt.push_back(t[i]);
-		delay.push_back(d[i]);
-		weight.push_back(w[i]);
-		plastic.push_back(p[i] != 0);
-		sid.push_back(id);
+		const size_t k = base + i;
+		src[k] = s[i];
+		tgt[k] = t[i];
+		delay[k] = d[i];
+		weight[k] = w[i];
+		plastic[k] = p[i] != 0;
+		sid[k] = id;
 		if(d[i] > maxDelay) maxDelay = d[i];
 		if(ids) ids[i] = ((uint64_t) s[i] << 32) | id;
 	}

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "common.hpp"
+#include "hugevec.hpp"
 
 namespace nemo_b200 {
 
@@ -47,10 +48,10 @@ public:
 	std::unordered_map<unsigned, uint64_t> neurons;  // gidx -> (type << 32) | index
 	std::unordered_map<unsigned, uint32_t> axonCount; // source gidx -> number of synapses
 	// synapses in insertion order
-	std::vector<unsigned> src, tgt, delay;
-	std::vector<float> weight;
-	std::vector<uint8_t> plastic;
-	std::vector<uint32_t> sid;  // per-source synapse index
+	hvector<unsigned> src, tgt, delay;
+	hvector<float> weight;
+	hvector<uint8_t> plastic;
+	hvector<uint32_t> sid;  // per-source synapse index
 	unsigned maxDelay = 0;
 	bool duplicate = false;
 	unsigned duplicateIdx = 0;

@@ -31,7 +31,7 @@ step_kernel(const DevSim S, uint32_t cur, uint32_t slot, uint32_t ring, int stdp
 	__shared__ uint32_t sFired[STEP_THREADS];
 	__shared__ uint32_t sStdp[STEP_THREADS];
 	__shared__ uint32_t sNF, sNS;
-	__shared__ unsigned long long sEvents;
+	__shared__ unsigned long long sEvents, sStdpWalk;
 
 	const uint32_t tid = threadIdx.x;
 	const uint32_t lane = tid & 31, warp = tid >> 5;
@@ -40,7 +40,7 @@ step_kernel(const DevSim S, uint32_t cur, uint32_t slot, uint32_t ring, int stdp
 	const uint64_t* histPrev = S.hist + (size_t) prev * S.N;
 	uint64_t* histCur = S.hist + (size_t) cur * S.N;
 
-	if(tid == 0) { sNF = 0; sNS = 0; sEvents = 0; }
+	if(tid == 0) { sNF = 0; sNS = 0; sEvents = 0; sStdpWalk = 0; }
 	__syncthreads();
 
 	bool fired = false, stdpTarget = false;
@@ -140,20 +140,23 @@ step_kernel(const DevSim S, uint32_t cur, uint32_t slot, uint32_t ring, int stdp
 	if(lane == 0 && events) atomicAdd(&sEvents, events);
 
 	// 5. STDP accumulation of the previous step
+	unsigned long long walked = 0;
 	for(uint32_t i = warp; i < ns; i += WARPS) {
-		stdp_accumulate_target(S, sStdp[i], histPrev, lane);
+		walked += stdp_accumulate_target(S, sStdp[i], histPrev, lane);
 	}
+	if(lane == 0 && walked) atomicAdd(&sStdpWalk, walked);
 
 	__syncthreads();
 	if(tid == 0) {
 		if(nf) atomicAdd(&S.firedCount[ring], nf);
 		if(sEvents) atomicAdd(&S.eventCount[ring], sEvents);
+		if(sStdpWalk) atomicAdd(&S.stdpCount[ring], sStdpWalk);
 	}
 }
 
 // Pending STDP accumulation of the last completed step (history buffer `par`)
 __global__ void __launch_bounds__(STEP_THREADS)
-stdp_kernel(const DevSim S, uint32_t par)
+stdp_kernel(const DevSim S, uint32_t par, uint32_t ring)
 {
 	__shared__ uint32_t sStdp[STEP_THREADS];
 	__shared__ uint32_t sNS;
@@ -171,9 +174,11 @@ stdp_kernel(const DevSim S, uint32_t par)
 		if(target) sStdp[base + __popc(sb & ((1u << lane) - 1u))] = n;
 	}
 	__syncthreads();
+	unsigned long long walked = 0;
 	for(uint32_t i = warp; i < sNS; i += STEP_THREADS / 32) {
-		stdp_accumulate_target(S, sStdp[i], hist, lane);
+		walked += stdp_accumulate_target(S, sStdp[i], hist, lane);
 	}
+	if(lane == 0 && walked) atomicAdd(&S.stdpCount[ring], walked);
 }
 
 // applyStdp (src/nemo/ConnectivityMatrix.cpp:241-294): one warp per target,
@@ -425,6 +430,8 @@ Simulation::Simulation(const Network& net, const Configuration& conf)
 	}
 	std::vector<unsigned long long> outPtr(N + 1);
 	for(unsigned s = 0; s <= N; ++s) outPtr[s] = rowStart[(size_t) s * D];
+	m_outDegree.resize(N);
+	for(unsigned s = 0; s < N; ++s) m_outDegree[s] = (uint32_t) (outPtr[s + 1] - outPtr[s]);
 	std::vector<uint2> syn(Sn);
 	for(size_t k = 0; k < Sn; ++k) {
 		syn[m_pos[k]] = make_uint2(ltgt[k] | ((net.delay[k] - 1) << 26), (uint32_t) fxw[k]);
@@ -500,6 +507,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf)
 		NB_CUDA(cudaMemcpyAsync(dRfwd, rfwd.data(), P * 4, cudaMemcpyHostToDevice, m_stream));
 		S.rcmSrc = dRsrc;
 		S.rcmFwd = dRfwd;
+		lastPlastic = P;
 		NB_CUDA(cudaStreamSynchronize(m_stream));
 	}
 	auto* dRcmPtr = dalloc<unsigned long long>(N + 1);
@@ -524,6 +532,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf)
 	S.firedRing = dalloc<uint32_t>((size_t) S.R * S.W);
 	S.firedCount = dalloc<uint32_t>(S.R);
 	S.eventCount = dalloc<unsigned long long>(S.R);
+	S.stdpCount = dalloc<unsigned long long>(S.R);
 	NB_CUDA(cudaMallocHost(&m_hFired, (size_t) S.R * S.W * 4));
 
 	if(needCalib) S.calib = device_calibration(m_device);
@@ -541,6 +550,7 @@ Simulation::~Simulation()
 	if(m_dStim) cudaFree(m_dStim);
 	if(m_ev0) cudaEventDestroy(m_ev0);
 	if(m_ev1) cudaEventDestroy(m_ev1);
+	for(cudaEvent_t e : m_evPool) cudaEventDestroy(e);
 	if(m_stream) cudaStreamDestroy(m_stream);
 }
 
@@ -563,13 +573,34 @@ void Simulation::locate(unsigned g, const HostType** t, unsigned* i) const
 	*i = l - (*t)->base;
 }
 
+void Simulation::timedBegin(int kind)
+{
+	if(!profiling || !m_inRun) return;
+	if(m_evNext + 2 > m_evPool.size()) {
+		size_t old = m_evPool.size();
+		m_evPool.resize(std::max<size_t>(64, old * 2));
+		for(size_t i = old; i < m_evPool.size(); ++i) NB_CUDA(cudaEventCreate(&m_evPool[i]));
+	}
+	m_evUse.emplace_back(kind, m_evNext);
+	NB_CUDA(cudaEventRecord(m_evPool[m_evNext], m_stream));
+	m_evNext += 2;
+}
+
+void Simulation::timedEnd()
+{
+	if(!profiling || !m_inRun) return;
+	NB_CUDA(cudaEventRecord(m_evPool[m_evUse.back().second + 1], m_stream));
+}
+
 void Simulation::launchStep(bool /*fullRecord*/)
 {
 	const uint32_t cur = (uint32_t) (m_cycle & 1);
 	const uint32_t slot = m_dev.D ? (uint32_t) (m_cycle % m_dev.D) : 0;
 	const uint32_t ring = (uint32_t) (m_cycle % m_dev.R);
 	const unsigned grid = (m_N + STEP_THREADS - 1) / STEP_THREADS;
+	timedBegin(K_STEP);
 	step_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, cur, slot, ring, m_stdpPending ? 1 : 0);
+	timedEnd();
 	m_stdpPending = m_dev.stdp != 0;
 	m_cycle++;
 	m_timerSteps++;
@@ -628,7 +659,9 @@ const std::vector<unsigned>& Simulation::step(const unsigned* fstim, size_t nf,
 		while(bits) {
 			uint32_t b = __builtin_ctz(bits);
 			bits &= bits - 1;
-			m_fired.push_back(m_l2g[w * 32 + b]);
+			const uint32_t l = w * 32 + b;
+			m_fired.push_back(m_l2g[l]);
+			stepEvents += m_outDegree[l];
 		}
 	}
 	return m_fired;
@@ -639,7 +672,9 @@ void Simulation::flushStdp()
 	if(!m_stdpPending) return;
 	const uint32_t par = (uint32_t) ((m_cycle - 1) & 1);
 	const unsigned grid = (m_N + STEP_THREADS - 1) / STEP_THREADS;
-	stdp_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, par);
+	timedBegin(K_STDP);
+	stdp_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, par, (uint32_t) ((m_cycle - 1) % m_dev.R));
+	timedEnd();
 	m_stdpPending = false;
 }
 
@@ -654,7 +689,9 @@ void Simulation::applyStdpDevice(int32_t R)
 	int sms = 148;
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m_device);
 	unsigned grid = std::min<unsigned>((m_N + 7) / 8, (unsigned) sms * 8);
+	timedBegin(K_APPLY);
 	apply_stdp_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, R, par, slot);
+	timedEnd();
 }
 
 /* ConnectivityMatrix::applyStdp argument checks (src/nemo/ConnectivityMatrix.cpp:241-259) */
@@ -683,26 +720,35 @@ void Simulation::run(unsigned steps, unsigned stdpPeriod, float reward, unsigned
 		if(R == 0 && reward != 0) NB_THROW(NEMO_INVALID_INPUT, "STDP reward rounded down to zero");
 	}
 	size_t total = 0;
-	float runMs = 0, kernelMs = 0;
-	unsigned launches = 0;
+	float runMs = 0;
+	for(int k = 0; k < K_KINDS; ++k) { kernelMs[k] = 0; kernelLaunches[k] = 0; }
+	lastFired = lastEvents = lastStdpEntries = 0;
 	unsigned done = 0;
+	struct InRun {
+		bool& f;
+		explicit InRun(bool& x) : f(x) { f = true; }
+		~InRun() { f = false; }
+	} inRun(m_inRun);
 	while(done < steps) {
 		const uint64_t first = m_cycle;
 		const unsigned chunk = std::min<unsigned>(steps - done, m_dev.R);
 		// the ring positions this chunk uses start at first % R and may wrap
 		NB_CUDA(cudaMemsetAsync(m_dev.firedCount, 0, m_dev.R * 4, m_stream));
 		NB_CUDA(cudaMemsetAsync(m_dev.eventCount, 0, m_dev.R * 8, m_stream));
+		NB_CUDA(cudaMemsetAsync(m_dev.stdpCount, 0, m_dev.R * 8, m_stream));
+		m_evUse.clear();
+		m_evNext = 0;
 		NB_CUDA(cudaEventRecord(m_ev0, m_stream));
 		for(unsigned i = 0; i < chunk; ++i) {
 			launchStep(false);
-			launches++;
 			if(stdpPeriod && (done + i + 1) % stdpPeriod == 0) applyStdpDevice(R);
 		}
 		NB_CUDA(cudaEventRecord(m_ev1, m_stream));
 		std::vector<uint32_t> hc(m_dev.R);
-		std::vector<unsigned long long> he(m_dev.R);
+		std::vector<unsigned long long> he(m_dev.R), hs(m_dev.R);
 		NB_CUDA(cudaMemcpyAsync(hc.data(), m_dev.firedCount, m_dev.R * 4, cudaMemcpyDeviceToHost, m_stream));
 		NB_CUDA(cudaMemcpyAsync(he.data(), m_dev.eventCount, m_dev.R * 8, cudaMemcpyDeviceToHost, m_stream));
+		NB_CUDA(cudaMemcpyAsync(hs.data(), m_dev.stdpCount, m_dev.R * 8, cudaMemcpyDeviceToHost, m_stream));
 		if(ids) {
 			NB_CUDA(cudaMemcpyAsync(m_hFired, m_dev.firedRing, (size_t) m_dev.R * m_dev.W * 4,
 					cudaMemcpyDeviceToHost, m_stream));
@@ -712,10 +758,21 @@ void Simulation::run(unsigned steps, unsigned stdpPeriod, float reward, unsigned
 		float ms = 0;
 		NB_CUDA(cudaEventElapsedTime(&ms, m_ev0, m_ev1));
 		runMs += ms;
+		for(const auto& u : m_evUse) {
+			float km = 0;
+			NB_CUDA(cudaEventElapsedTime(&km, m_evPool[u.second], m_evPool[u.second + 1]));
+			kernelMs[u.first] += km;
+			kernelLaunches[u.first]++;
+		}
+		m_evUse.clear();
+		m_evNext = 0;
+		for(uint32_t r = 0; r < m_dev.R; ++r) lastStdpEntries += hs[r];
 		for(unsigned i = 0; i < chunk; ++i) {
 			uint32_t r = (uint32_t) ((first + i) % m_dev.R);
 			if(counts) counts[done + i] = hc[r];
 			if(events) events[done + i] = he[r];
+			lastFired += hc[r];
+			lastEvents += he[r];
 			if(ids) {
 				const uint32_t* words = m_hFired + (size_t) r * m_dev.W;
 				for(uint32_t w = 0; w < m_dev.W; ++w) {
@@ -735,8 +792,6 @@ void Simulation::run(unsigned steps, unsigned stdpPeriod, float reward, unsigned
 	}
 	if(len) *len = total;
 	lastRunMs = runMs;
-	lastStepKernelMs = kernelMs;
-	lastStepLaunches = launches;
 }
 
 float Simulation::getNeuronState(unsigned g, unsigned var)

@@ -54,6 +54,7 @@ struct DevSim {
 	uint32_t* firedRing;      // [R][W] fired bit-vector per step
 	uint32_t* firedCount;     // [R]
 	unsigned long long* eventCount; // [R] synaptic events (out-degree of fired neurons)
+	unsigned long long* stdpCount;  // [R] incoming plastic synapses walked by STDP
 	int stdp;
 	const unsigned long long* rcmPtr; // [N+1] incoming plastic synapses per target
 	const uint32_t* rcmSrc;   // source | (delay - 1) << 26
@@ -95,8 +96,15 @@ public:
 	unsigned long elapsedSimulation() const { return m_timerSteps; }
 	void resetTimer();
 
-	float lastRunMs = 0, lastStepKernelMs = 0;
-	unsigned lastStepLaunches = 0;
+	// timing of the last run(): whole run and, when profiling is on, each
+	// kernel kind (CUDA events around every launch)
+	enum { K_STEP = 0, K_STDP = 1, K_APPLY = 2, K_KINDS = 3 };
+	float lastRunMs = 0;
+	float kernelMs[K_KINDS] = {0, 0, 0};
+	unsigned kernelLaunches[K_KINDS] = {0, 0, 0};
+	uint64_t lastFired = 0, lastEvents = 0, lastStdpEntries = 0, lastPlastic = 0;
+	bool profiling = false;
+	uint64_t stepEvents = 0;  // synaptic events of all step() calls so far
 
 private:
 	struct HostType {
@@ -150,8 +158,15 @@ private:
 	uint32_t* m_dStim = nullptr;
 	size_t m_stimCap = 0;
 	std::vector<unsigned> m_fired;
+	std::vector<uint32_t> m_outDegree;
 
 	cudaEvent_t m_ev0 = nullptr, m_ev1 = nullptr;
+	std::vector<cudaEvent_t> m_evPool;
+	std::vector<std::pair<int, size_t>> m_evUse;  // (kernel kind, first event index)
+	size_t m_evNext = 0;
+	bool m_inRun = false;
+	void timedBegin(int kind);
+	void timedEnd();
 	std::vector<void*> m_allocs;
 	template<typename T> T* dalloc(size_t n);
 };
