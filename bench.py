@@ -109,8 +109,8 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
@@ -254,8 +254,11 @@ def run_b200(args, rank, world, local):
     build_s = time.perf_counter() - t0
     W = args.window
 
-    # warm-up
+    # warm-up, then the launch-shape autotuner (its trial steps start from a
+    # snapshot of the state and leave it unchanged)
     sim.run(W * args.warmup, W, 1.0, ids=False)
+    tuned_us = sim.autotune(50) if not args.no_autotune else None
+    launch = sim.launch()
 
     # timed: K periods, device-resident, CUDA events inside the run loop
     barrier(world)
@@ -338,6 +341,7 @@ def run_b200(args, rank, world, local):
             "gpu_launches": args.steps * (W + 2),
             "clocks": clk.summary(),
             "build_s": build_s,
+            "launch": {"partition": launch[0], "threads": launch[1], "autotuned_us_per_step": tuned_us},
             "spikes_per_neuron_s": st["fired"] / args.neurons / (args.steps * W / 1e3),
         }
         print(json.dumps(line), flush=True)
@@ -359,6 +363,7 @@ def main():
     ap.add_argument("--cpu-ms", type=int, default=200)
     ap.add_argument("--cpu-warm-ms", type=int, default=50)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

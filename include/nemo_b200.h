@@ -261,6 +261,16 @@ NEMO_B200_API nemo_status_t nemo_b200_set_profiling(nemo_simulation_t, int on);
 NEMO_B200_API nemo_status_t nemo_b200_run_stats(nemo_simulation_t, float* run_ms,
 		float kernel_ms[3], unsigned kernel_launches[3],
 		uint64_t* fired, uint64_t* events, uint64_t* stdp_entries, uint64_t* plastic_synapses);
+/* Launch shape of the per-step kernel: neurons per CTA ("partition",
+ * rounded up to a multiple of 32, at most 2048) and threads per CTA (a
+ * multiple of 32, at most 1024).  Results are identical for every shape. */
+NEMO_B200_API nemo_status_t nemo_b200_set_launch(nemo_simulation_t, unsigned partition, unsigned threads);
+NEMO_B200_API nemo_status_t nemo_b200_get_launch(nemo_simulation_t, unsigned* partition, unsigned* threads);
+/* Autotuner: times candidate launch shapes on `trial_steps` steps each,
+ * starting every trial from a device-side snapshot of the simulation state
+ * and restoring it afterwards (the simulation is left exactly as it was),
+ * then keeps the fastest shape.  *us_per_step receives its time. */
+NEMO_B200_API nemo_status_t nemo_b200_autotune(nemo_simulation_t, unsigned trial_steps, float* us_per_step);
 /* Synaptic events (sum of the out-degrees of the fired neurons) of all
  * nemo_step calls on this simulation so far. */
 NEMO_B200_API nemo_status_t nemo_b200_step_events(nemo_simulation_t, uint64_t* events);

@@ -344,6 +344,22 @@ class Simulation:
                 "fired": vals[0].value, "events": vals[1].value,
                 "stdp_entries": vals[2].value, "plastic_synapses": vals[3].value}
 
+    def set_launch(self, partition: int, threads: int):
+        """Launch shape of the step kernel (an extension); results do not depend on it."""
+        _check(lib().nemo_b200_set_launch(self._h, partition, threads))
+
+    def launch(self):
+        p, t = C.c_uint(), C.c_uint()
+        _check(lib().nemo_b200_get_launch(self._h, C.byref(p), C.byref(t)))
+        return p.value, t.value
+
+    def autotune(self, trial_steps: int = 50) -> float:
+        """Pick the fastest launch shape on trial steps run from a snapshot
+        (the simulation state is restored); returns microseconds per step."""
+        us = C.c_float()
+        _check(lib().nemo_b200_autotune(self._h, trial_steps, C.byref(us)))
+        return us.value
+
     def step_events(self) -> int:
         """Synaptic events of all step() calls so far (an extension)."""
         v = C.c_uint64()

@@ -93,6 +93,9 @@ SIGNATURES = {
     "nemo_b200_synapse_count": (st, [vp, C.POINTER(C.c_uint64)]),
     "nemo_b200_set_profiling": (st, [vp, C.c_int]),
     "nemo_b200_run_stats": (st, [vp, PF, PF, PU] + [C.POINTER(C.c_uint64)] * 4),
+    "nemo_b200_set_launch": (st, [vp, C.c_uint, C.c_uint]),
+    "nemo_b200_get_launch": (st, [vp, PU, PU]),
+    "nemo_b200_autotune": (st, [vp, C.c_uint, PF]),
     "nemo_b200_step_events": (st, [vp, C.POINTER(C.c_uint64)]),
     "nemo_b200_neuron_type_count": (C.c_uint, []),
     "nemo_b200_neuron_type_name": (C.c_char_p, [C.c_uint]),

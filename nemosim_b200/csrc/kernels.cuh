@@ -171,22 +171,4 @@ __device__ __forceinline__ bool update_poisson(const DevSim& S, const TypeRange&
 	return p1 < p0 || fs;
 }
 
-// Walk the incoming plastic synapses of `tgt` and accumulate their STDP
-// weight change (ConnectivityMatrix::accumulateStdp,
-// src/nemo/ConnectivityMatrix.cpp:193-227).  Called by a whole warp.
-__device__ __forceinline__ unsigned long long stdp_accumulate_target(const DevSim& S, uint32_t tgt,
-		const uint64_t* histPrev, uint32_t lane)
-{
-	unsigned long long b = S.rcmPtr[tgt], e = S.rcmPtr[tgt + 1];
-	for(unsigned long long p = b + lane; p < e; p += 32) {
-		uint32_t sd = S.rcmSrc[p];
-		uint32_t src = sd & (MAX_NEURONS - 1);
-		uint32_t delay = (sd >> 26) + 1;
-		uint64_t pre = histPrev[src] >> (delay & 63);
-		int32_t dw = stdp_weight_change(S.sp, pre);
-		if(dw != 0) S.rcmAcc[p] = (int32_t) ((uint32_t) S.rcmAcc[p] + (uint32_t) dw);
-	}
-	return e - b;
-}
-
 } // namespace nemo_b200

@@ -569,6 +569,30 @@ nemo_status_t nemo_b200_run_stats(nemo_simulation_t s, float* runMs, float kerne
 	});
 }
 
+nemo_status_t nemo_b200_set_launch(nemo_simulation_t s, unsigned partition, unsigned threads)
+{
+	NULLCHECK(s);
+	CALL(S(s).setLaunch(partition, threads));
+}
+
+nemo_status_t nemo_b200_get_launch(nemo_simulation_t s, unsigned* partition, unsigned* threads)
+{
+	NULLCHECK(s);
+	CALL({
+		if(partition) *partition = S(s).partition();
+		if(threads) *threads = S(s).threads();
+	});
+}
+
+nemo_status_t nemo_b200_autotune(nemo_simulation_t s, unsigned trial_steps, float* us_per_step)
+{
+	NULLCHECK(s);
+	CALL({
+		float us = S(s).autotune(trial_steps);
+		if(us_per_step) *us_per_step = us;
+	});
+}
+
 nemo_status_t nemo_b200_step_events(nemo_simulation_t s, uint64_t* events)
 {
 	NULLCHECK(s);

@@ -23,162 +23,267 @@ namespace nemo_b200 {
 // ---------------------------------------------------------------------------
 // kernels
 
-// One simulation step (see kernels.cuh).  Block = STEP_THREADS threads, one
-// neuron per thread, warps aligned to 32-neuron words of the bit-vectors.
-__global__ void __launch_bounds__(STEP_THREADS)
-step_kernel(const DevSim S, uint32_t cur, uint32_t slot, uint32_t ring, int stdpPrev)
+// Shared-memory work list of one CTA: the items (fired neurons or STDP
+// targets) it collected, each with a span of consecutive entries of a CSR
+// array (outgoing synapses or incoming plastic synapses).  off[] is the
+// exclusive prefix sum of the span lengths and adj[i] = start(i) - off[i],
+// so flat work item k of the CTA is entry adj[i] + k for the i whose span
+// contains k.  Spreading all spans over all threads of the CTA keeps every
+// thread's loads independent of the item sizes.
+struct WorkList {
+	uint32_t* item;               // [cap]
+	uint32_t* off;                // [cap + 1]
+	unsigned long long* adj;      // [cap]
+};
+
+__device__ __forceinline__ WorkList carve_list(unsigned char*& p, uint32_t cap)
 {
-	__shared__ uint32_t sFired[STEP_THREADS];
-	__shared__ uint32_t sStdp[STEP_THREADS];
-	__shared__ uint32_t sNF, sNS;
-	__shared__ unsigned long long sEvents, sStdpWalk;
+	WorkList w;
+	w.adj = reinterpret_cast<unsigned long long*>(p);
+	p += 8 * (size_t) cap;
+	w.item = reinterpret_cast<uint32_t*>(p);
+	p += 4 * (size_t) cap;
+	w.off = reinterpret_cast<uint32_t*>(p);
+	p += 4 * (size_t) (cap + 1);
+	p = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
+	return w;
+}
 
-	const uint32_t tid = threadIdx.x;
-	const uint32_t lane = tid & 31, warp = tid >> 5;
-	const uint32_t n = blockIdx.x * STEP_THREADS + tid;
-	const uint32_t prev = cur ^ 1u;
-	const uint64_t* histPrev = S.hist + (size_t) prev * S.N;
+// Block-wide exclusive scan of the span lengths ptr[item+1] - ptr[item] of
+// the n collected items; returns the total.  All threads must call it.
+__device__ uint32_t build_offsets(const WorkList& L, uint32_t n, const unsigned long long* ptr, uint32_t* warpTmp)
+{
+	const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+	uint32_t carry = 0;
+	for(uint32_t base = 0; base < n; base += blockDim.x) {
+		const uint32_t i = base + tid;
+		unsigned long long b = 0;
+		uint32_t c = 0;
+		if(i < n) {
+			const uint32_t it = L.item[i];
+			b = ptr[it];
+			c = (uint32_t) (ptr[it + 1] - b);
+		}
+		uint32_t x = c;
+#pragma unroll
+		for(int o = 1; o < 32; o <<= 1) {
+			uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+			if(lane >= (uint32_t) o) x += y;
+		}
+		if(lane == 31) warpTmp[warp] = x;
+		__syncthreads();
+		if(warp == 0) {
+			uint32_t s = lane < nwarps ? warpTmp[lane] : 0;
+#pragma unroll
+			for(int o = 1; o < 32; o <<= 1) {
+				uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+				if(lane >= (uint32_t) o) s += y;
+			}
+			warpTmp[lane] = s;
+		}
+		__syncthreads();
+		const uint32_t o = carry + (warp ? warpTmp[warp - 1] : 0) + x - c;
+		if(i < n) {
+			L.off[i] = o;
+			L.adj[i] = b - o;
+		}
+		carry += warpTmp[nwarps - 1];
+		__syncthreads();
+	}
+	if(threadIdx.x == 0) L.off[n] = carry;
+	__syncthreads();
+	return carry;
+}
+
+// the item whose span holds flat work item k: largest i < n with off[i] <= k
+__device__ __forceinline__ uint32_t find_item(const uint32_t* off, uint32_t n, uint32_t k)
+{
+	uint32_t lo = 0, hi = n;
+	while(hi - lo > 1) {
+		uint32_t mid = (lo + hi) >> 1;
+		if(off[mid] <= k) lo = mid; else hi = mid;
+	}
+	return lo;
+}
+
+constexpr uint32_t ILP = 4;
+
+// scatter: add every outgoing synapse of the CTA's fired neurons into the
+// accumulator slot of its arrival step (64-bit integer atomics)
+__device__ __forceinline__ void scatter_phase(const DevSim& S, const WorkList& L, uint32_t n, uint32_t total, uint32_t slot)
+{
+	const uint32_t T = blockDim.x;
+	for(uint32_t k0 = threadIdx.x; k0 < total; k0 += ILP * T) {
+		uint2 s[ILP];
+#pragma unroll
+		for(uint32_t j = 0; j < ILP; ++j) {
+			const uint32_t k = k0 + j * T;
+			if(k < total) {
+				const uint32_t i = find_item(L.off, n, k);
+				s[j] = S.syn[L.adj[i] + k];
+			}
+		}
+#pragma unroll
+		for(uint32_t j = 0; j < ILP; ++j) {
+			if(k0 + j * T < total) {
+				uint32_t d = (s[j].x >> 26) + 1;
+				uint32_t sl = slot + d;
+				sl = sl >= S.D ? sl - S.D : sl;
+				add_current(S.slots + (size_t) sl * S.N + (s[j].x & (MAX_NEURONS - 1)), (int32_t) s[j].y);
+			}
+		}
+	}
+}
+
+// STDP accumulation over the incoming plastic synapses of the CTA's targets
+// (ConnectivityMatrix::accumulateStdp, src/nemo/ConnectivityMatrix.cpp:193-227)
+__device__ __forceinline__ void stdp_phase(const DevSim& S, const WorkList& L, uint32_t n, uint32_t total,
+		const uint64_t* hist)
+{
+	const uint32_t T = blockDim.x;
+	for(uint32_t k0 = threadIdx.x; k0 < total; k0 += ILP * T) {
+		unsigned long long p[ILP];
+		uint32_t sd[ILP];
+		int32_t acc[ILP];
+		uint64_t h[ILP];
+#pragma unroll
+		for(uint32_t j = 0; j < ILP; ++j) {
+			const uint32_t k = k0 + j * T;
+			if(k < total) {
+				const uint32_t i = find_item(L.off, n, k);
+				p[j] = L.adj[i] + k;
+				sd[j] = S.rcmSrc[p[j]];
+				acc[j] = S.rcmAcc[p[j]];
+			}
+		}
+#pragma unroll
+		for(uint32_t j = 0; j < ILP; ++j) {
+			if(k0 + j * T < total) h[j] = hist[sd[j] & (MAX_NEURONS - 1)];
+		}
+#pragma unroll
+		for(uint32_t j = 0; j < ILP; ++j) {
+			if(k0 + j * T < total) {
+				const uint32_t delay = (sd[j] >> 26) + 1;
+				int32_t dw = stdp_weight_change(S.sp, h[j] >> (delay & 63));
+				if(dw != 0) S.rcmAcc[p[j]] = (int32_t) ((uint32_t) acc[j] + (uint32_t) dw);
+			}
+		}
+	}
+}
+
+// warp-aggregated append of the lanes whose flag is set
+__device__ __forceinline__ void append(uint32_t* list, uint32_t* count, bool flag, uint32_t value)
+{
+	const uint32_t lane = threadIdx.x & 31;
+	const uint32_t b = __ballot_sync(0xffffffffu, flag);
+	if(!b) return;
+	uint32_t base = 0;
+	if(lane == 0) base = atomicAdd(count, (uint32_t) __popc(b));
+	base = __shfl_sync(0xffffffffu, base, 0);
+	if(flag) list[base + __popc(b & ((1u << lane) - 1u))] = value;
+}
+
+// One simulation step (see kernels.cuh).  CTA c owns the partition of P
+// consecutive neurons starting at c * P (P a multiple of 32, so warps cover
+// whole bit-vector words); its blockDim.x threads loop over them.
+__global__ void __launch_bounds__(1024)
+step_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t slot, uint32_t ring, int stdpPrev)
+{
+	extern __shared__ __align__(16) unsigned char smem[];
+	__shared__ uint32_t sNF, sNS, warpTmp[32];
+
+	const uint32_t tid = threadIdx.x, lane = tid & 31;
+	const uint32_t first = blockIdx.x * P;
+	const uint32_t last = min(S.N, first + P);
+	const uint64_t* histPrev = S.hist + (size_t) (cur ^ 1u) * S.N;
 	uint64_t* histCur = S.hist + (size_t) cur * S.N;
+	unsigned char* sp = smem;
+	WorkList LF = carve_list(sp, P);
+	WorkList LS = carve_list(sp, P);
 
-	if(tid == 0) { sNF = 0; sNS = 0; sEvents = 0; sStdpWalk = 0; }
+	if(tid == 0) { sNF = 0; sNS = 0; }
 	__syncthreads();
 
-	bool fired = false, stdpTarget = false;
-	uint32_t fw = 0;
-	if(n < S.N) {
-		uint32_t k = 0;
-		while(k + 1 < S.ntypes && n >= S.types[k + 1].base) ++k;
-		const TypeRange& T = S.types[k];
-		const uint32_t nl = n - T.base;
-
-		// 1. this step's synaptic input (deliverSpikes + wfx_toFloat,
-		//    src/nemo/cpu/Simulation.cpp:259-288)
-		float cE = 0.0f, cI = 0.0f;
-		if(S.D) {
-			longlong2* sp = S.slots + (size_t) slot * S.N + n;
-			longlong2 acc = *sp;
-			if(acc.x | acc.y) *sp = make_longlong2(0, 0);
-			cE = wfx_to_float(acc.x);
-			cI = wfx_to_float(acc.y);
+	// 1-3: read-out, update, history, fired bit-vector, compaction
+	for(uint32_t base = first; base < last; base += blockDim.x) {
+		const uint32_t n = base + tid;
+		bool fired = false, stdpTarget = false;
+		uint32_t fw = 0;
+		if(n < last) {
+			uint32_t k = 0;
+			while(k + 1 < S.ntypes && n >= S.types[k + 1].base) ++k;
+			const TypeRange& T = S.types[k];
+			const uint32_t nl = n - T.base;
+			float cE = 0.0f, cI = 0.0f;
+			if(S.D) {
+				longlong2* a = S.slots + (size_t) slot * S.N + n;
+				longlong2 acc = *a;
+				if(acc.x | acc.y) *a = make_longlong2(0, 0);
+				cE = wfx_to_float(acc.x);
+				cI = wfx_to_float(acc.y);
+			}
+			float ext = S.curExt[n];
+			if(__float_as_uint(ext) != 0u) S.curExt[n] = 0.0f;
+			fw = S.fstim[n >> 5];
+			const bool fs = (fw >> lane) & 1u;
+			switch(T.kind) {
+				case KIND_IZHIKEVICH: fired = update_izhikevich(S, T, nl, n, cE, cI, ext, fs); break;
+				case KIND_IF_CURR_EXP: fired = update_if_curr_exp(T, nl, cE, cI, ext, fs); break;
+				case KIND_POISSON: fired = update_poisson(S, T, nl, n, fs); break;
+				default: fired = fs; break; // Input, src/nemo/cpu/plugins/Input.cpp:17-22
+			}
+			const uint64_t h = histPrev[n];
+			histCur[n] = (h << 1) | (uint64_t) fired;
+			stdpTarget = stdpPrev && (h & S.sp.postFireMask) && S.rcmPtr[n + 1] > S.rcmPtr[n];
 		}
-		float ext = S.curExt[n];
-		if(__float_as_uint(ext) != 0u) S.curExt[n] = 0.0f;
-		fw = S.fstim[n >> 5];
-		const bool fs = (fw >> lane) & 1u;
-
-		// 2. plugin update
-		switch(T.kind) {
-			case KIND_IZHIKEVICH: fired = update_izhikevich(S, T, nl, n, cE, cI, ext, fs); break;
-			case KIND_IF_CURR_EXP: fired = update_if_curr_exp(T, nl, cE, cI, ext, fs); break;
-			case KIND_POISSON: fired = update_poisson(S, T, nl, n, fs); break;
-			default: fired = fs; break; // Input, src/nemo/cpu/plugins/Input.cpp:17-22
+		const uint32_t fb = __ballot_sync(0xffffffffu, fired);
+		if(lane == 0 && n < last) {
+			S.firedRing[(size_t) ring * S.W + (n >> 5)] = fb;
+			if(fw) S.fstim[n >> 5] = 0u;
 		}
-
-		// 3. history (recentFiring = recentFiring << 1 | fired)
-		const uint64_t h = histPrev[n];
-		histCur[n] = (h << 1) | (uint64_t) fired;
-		stdpTarget = stdpPrev && (h & S.sp.postFireMask) && S.rcmPtr[n + 1] > S.rcmPtr[n];
-	}
-
-	const uint32_t fb = __ballot_sync(0xffffffffu, fired);
-	const uint32_t sb = __ballot_sync(0xffffffffu, stdpTarget);
-	if(lane == 0 && n < S.N) {
-		S.firedRing[(size_t) ring * S.W + (n >> 5)] = fb;
-		if(fw) S.fstim[n >> 5] = 0u;
-	}
-	// ballot/popc compaction of fired neurons and STDP targets
-	if(fb) {
-		uint32_t base = 0;
-		if(lane == 0) base = atomicAdd(&sNF, (uint32_t) __popc(fb));
-		base = __shfl_sync(0xffffffffu, base, 0);
-		if(fired) sFired[base + __popc(fb & ((1u << lane) - 1u))] = n;
-	}
-	if(sb) {
-		uint32_t base = 0;
-		if(lane == 0) base = atomicAdd(&sNS, (uint32_t) __popc(sb));
-		base = __shfl_sync(0xffffffffu, base, 0);
-		if(stdpTarget) sStdp[base + __popc(sb & ((1u << lane) - 1u))] = n;
+		append(LF.item, &sNF, fired, n);
+		append(LS.item, &sNS, stdpTarget, n);
 	}
 	__syncthreads();
 	const uint32_t nf = sNF, ns = sNS;
 
-	// 4. scatter the fired neurons' outgoing synapses into the slots of
-	//    their arrival steps (128-bit loads: two synapses per lane)
-	constexpr uint32_t WARPS = STEP_THREADS / 32;
-	unsigned long long events = 0;
-	for(uint32_t i = warp; i < nf; i += WARPS) {
-		const uint32_t src = sFired[i];
-		unsigned long long b = S.outPtr[src], e = S.outPtr[src + 1];
-		events += e - b;
-		if(!S.D) continue;
-		// align the start to 16 bytes
-		if((b & 1ull) && b < e) {
-			if(lane == 0) {
-				uint2 s = S.syn[b];
-				uint32_t d = (s.x >> 26) + 1;
-				uint32_t sl = slot + d; sl = sl >= S.D ? sl - S.D : sl;
-				add_current(S.slots + (size_t) sl * S.N + (s.x & (MAX_NEURONS - 1)), (int32_t) s.y);
-			}
-			++b;
-		}
-		for(unsigned long long p = b + 2 * lane; p < e; p += 64) {
-			if(p + 1 < e) {
-				uint4 s2 = *reinterpret_cast<const uint4*>(S.syn + p);
-				uint32_t d0 = (s2.x >> 26) + 1, d1 = (s2.z >> 26) + 1;
-				uint32_t sl0 = slot + d0; sl0 = sl0 >= S.D ? sl0 - S.D : sl0;
-				uint32_t sl1 = slot + d1; sl1 = sl1 >= S.D ? sl1 - S.D : sl1;
-				add_current(S.slots + (size_t) sl0 * S.N + (s2.x & (MAX_NEURONS - 1)), (int32_t) s2.y);
-				add_current(S.slots + (size_t) sl1 * S.N + (s2.z & (MAX_NEURONS - 1)), (int32_t) s2.w);
-			} else {
-				uint2 s = S.syn[p];
-				uint32_t d = (s.x >> 26) + 1;
-				uint32_t sl = slot + d; sl = sl >= S.D ? sl - S.D : sl;
-				add_current(S.slots + (size_t) sl * S.N + (s.x & (MAX_NEURONS - 1)), (int32_t) s.y);
-			}
-		}
-	}
-	if(lane == 0 && events) atomicAdd(&sEvents, events);
+	// 4. scatter, 5. STDP of the previous step
+	const uint32_t wf = nf ? build_offsets(LF, nf, S.outPtr, warpTmp) : 0;
+	const uint32_t ws = ns ? build_offsets(LS, ns, S.rcmPtr, warpTmp) : 0;
+	if(S.D && wf) scatter_phase(S, LF, nf, wf, slot);
+	if(ws) stdp_phase(S, LS, ns, ws, histPrev);
 
-	// 5. STDP accumulation of the previous step
-	unsigned long long walked = 0;
-	for(uint32_t i = warp; i < ns; i += WARPS) {
-		walked += stdp_accumulate_target(S, sStdp[i], histPrev, lane);
-	}
-	if(lane == 0 && walked) atomicAdd(&sStdpWalk, walked);
-
-	__syncthreads();
 	if(tid == 0) {
 		if(nf) atomicAdd(&S.firedCount[ring], nf);
-		if(sEvents) atomicAdd(&S.eventCount[ring], sEvents);
-		if(sStdpWalk) atomicAdd(&S.stdpCount[ring], sStdpWalk);
+		if(wf) atomicAdd(&S.eventCount[ring], (unsigned long long) wf);
+		if(ws) atomicAdd(&S.stdpCount[ring], (unsigned long long) ws);
 	}
 }
 
 // Pending STDP accumulation of the last completed step (history buffer `par`)
-__global__ void __launch_bounds__(STEP_THREADS)
-stdp_kernel(const DevSim S, uint32_t par, uint32_t ring)
+__global__ void __launch_bounds__(1024)
+stdp_kernel(const DevSim S, uint32_t P, uint32_t par, uint32_t ring)
 {
-	__shared__ uint32_t sStdp[STEP_THREADS];
-	__shared__ uint32_t sNS;
-	const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-	const uint32_t n = blockIdx.x * STEP_THREADS + tid;
+	extern __shared__ __align__(16) unsigned char smem[];
+	__shared__ uint32_t sNS, warpTmp[32];
+	const uint32_t tid = threadIdx.x;
+	const uint32_t first = blockIdx.x * P;
+	const uint32_t last = min(S.N, first + P);
 	const uint64_t* hist = S.hist + (size_t) par * S.N;
+	unsigned char* sp = smem;
+	WorkList LS = carve_list(sp, P);
 	if(tid == 0) sNS = 0;
 	__syncthreads();
-	bool target = n < S.N && (hist[n] & S.sp.postFireMask) && S.rcmPtr[n + 1] > S.rcmPtr[n];
-	uint32_t sb = __ballot_sync(0xffffffffu, target);
-	if(sb) {
-		uint32_t base = 0;
-		if(lane == 0) base = atomicAdd(&sNS, (uint32_t) __popc(sb));
-		base = __shfl_sync(0xffffffffu, base, 0);
-		if(target) sStdp[base + __popc(sb & ((1u << lane) - 1u))] = n;
+	for(uint32_t base = first; base < last; base += blockDim.x) {
+		const uint32_t n = base + tid;
+		bool target = n < last && (hist[n] & S.sp.postFireMask) && S.rcmPtr[n + 1] > S.rcmPtr[n];
+		append(LS.item, &sNS, target, n);
 	}
 	__syncthreads();
-	unsigned long long walked = 0;
-	for(uint32_t i = warp; i < sNS; i += STEP_THREADS / 32) {
-		walked += stdp_accumulate_target(S, sStdp[i], hist, lane);
-	}
-	if(lane == 0 && walked) atomicAdd(&S.stdpCount[ring], walked);
+	const uint32_t ns = sNS;
+	const uint32_t ws = ns ? build_offsets(LS, ns, S.rcmPtr, warpTmp) : 0;
+	if(ws) stdp_phase(S, LS, ns, ws, hist);
+	if(tid == 0 && ws) atomicAdd(&S.stdpCount[ring], (unsigned long long) ws);
 }
 
 // applyStdp (src/nemo/ConnectivityMatrix.cpp:241-294): one warp per target,
@@ -187,7 +292,7 @@ stdp_kernel(const DevSim S, uint32_t par, uint32_t ring)
 // the old weight but not yet arrived (source fired k < delay steps ago) are
 // corrected in their accumulator slots.
 __global__ void __launch_bounds__(STEP_THREADS)
-apply_stdp_kernel(const DevSim S, int32_t reward, uint32_t par, uint32_t slot)
+apply_stdp_kernel(const DevSim S, int32_t reward, uint32_t par, uint32_t slot, int fullPass)
 {
 	const uint32_t lane = threadIdx.x & 31;
 	const uint32_t warpsTotal = gridDim.x * (STEP_THREADS / 32);
@@ -195,8 +300,12 @@ apply_stdp_kernel(const DevSim S, int32_t reward, uint32_t par, uint32_t slot)
 	for(uint32_t tgt = blockIdx.x * (STEP_THREADS / 32) + (threadIdx.x >> 5); tgt < S.N; tgt += warpsTotal) {
 		unsigned long long b = S.rcmPtr[tgt], e = S.rcmPtr[tgt + 1];
 		for(unsigned long long p = b + lane; p < e; p += 32) {
-			uint32_t fwd = S.rcmFwd[p];
 			int32_t acc = S.rcmAcc[p];
+			// Once every plastic weight lies within its clamp range (after the
+			// first pass), a zero accumulator leaves the weight unchanged:
+			// updatedWeight(w, 0) == w.
+			if(acc == 0 && !fullPass) continue;
+			uint32_t fwd = S.rcmFwd[p];
 			int32_t w = (int32_t) S.syn[fwd].y;
 			int32_t nw = stdp_updated_weight(S.sp, w, fx_mul_dev(reward, acc));
 			if(nw != w) {
@@ -431,7 +540,10 @@ Simulation::Simulation(const Network& net, const Configuration& conf)
 	std::vector<unsigned long long> outPtr(N + 1);
 	for(unsigned s = 0; s <= N; ++s) outPtr[s] = rowStart[(size_t) s * D];
 	m_outDegree.resize(N);
-	for(unsigned s = 0; s < N; ++s) m_outDegree[s] = (uint32_t) (outPtr[s + 1] - outPtr[s]);
+	for(unsigned s = 0; s < N; ++s) {
+		m_outDegree[s] = (uint32_t) (outPtr[s + 1] - outPtr[s]);
+		m_maxOutDeg = std::max(m_maxOutDeg, m_outDegree[s]);
+	}
 	std::vector<uint2> syn(Sn);
 	for(size_t k = 0; k < Sn; ++k) {
 		syn[m_pos[k]] = make_uint2(ltgt[k] | ((net.delay[k] - 1) << 26), (uint32_t) fxw[k]);
@@ -489,7 +601,10 @@ Simulation::Simulation(const Network& net, const Configuration& conf)
 		sp.postFireMask = shl64(1ull, sp.npost);
 
 		for(size_t k = 0; k < Sn; ++k) if(net.plastic[k]) rcmPtr[ltgt[k] + 1]++;
-		for(unsigned t = 0; t < N; ++t) rcmPtr[t + 1] += rcmPtr[t];
+		for(unsigned t = 0; t < N; ++t) {
+			m_maxPlasticInDeg = std::max(m_maxPlasticInDeg, (uint32_t) rcmPtr[t + 1]);
+			rcmPtr[t + 1] += rcmPtr[t];
+		}
 		size_t P = rcmPtr[N];
 		std::vector<uint32_t> rsrc(P), rfwd(P);
 		std::vector<unsigned long long> fill(rcmPtr.begin(), rcmPtr.end() - 1);
@@ -536,6 +651,14 @@ Simulation::Simulation(const Network& net, const Configuration& conf)
 	NB_CUDA(cudaMallocHost(&m_hFired, (size_t) S.R * S.W * 4));
 
 	if(needCalib) S.calib = device_calibration(m_device);
+	NB_CUDA(cudaDeviceGetAttribute(&m_sms, cudaDevAttrMultiProcessorCount, m_device));
+	NB_CUDA(cudaFuncSetAttribute(step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) stepSmem(MAX_PARTITION)));
+	NB_CUDA(cudaFuncSetAttribute(stdp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) stepSmem(MAX_PARTITION)));
+	// default launch shape: two partitions per SM
+	{
+		uint32_t P = (uint32_t) ((N + 2 * m_sms - 1) / (2 * m_sms));
+		setLaunch(P, std::min<uint32_t>(1024, std::max<uint32_t>(128, (P + 31) & ~31u)));
+	}
 	NB_CUDA(cudaStreamSynchronize(m_stream));
 	resetTimer();
 }
@@ -592,14 +715,30 @@ void Simulation::timedEnd()
 	NB_CUDA(cudaEventRecord(m_evPool[m_evUse.back().second + 1], m_stream));
 }
 
+size_t Simulation::stepSmem(uint32_t P) const
+{
+	size_t list = ((size_t) 8 * P + 4 * P + 4 * (P + 1) + 15) & ~(size_t) 15;
+	return 2 * list;
+}
+
+void Simulation::setLaunch(uint32_t P, uint32_t T)
+{
+	P = std::max<uint32_t>(32, std::min<uint32_t>(MAX_PARTITION, (P + 31) & ~31u));
+	T = std::max<uint32_t>(32, std::min<uint32_t>(1024, (T + 31) & ~31u));
+	// the per-CTA work offsets are 32-bit
+	while(P > 32 && ((uint64_t) P * std::max(m_maxOutDeg, m_maxPlasticInDeg) >= (1ull << 31))) P -= 32;
+	m_P = P;
+	m_T = T;
+}
+
 void Simulation::launchStep(bool /*fullRecord*/)
 {
 	const uint32_t cur = (uint32_t) (m_cycle & 1);
 	const uint32_t slot = m_dev.D ? (uint32_t) (m_cycle % m_dev.D) : 0;
 	const uint32_t ring = (uint32_t) (m_cycle % m_dev.R);
-	const unsigned grid = (m_N + STEP_THREADS - 1) / STEP_THREADS;
+	const unsigned grid = (m_N + m_P - 1) / m_P;
 	timedBegin(K_STEP);
-	step_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, cur, slot, ring, m_stdpPending ? 1 : 0);
+	step_kernel<<<grid, m_T, stepSmem(m_P), m_stream>>>(m_dev, m_P, cur, slot, ring, m_stdpPending ? 1 : 0);
 	timedEnd();
 	m_stdpPending = m_dev.stdp != 0;
 	m_cycle++;
@@ -671,9 +810,9 @@ void Simulation::flushStdp()
 {
 	if(!m_stdpPending) return;
 	const uint32_t par = (uint32_t) ((m_cycle - 1) & 1);
-	const unsigned grid = (m_N + STEP_THREADS - 1) / STEP_THREADS;
+	const unsigned grid = (m_N + m_P - 1) / m_P;
 	timedBegin(K_STDP);
-	stdp_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, par, (uint32_t) ((m_cycle - 1) % m_dev.R));
+	stdp_kernel<<<grid, m_T, stepSmem(m_P) / 2, m_stream>>>(m_dev, m_P, par, (uint32_t) ((m_cycle - 1) % m_dev.R));
 	timedEnd();
 	m_stdpPending = false;
 }
@@ -690,8 +829,11 @@ void Simulation::applyStdpDevice(int32_t R)
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m_device);
 	unsigned grid = std::min<unsigned>((m_N + 7) / 8, (unsigned) sms * 8);
 	timedBegin(K_APPLY);
-	apply_stdp_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, R, par, slot);
+	apply_stdp_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, R, par, slot, m_weightsClamped ? 0 : 1);
 	timedEnd();
+	// updatedWeight's result always lies within the clamp range of its sign
+	// class, so after one full pass every plastic weight does
+	m_weightsClamped = true;
 }
 
 /* ConnectivityMatrix::applyStdp argument checks (src/nemo/ConnectivityMatrix.cpp:241-259) */
@@ -792,6 +934,94 @@ void Simulation::run(unsigned steps, unsigned stdpPeriod, float reward, unsigned
 	}
 	if(len) *len = total;
 	lastRunMs = runMs;
+}
+
+float Simulation::autotune(unsigned trialSteps)
+{
+	NB_CUDA(cudaSetDevice(m_device));
+	sync();
+	trialSteps = std::max(1u, trialSteps);
+	// the state that trial steps modify
+	std::vector<std::pair<void*, size_t>> regions;
+	for(const HostType& t : m_types) regions.emplace_back(t.dState, (size_t) t.n * t.desc->nstate * 4);
+	regions.emplace_back(m_dev.rng, (size_t) 4 * m_N * 4);
+	regions.emplace_back(m_dev.hist, (size_t) 2 * m_N * 8);
+	regions.emplace_back(m_dev.fstim, (size_t) m_dev.W * 4);
+	regions.emplace_back(m_dev.curExt, (size_t) m_N * 4);
+	if(m_dev.D) regions.emplace_back(m_dev.slots, (size_t) m_dev.D * m_N * 16);
+	if(m_dev.stdp) regions.emplace_back(m_dev.rcmAcc, (size_t) lastPlastic * 4);
+	std::vector<void*> backup;
+	for(auto& r : regions) {
+		void* p = nullptr;
+		if(r.second == 0) { backup.push_back(nullptr); continue; }
+		cudaError_t err = cudaMalloc(&p, r.second);
+		if(err != cudaSuccess) {
+			for(void* b : backup) if(b) cudaFree(b);
+			NB_THROW(NEMO_CUDA_MEMORY_ERROR, "autotune: no device memory for the state snapshot");
+		}
+		NB_CUDA(cudaMemcpyAsync(p, r.first, r.second, cudaMemcpyDeviceToDevice, m_stream));
+		backup.push_back(p);
+	}
+	const uint64_t cycle = m_cycle;
+	const bool pending = m_stdpPending;
+	const unsigned long timerSteps = m_timerSteps;
+	const bool prof = profiling;
+	profiling = false;
+	auto restore = [&]() {
+		for(size_t i = 0; i < regions.size(); ++i) {
+			if(backup[i]) {
+				NB_CUDA(cudaMemcpyAsync(regions[i].first, backup[i], regions[i].second, cudaMemcpyDeviceToDevice, m_stream));
+			}
+		}
+		m_cycle = cycle;
+		m_stdpPending = pending;
+		m_timerSteps = timerSteps;
+	};
+
+	// candidates: 1 to 16 partitions per SM, 128 to 1024 threads per CTA
+	std::vector<std::pair<uint32_t, uint32_t>> cands;
+	for(unsigned k : {1u, 2u, 3u, 4u, 6u, 8u, 12u, 16u}) {
+		uint32_t P = (uint32_t) ((m_N + (size_t) k * m_sms - 1) / ((size_t) k * m_sms));
+		P = std::max<uint32_t>(32, std::min<uint32_t>(MAX_PARTITION, (P + 31) & ~31u));
+		for(uint32_t T : {128u, 256u, 512u, 1024u}) {
+			if(T > std::max<uint32_t>(128, P)) continue;
+			if(std::find(cands.begin(), cands.end(), std::make_pair(P, T)) == cands.end()) cands.emplace_back(P, T);
+		}
+	}
+	const uint32_t P0 = m_P, T0 = m_T;
+	float best = -1;
+	uint32_t bestP = P0, bestT = T0;
+	try {
+		for(auto& c : cands) {
+			setLaunch(c.first, c.second);
+			launchStep(false); // untimed warm-up of this shape
+			NB_CUDA(cudaEventRecord(m_ev0, m_stream));
+			for(unsigned i = 0; i < trialSteps; ++i) launchStep(false);
+			NB_CUDA(cudaEventRecord(m_ev1, m_stream));
+			sync();
+			NB_CUDA(cudaGetLastError());
+			float ms = 0;
+			NB_CUDA(cudaEventElapsedTime(&ms, m_ev0, m_ev1));
+			if(best < 0 || ms < best) {
+				best = ms;
+				bestP = m_P;
+				bestT = m_T;
+			}
+			restore();
+		}
+	} catch(...) {
+		restore();
+		sync();
+		for(void* b : backup) if(b) cudaFree(b);
+		setLaunch(P0, T0);
+		profiling = prof;
+		throw;
+	}
+	sync();
+	for(void* b : backup) if(b) cudaFree(b);
+	profiling = prof;
+	setLaunch(bestP, bestT);
+	return best * 1e3f / trialSteps;
 }
 
 float Simulation::getNeuronState(unsigned g, unsigned var)

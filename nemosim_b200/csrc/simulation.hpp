@@ -16,7 +16,8 @@
 namespace nemo_b200 {
 
 constexpr unsigned MAX_TYPES = 8;
-constexpr unsigned STEP_THREADS = 256;
+constexpr unsigned STEP_THREADS = 256;   // block size of the apply/stimulus kernels
+constexpr unsigned MAX_PARTITION = 2048; // neurons per CTA of the step kernel
 
 struct TypeRange {
 	int kind;
@@ -104,6 +105,16 @@ public:
 	unsigned kernelLaunches[K_KINDS] = {0, 0, 0};
 	uint64_t lastFired = 0, lastEvents = 0, lastStdpEntries = 0, lastPlastic = 0;
 	bool profiling = false;
+
+	// partition size (neurons per CTA) and threads per CTA of the step
+	// kernel; results do not depend on them
+	uint32_t partition() const { return m_P; }
+	uint32_t threads() const { return m_T; }
+	void setLaunch(uint32_t P, uint32_t T);
+	// time candidate launch shapes on trial steps from a saved copy of the
+	// simulation state, restore it, and keep the fastest; returns its time
+	// per step in microseconds
+	float autotune(unsigned trialSteps);
 	uint64_t stepEvents = 0;  // synaptic events of all step() calls so far
 
 private:
@@ -119,6 +130,10 @@ private:
 	void locate(unsigned g, const HostType** t, unsigned* i) const;
 	size_t synapseKey(uint64_t id) const;
 	void launchStep(bool fullRecord);
+	size_t stepSmem(uint32_t P) const;
+	uint32_t m_P = 256, m_T = 256;
+	uint32_t m_maxOutDeg = 0, m_maxPlasticInDeg = 0;
+	int m_sms = 148;
 	void flushStdp();
 	void applyStdpDevice(int32_t fxReward);
 	void sync();
@@ -149,6 +164,7 @@ private:
 	// step state
 	uint64_t m_cycle = 0;        // steps since creation (never reset)
 	bool m_stdpPending = false;  // STDP accumulation of step m_cycle-1 not yet run
+	bool m_weightsClamped = false; // every plastic weight within its STDP limits
 	unsigned long m_timerSteps = 0;
 	std::chrono::steady_clock::time_point m_timerStart;
 

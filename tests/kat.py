@@ -1,0 +1,202 @@
+"""The reference's known-answer tests, written once against the shared
+Network/Configuration/Simulation interface so that they run on the oracle
+(tests/test_oracle_kat.py, CPU) and on the B200 backend
+(tests/test_parity_gpu.py).  Each cites the reference test it restates."""
+from __future__ import annotations
+
+import numpy as np
+
+from tests import nets
+
+f32 = np.float32
+
+
+def ring(mod, ncount, delay):
+    """runRing (src/test/test.cpp:300-325)"""
+    sim = mod.Simulation(nets.create_ring(mod, mod.Network(), ncount, delay=delay), mod.Configuration())
+    assert sim.step([0]) == [0]
+    for ms in range(1, ncount * 5 // 2):
+        fired = sim.step()
+        if delay == 1:
+            assert fired == [ms % ncount], (ms, fired)
+        elif ms % delay == 0:
+            assert fired == [(ms // delay) % ncount], (ms, fired)
+        else:
+            assert fired == [], (ms, fired)
+
+
+def double_ring(mod):
+    """runDoubleRing (src/test/test.cpp:328-362)"""
+    ncount = 512
+    net = mod.Network()
+    nets.create_ring(mod, net, ncount, 0, False, 1, 1)
+    nets.create_ring(mod, net, ncount, ncount, False, 1, 2)
+    sim = mod.Simulation(net, mod.Configuration())
+    sim.step([0, ncount])
+    for ms in range(1, ncount * 5 // 2):
+        fired = sim.step()
+        if ms % 2 == 0:
+            assert fired == [ms % ncount, ncount + (ms // 2) % ncount]
+        else:
+            assert fired == [ms % ncount]
+
+
+def firing_stimulus(mod):
+    """testFiringStimulus (src/test/test.cpp:202-238): fired == stimulated."""
+    ncount = 3000
+    net = mod.Network()
+    iz = net.add_neuron_type("Izhikevich")
+    net.add_neuron(iz, np.arange(ncount, dtype=np.uint32), *nets.exc_neuron_args())
+    sim = mod.Simulation(net, mod.Configuration())
+    rng = np.random.default_rng(0)
+    for _ in range(1000):
+        fstim = np.flatnonzero(rng.random(ncount) < 10 / ncount).tolist()
+        assert sorted(sim.step(fstim)) == sorted(fstim)
+
+
+def current_stimulus(mod):
+    """testCurrentStimulus (src/test/test.cpp:244-268)"""
+    ncount = 1500
+    sim = mod.Simulation(nets.create_ring(mod, mod.Network(), ncount), mod.Configuration())
+    sim.step(istim=[(5, 0.001), (8, 0.001), (0, 1000.0), (100, 0.001), (1, 0.001)])
+    for ms in range(1, ncount * 2):
+        assert sim.step() == [ms % ncount]
+
+
+def invalid_current_stimulus(mod):
+    """testInvalidCurrentStimulus (src/test/test.cpp:271-284)"""
+    ncount = 1000
+    sim = mod.Simulation(nets.create_ring(mod, mod.Network(), ncount), mod.Configuration())
+    sim.step()
+    sim.step()
+    try:
+        sim.step(istim=[(ncount + 1, 0.5)])
+    except mod.NemoError as e:
+        assert e.code == 6
+    else:
+        raise AssertionError("invalid current stimulus accepted")
+
+
+def saturation_network(mod):
+    net = mod.Network()
+    iz = net.add_neuron_type("Izhikevich")
+    params = [0.02, 0.2, -65.0, 8.0, 0.0, -13.0, -65.0]
+    for n in range(5):
+        net.add_neuron(iz, n, *params)
+    INPUT0, INPUT1, OUT_SAT, OUT_REF, OUT_WEAK = range(5)
+    for s, t, w in [(INPUT0, OUT_REF, 1024.0), (INPUT1, OUT_REF, 1024.0), (INPUT0, OUT_WEAK, 1000.0),
+                    (INPUT1, OUT_WEAK, 1000.0), (INPUT0, OUT_SAT, 1100.0), (INPUT1, OUT_SAT, 1100.0)]:
+        net.add_synapse(s, t, 1, w, False)
+    return net
+
+
+def fixed_point_saturation(mod):
+    """testFixedPointSaturation (src/test/test.cpp:414-467); returns u of
+    (ref, weak, saturated) outputs."""
+    sim = mod.Simulation(saturation_network(mod), mod.Configuration())
+    assert len(sim.step([0, 1])) == 2
+    assert len(sim.step()) == 3
+    u_ref, u_weak, u_sat = (sim.get_neuron_state(k, 0) for k in (3, 4, 2))
+    assert abs(u_ref - u_weak) > 1e-5
+    assert abs(u_ref - u_sat) < 1e-5
+    return [u_ref, u_weak, u_sat]
+
+
+def non_contiguous_indices(mod, n0, nstep):
+    """testNonContigousNeuronIndices (src/test/test.cpp:517-547)"""
+    ncount = 1000
+    s0 = mod.Simulation(nets.create_ring(mod, mod.Network(), ncount, 0, False, nstep), mod.Configuration())
+    s1 = mod.Simulation(nets.create_ring(mod, mod.Network(), ncount, n0, False, nstep), mod.Configuration())
+    assert s0.step([0]) == [0]
+    assert s1.step([n0]) == [n0]
+    for _ in range(1, 2000):
+        a, b = s0.step(), s1.step()
+        assert len(a) == len(b) == 1 and a[0] == b[0] - n0
+
+
+def type_mixture_network(mod, iz_first):
+    net = mod.Network()
+    if iz_first:
+        nets.create_ring(mod, net, 1024)
+    ps = net.add_neuron_type("PoissonSource")
+    net.add_neuron(ps, np.arange(1024, 1024 + 1000, dtype=np.uint32), 0.001)
+    if not iz_first:
+        nets.create_ring(mod, net, 1024)
+    return net
+
+
+def neuron_type_mixture(mod, iz_first):
+    """testNeuronTypeMixture (src/test/test.cpp:369-410)"""
+    sim = mod.Simulation(type_mixture_network(mod, iz_first), mod.Configuration())
+    stream = []
+    for ms in range(1000):
+        fired = sorted(sim.step([0] if ms == 0 else None))
+        assert fired[0] == ms % 1024
+        assert all(f >= 1024 for f in fired[1:])
+        stream.append(fired)
+    return stream
+
+
+def poisson_rate(mod, duration=10000, others=False):
+    """testRate (src/test/PoissonSource.cpp:11-31)"""
+    net = mod.Network()
+    if others:
+        nets.create_ring(mod, net, 1024, 1)
+    ps = net.add_neuron_type("PoissonSource")
+    net.add_neuron(ps, 0, 0.010)
+    sim = mod.Simulation(net, mod.Configuration())
+    nfired = sum(len(sim.step()) for _ in range(duration))
+    expected = int(duration * 0.010)
+    assert nfired > 0 and abs(nfired - expected) < 2 * expected
+    return nfired
+
+
+GROUP = 2 * 768
+INIT_W = 5.0
+
+
+def stdp_analytic_network(mod):
+    """construct() of src/test/stdp.cpp:121-168 without noise connections"""
+    net = mod.Network()
+    iz = net.add_neuron_type("Izhikevich")
+    r = f32(0.5)
+    b = f32(f32(0.25) - f32(0.05) * r)
+    v = f32(-65.0)
+    for g in range(2):
+        net.add_neuron(iz, np.arange(g * GROUP, (g + 1) * GROUP, dtype=np.uint32),
+                       f32(f32(0.02) + f32(0.08) * r), b, v, 2.0, 0.0, f32(b * v), v)
+    loc = np.arange(GROUP, dtype=np.uint32)
+    net.add_synapse(loc, GROUP + loc, 1 + loc % 20, np.full(GROUP, INIT_W, f32), np.ones(GROUP, np.uint8))
+    return net
+
+
+def stdp_analytic(mod, reward, epochs=4):
+    """testStdp (src/test/stdp.cpp:243-265): after each epoch every plastic
+    synapse must have changed by epoch * reward * dw(dt) (within 0.001 %).
+    Returns the weights of every synapse after each epoch."""
+    sim = mod.Simulation(stdp_analytic_network(mod), nets.stdp_test_configuration(mod))
+    history = []
+    for epoch in range(1, epochs + 1):
+        for ms in range(100):
+            fstim = None
+            if ms == 10:
+                fstim = list(range(GROUP))
+            elif ms == 20:
+                fstim = list(range(GROUP, 2 * GROUP))
+            sim.step(fstim)
+        sim.apply_stdp(reward)
+        ws = []
+        for local in range(GROUP):
+            sid = sim.get_synapses_from(local)[0]
+            d = sim.get_synapse_delay(sid)
+            assert d == 1 + local % 20
+            assert sim.get_synapse_plastic(sid)
+            assert sim.get_synapse_target(sid) == GROUP + local
+            dt = -(10 - d)
+            dw = (-0.8 * np.exp(-(dt - 1) / 20.0)) if dt > 0 else (1.0 * np.exp(dt / 20.0))
+            expect = INIT_W + epoch * reward * dw
+            got = sim.get_synapse_weight(sid)
+            assert abs(got - expect) <= 1e-5 * abs(expect), (local, got, expect)
+            ws.append(got)
+        history.append(ws)
+    return history

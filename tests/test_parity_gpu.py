@@ -8,7 +8,7 @@ import pytest
 
 import nemosim_b200 as nb
 import oracle as O
-from tests import nets
+from tests import kat, nets
 
 pytestmark = pytest.mark.gpu
 
@@ -44,149 +44,48 @@ def assert_streams_equal(p, o):
 
 
 # ---------------------------------------------------------------------------
-# known-answer tests of the reference (src/test/test.cpp)
+# known-answer tests of the reference (src/test/test.cpp), on the device
 
-@pytest.mark.parametrize("ncount,delay", [(1000, 1), (1024, 1), (2000, 1), (4000, 1), (2000, 20)])
+@pytest.mark.parametrize("ncount,delay", [(1000, 1), (1024, 1), (2000, 1), (4000, 1), (2000, 20), (1000, 63)])
 def test_ring(ncount, delay):
-    """runRing (src/test/test.cpp:300-325)"""
-    net = nets.create_ring(nb, nb.Network(), ncount, delay=delay)
-    sim = nb.Simulation(net, nb.Configuration())
-    assert sim.step([0]) == [0]
-    for ms in range(1, ncount * 5 // 2):
-        fired = sim.step()
-        if delay == 1:
-            assert fired == [ms % ncount], (ms, fired)
-        elif ms % delay == 0:
-            assert fired == [(ms // delay) % ncount], (ms, fired)
-        else:
-            assert fired == [], (ms, fired)
+    kat.ring(nb, ncount, delay)
 
 
 def test_double_ring():
-    """runDoubleRing (src/test/test.cpp:328-362)"""
-    ncount = 512
-    net = nb.Network()
-    nets.create_ring(nb, net, ncount, 0, False, 1, 1)
-    nets.create_ring(nb, net, ncount, ncount, False, 1, 2)
-    sim = nb.Simulation(net, nb.Configuration())
-    sim.step([0, ncount])
-    for ms in range(1, ncount * 5 // 2):
-        fired = sim.step()
-        if ms % 2 == 0:
-            assert fired == [ms % ncount, ncount + (ms // 2) % ncount]
-        else:
-            assert fired == [ms % ncount]
+    kat.double_ring(nb)
 
 
 def test_firing_stimulus():
-    """testFiringStimulus (src/test/test.cpp:202-238): fired == stimulated."""
-    ncount = 3000
-    net = nb.Network()
-    iz = net.add_neuron_type("Izhikevich")
-    net.add_neuron(iz, np.arange(ncount, dtype=np.uint32), *nets.exc_neuron_args())
-    sim = nb.Simulation(net, nb.Configuration())
-    rng = np.random.default_rng(0)
-    for _ in range(1000):
-        fstim = np.flatnonzero(rng.random(ncount) < 10 / ncount).tolist()
-        assert sorted(sim.step(fstim)) == sorted(fstim)
+    kat.firing_stimulus(nb)
 
 
 def test_current_stimulus():
-    """testCurrentStimulus (src/test/test.cpp:244-268)"""
-    ncount = 1500
-    sim = nb.Simulation(nets.create_ring(nb, nb.Network(), ncount), nb.Configuration())
-    istim = [(5, 0.001), (8, 0.001), (0, 1000.0), (100, 0.001), (1, 0.001)]
-    sim.step(istim=istim)
-    for ms in range(1, ncount * 2):
-        assert sim.step() == [ms % ncount]
+    kat.current_stimulus(nb)
 
 
 def test_invalid_current_stimulus():
-    """testInvalidCurrentStimulus (src/test/test.cpp:271-284)"""
-    ncount = 1000
-    sim = nb.Simulation(nets.create_ring(nb, nb.Network(), ncount), nb.Configuration())
-    sim.step()
-    sim.step()
-    with pytest.raises(nb.NemoError) as e:
-        sim.step(istim=[(ncount + 1, 0.5)])
-    assert e.value.code == 6
+    kat.invalid_current_stimulus(nb)
 
 
 def test_fixed_point_saturation():
-    """testFixedPointSaturation (src/test/test.cpp:414-467), also bit-exact
-    against the oracle."""
-    def build(mod):
-        net = mod.Network()
-        iz = net.add_neuron_type("Izhikevich")
-        params = [0.02, 0.2, -65.0, 8.0, 0.0, -13.0, -65.0]
-        for n in range(5):
-            net.add_neuron(iz, n, *params)
-        INPUT0, INPUT1, OUT_SAT, OUT_REF, OUT_WEAK = range(5)
-        for s, t, w in [(INPUT0, OUT_REF, 1024.0), (INPUT1, OUT_REF, 1024.0), (INPUT0, OUT_WEAK, 1000.0),
-                        (INPUT1, OUT_WEAK, 1000.0), (INPUT0, OUT_SAT, 1100.0), (INPUT1, OUT_SAT, 1100.0)]:
-            net.add_synapse(s, t, 1, w, False)
-        return net
-    sims = [m.Simulation(build(m), m.Configuration()) for m in (nb, O)]
-    for sim in sims:
-        assert len(sim.step([0, 1])) == 2
-        assert len(sim.step()) == 3
-    u = [[sim.get_neuron_state(k, 0) for k in (3, 4, 2)] for sim in sims]
-    u_ref, u_weak, u_sat = u[0]
-    assert abs(u_ref - u_weak) > 1e-5
-    assert abs(u_ref - u_sat) < 1e-5
-    assert same_bits(u[0], u[1])
+    """... and bit-exact against the oracle"""
+    assert same_bits(kat.fixed_point_saturation(nb), kat.fixed_point_saturation(O))
 
 
 @pytest.mark.parametrize("n0,nstep", [(1, 1), (1000000, 1), (1, 4), (1000000, 4)])
 def test_non_contiguous_indices(n0, nstep):
-    """testNonContigousNeuronIndices (src/test/test.cpp:517-547)"""
-    ncount = 1000
-    s0 = nb.Simulation(nets.create_ring(nb, nb.Network(), ncount, 0, False, nstep), nb.Configuration())
-    s1 = nb.Simulation(nets.create_ring(nb, nb.Network(), ncount, n0, False, nstep), nb.Configuration())
-    f0 = s0.step([0])
-    f1 = s1.step([n0])
-    assert f0 == [0] and f1 == [n0]
-    for _ in range(1, 2000):
-        a, b = s0.step(), s1.step()
-        assert len(a) == len(b) == 1 and a[0] == b[0] - n0
+    kat.non_contiguous_indices(nb, n0, nstep)
 
 
 @pytest.mark.parametrize("iz_first", [True, False])
 def test_neuron_type_mixture(iz_first):
-    """testNeuronTypeMixture (src/test/test.cpp:369-410): a Poisson
-    population beside a ring must not disturb it; bit-exact with the oracle."""
-    def build(mod):
-        net = mod.Network()
-        if iz_first:
-            nets.create_ring(mod, net, 1024)
-        ps = net.add_neuron_type("PoissonSource")
-        net.add_neuron(ps, np.arange(1024, 1024 + 1000, dtype=np.uint32), 0.001)
-        if not iz_first:
-            nets.create_ring(mod, net, 1024)
-        return net
-    sp = nb.Simulation(build(nb), nb.Configuration())
-    so = O.Simulation(build(O), O.Configuration())
-    for ms in range(1000):
-        st = [0] if ms == 0 else None
-        a = sp.step(st)
-        b = so.step(st)
-        assert a == b
-        fired = sorted(a)
-        assert fired[0] == ms % 1024
-        assert all(f >= 1024 for f in fired[1:])
+    """... and the Poisson firing is bit-exact against the oracle"""
+    assert kat.neuron_type_mixture(nb, iz_first) == kat.neuron_type_mixture(O, iz_first)
 
 
-def test_poisson_rate():
-    """testRate (src/test/PoissonSource.cpp:11-31) plus oracle parity."""
-    for mod in (nb,):
-        net = mod.Network()
-        ps = net.add_neuron_type("PoissonSource")
-        net.add_neuron(ps, 0, 0.010)
-        sim = mod.Simulation(net, mod.Configuration())
-        counts, _, _ = sim.run(10000)
-        nfired = int(counts.sum())
-        expected = int(10000 * 0.010)
-        assert nfired > 0 and abs(nfired - expected) < 2 * expected
+@pytest.mark.parametrize("others", [False, True])
+def test_poisson_rate(others):
+    assert kat.poisson_rate(nb, 10000, others) == kat.poisson_rate(O, 10000, others)
 
 
 # ---------------------------------------------------------------------------
@@ -254,6 +153,35 @@ def test_mixed_plugins_bitexact():
         assert same_bits(sims[0].type_state(t, ns, n), sims[1].type_state(t, ns, n))
 
 
+@pytest.mark.parametrize("shape", [(32, 32), (64, 64), (96, 128), (256, 128), (1024, 256), (2048, 1024)])
+def test_launch_shape_does_not_change_results(shape):
+    """Any partition size / block size gives the same bit-exact results."""
+    ref = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
+    sim = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
+    sim.set_launch(*shape)
+    assert sim.launch()[0] == shape[0]
+    a = ref.run(300, 100, 1.0)
+    b = sim.run(300, 100, 1.0)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[2], b[2])
+    assert np.array_equal(ref.weights_fx(450000), sim.weights_fx(450000))
+
+
+def test_autotune_restores_state():
+    """The autotuner's trial steps leave the simulation exactly as it was."""
+    ref = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
+    sim = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
+    a0 = ref.run(150, 100, 1.0)
+    b0 = sim.run(150, 100, 1.0)
+    us = sim.autotune(20)
+    assert us > 0
+    a = ref.run(250, 100, 1.0)
+    b = sim.run(250, 100, 1.0)
+    assert np.array_equal(a0[2], b0[2])
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[2], b[2])
+    assert np.array_equal(ref.weights_fx(450000), sim.weights_fx(450000))
+    assert sim.elapsed_simulation() == ref.elapsed_simulation() == 400
+
+
 def test_stimulus_parity():
     """Firing and current stimulus on a noisy network, including duplicate
     current entries (the last one wins, src/nemo/cpu/Simulation.cpp:160-163)."""
@@ -268,48 +196,10 @@ def test_stimulus_parity():
         assert sp.step(fstim, istim) == so.step(fstim, istim)
 
 
-def test_stdp_analytic():
-    """testStdp (src/test/stdp.cpp:243-265): after each epoch every
-    one-to-one plastic synapse must have changed by epoch*reward*dw(dt)."""
-    group = 2 * 768
-    init_w = 5.0
-
-    def build(mod):
-        net = mod.Network()
-        iz = net.add_neuron_type("Izhikevich")
-        r = f32(0.5)
-        b = f32(f32(0.25) - f32(0.05) * r)
-        v = f32(-65.0)
-        for g in range(2):
-            net.add_neuron(iz, np.arange(g * group, (g + 1) * group, dtype=np.uint32),
-                           f32(f32(0.02) + f32(0.08) * r), b, v, 2.0, 0.0, f32(b * v), v)
-        loc = np.arange(group, dtype=np.uint32)
-        net.add_synapse(loc, group + loc, 1 + loc % 20, np.full(group, init_w, f32), np.ones(group, np.uint8))
-        return net
-
-    for reward in (1.0, 0.8):
-        sims = [m.Simulation(build(m), nets.stdp_test_configuration(m)) for m in (nb, O)]
-        for epoch in range(1, 5):
-            for ms in range(100):
-                fstim = None
-                if ms == 10:
-                    fstim = list(range(group))
-                elif ms == 20:
-                    fstim = list(range(group, 2 * group))
-                a = sims[0].step(fstim)
-                assert a == sims[1].step(fstim)
-            for s in sims:
-                s.apply_stdp(reward)
-            for local in range(0, group, 37):
-                sid = sims[0].get_synapses_from(local)[0]
-                d = sims[0].get_synapse_delay(sid)
-                assert d == 1 + local % 20
-                dt = -(10 - d)
-                dw = (-0.8 * np.exp(-(dt - 1) / 20.0)) if dt > 0 else (1.0 * np.exp(dt / 20.0))
-                expect = init_w + epoch * reward * dw
-                got = sims[0].get_synapse_weight(sid)
-                assert got == pytest.approx(expect, rel=1e-5)
-                assert got == sims[1].get_synapse_weight(sid)
+@pytest.mark.parametrize("reward", [1.0, 0.8, 0.9])
+def test_stdp_analytic(reward):
+    """testStdp (src/test/stdp.cpp:243-265) plus every weight equal to the oracle's"""
+    assert kat.stdp_analytic(nb, reward) == kat.stdp_analytic(O, reward)
 
 
 # ---------------------------------------------------------------------------
