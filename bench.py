@@ -277,10 +277,15 @@ def run_b200(args, rank, world, local):
     sim.run(W * kp, W, 1.0, ids=False)
     sim.set_profiling(False)
     ps = sim.run_stats()
-    launches = ps["kernel_launches"]["step"]
-    step_ms = ps["kernel_ms"]["step"] / max(1, launches)
-    alg_bytes = (args.neurons * B_NEURON * launches + ps["fired"] * B_FIRED + ps["events"] * B_EVENT
-                 + ps["stdp_entries"] * B_STDP) / max(1, launches)
+    nsteps_p = max(1, ps["kernel_launches"]["step"])
+    upd_ms = ps["kernel_ms"]["step"] / nsteps_p
+    dlv_ms = ps["kernel_ms"]["stdp"] / max(1, ps["kernel_launches"]["stdp"])
+    # algorithmic bytes per launch of each kernel of the step
+    upd_bytes = (args.neurons * B_NEURON * nsteps_p + ps["fired"] * B_FIRED) / nsteps_p
+    dlv_bytes = (ps["events"] * B_EVENT + ps["stdp_entries"] * B_STDP) / nsteps_p
+    kernels = {"update_kernel": (upd_bytes, upd_ms), "deliver_kernel": (dlv_bytes, dlv_ms)}
+    dominant = max(kernels, key=lambda k: kernels[k][1])
+    alg_bytes, step_ms = kernels[dominant]
     achieved = alg_bytes / (step_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak_gbs()
     apply_ms = ps["kernel_ms"]["apply"] / max(1, ps["kernel_launches"]["apply"])
@@ -289,10 +294,14 @@ def run_b200(args, rank, world, local):
     tfile = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
-            tj = json.load(f)
+            tj = json.load(f).get(dominant, {})
         # scale the captured bytes per launch to this run's per-launch work
         if tj.get("alg_bytes_per_launch"):
             traffic = tj["dram_bytes_per_launch"] * alg_bytes / tj["alg_bytes_per_launch"]
+    per_kernel = {k: {"alg_bytes_per_launch": v[0], "avg_launch_us": v[1] * 1e3,
+                      "achieved_gbs": v[0] / (v[1] / 1e3) / 1e9 if v[1] else None} for k, v in kernels.items()}
+    per_kernel["apply_kernel"] = {"avg_launch_us": apply_ms * 1e3, "achieved_gbs": apply_gbs,
+                                  "alg_bytes_per_launch": ps["plastic_synapses"] * B_APPLY}
 
     # e2e through the C ABI with host buffers
     rng = np.random.default_rng(rank)
@@ -331,14 +340,13 @@ def run_b200(args, rank, world, local):
             "sim_ms_per_s": sim_ms_per_s,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "step_kernel", "alg_bytes_per_launch": alg_bytes,
-                         "avg_launch_us": step_ms * 1e3,
-                         "apply_stdp_kernel": {"avg_launch_us": apply_ms * 1e3, "achieved_gbs": apply_gbs}},
+                         "kernel": dominant, "alg_bytes_per_launch": alg_bytes,
+                         "avg_launch_us": step_ms * 1e3, "kernels": per_kernel},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_events / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 4 * W,
                     "d2h_bytes_per_step": 4 * words * W, "api": "nemo_step + nemo_apply_stdp (C ABI)",
                     "sim_ms_per_s": ke * W / e2e_s},
-            "gpu_launches": args.steps * (W + 2),
+            "gpu_launches": args.steps * (2 * W + 1),
             "clocks": clk.summary(),
             "build_s": build_s,
             "launch": {"partition": launch[0], "threads": launch[1], "autotuned_us_per_step": tuned_us},

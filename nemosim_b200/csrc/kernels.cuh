@@ -171,4 +171,27 @@ __device__ __forceinline__ bool update_poisson(const DevSim& S, const TypeRange&
 	return p1 < p0 || fs;
 }
 
+// A weight that applyStdp changes was already scattered, with its old value,
+// for the spikes its source emitted k < delay steps before the last step and
+// that have not arrived yet.  The reference reads the weight on arrival
+// (deliverSpikesOne, src/nemo/cpu/Simulation.cpp:293-307), so move each such
+// contribution from the old weight's class (E if >= 0, else I) to the new
+// weight's class with the new value.
+__device__ __forceinline__ void compensate_inflight(const DevSim& S, const uint64_t* hist, uint32_t sd,
+		uint32_t tgt, uint32_t slot, int32_t w, int32_t nw)
+{
+	const uint32_t src = sd & (MAX_NEURONS - 1);
+	const uint32_t delay = (sd >> 26) + 1;
+	uint64_t inflight = hist[src] & ((delay >= 64) ? ~0ull : ((1ull << delay) - 1ull));
+	while(inflight) {
+		const uint32_t k = __ffsll((long long) inflight) - 1;
+		inflight &= inflight - 1;
+		// emitted k steps before the last step, arrives delay - k steps after it
+		const uint32_t sl = (slot + delay - k) % S.D;
+		unsigned long long* a = reinterpret_cast<unsigned long long*>(S.slots + (size_t) sl * S.N + tgt);
+		atomicAdd(a + (w < 0 ? 1 : 0), (unsigned long long) (-(long long) w));
+		atomicAdd(a + (nw < 0 ? 1 : 0), (unsigned long long) (long long) nw);
+	}
+}
+
 } // namespace nemo_b200

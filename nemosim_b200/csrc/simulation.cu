@@ -23,197 +23,85 @@ namespace nemo_b200 {
 // ---------------------------------------------------------------------------
 // kernels
 
-// Shared-memory work list of one CTA: the items (fired neurons or STDP
-// targets) it collected, each with a span of consecutive entries of a CSR
-// array (outgoing synapses or incoming plastic synapses).  off[] is the
-// exclusive prefix sum of the span lengths and adj[i] = start(i) - off[i],
-// so flat work item k of the CTA is entry adj[i] + k for the i whose span
-// contains k.  Spreading all spans over all threads of the CTA keeps every
-// thread's loads independent of the item sizes.
-struct WorkList {
-	uint32_t* item;               // [cap]
-	uint32_t* off;                // [cap + 1]
-	unsigned long long* adj;      // [cap]
-};
+// The step is two launches.  update_kernel advances every neuron and, for
+// each fired neuron and each STDP target, publishes the CSR span of work it
+// implies (its outgoing synapses; its incoming plastic synapses) as chunks of
+// at most CHUNK entries in a global list.  deliver_kernel then spreads those
+// chunks over all warps of the GPU.  The work of a step is therefore balanced
+// across the device however the spikes fall, and every lane keeps ILP
+// independent loads in flight.
 
-__device__ __forceinline__ WorkList carve_list(unsigned char*& p, uint32_t cap)
-{
-	WorkList w;
-	w.adj = reinterpret_cast<unsigned long long*>(p);
-	p += 8 * (size_t) cap;
-	w.item = reinterpret_cast<uint32_t*>(p);
-	p += 4 * (size_t) cap;
-	w.off = reinterpret_cast<uint32_t*>(p);
-	p += 4 * (size_t) (cap + 1);
-	p = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 15) & ~uintptr_t(15));
-	return w;
-}
+constexpr uint32_t CHUNK = 128;  // entries per chunk: 4 per lane of a warp
+constexpr uint32_t ILP = CHUNK / 32;
 
-// Block-wide exclusive scan of the span lengths ptr[item+1] - ptr[item] of
-// the n collected items; returns the total.  All threads must call it.
-__device__ uint32_t build_offsets(const WorkList& L, uint32_t n, const unsigned long long* ptr, uint32_t* warpTmp)
-{
-	const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-	uint32_t carry = 0;
-	for(uint32_t base = 0; base < n; base += blockDim.x) {
-		const uint32_t i = base + tid;
-		unsigned long long b = 0;
-		uint32_t c = 0;
-		if(i < n) {
-			const uint32_t it = L.item[i];
-			b = ptr[it];
-			c = (uint32_t) (ptr[it + 1] - b);
-		}
-		uint32_t x = c;
-#pragma unroll
-		for(int o = 1; o < 32; o <<= 1) {
-			uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-			if(lane >= (uint32_t) o) x += y;
-		}
-		if(lane == 31) warpTmp[warp] = x;
-		__syncthreads();
-		if(warp == 0) {
-			uint32_t s = lane < nwarps ? warpTmp[lane] : 0;
-#pragma unroll
-			for(int o = 1; o < 32; o <<= 1) {
-				uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
-				if(lane >= (uint32_t) o) s += y;
-			}
-			warpTmp[lane] = s;
-		}
-		__syncthreads();
-		const uint32_t o = carry + (warp ? warpTmp[warp - 1] : 0) + x - c;
-		if(i < n) {
-			L.off[i] = o;
-			L.adj[i] = b - o;
-		}
-		carry += warpTmp[nwarps - 1];
-		__syncthreads();
-	}
-	if(threadIdx.x == 0) L.off[n] = carry;
-	__syncthreads();
-	return carry;
-}
-
-// the item whose span holds flat work item k: largest i < n with off[i] <= k
-__device__ __forceinline__ uint32_t find_item(const uint32_t* off, uint32_t n, uint32_t k)
-{
-	uint32_t lo = 0, hi = n;
-	while(hi - lo > 1) {
-		uint32_t mid = (lo + hi) >> 1;
-		if(off[mid] <= k) lo = mid; else hi = mid;
-	}
-	return lo;
-}
-
-constexpr uint32_t ILP = 4;
-
-// scatter: add every outgoing synapse of the CTA's fired neurons into the
-// accumulator slot of its arrival step (64-bit integer atomics)
-__device__ __forceinline__ void scatter_phase(const DevSim& S, const WorkList& L, uint32_t n, uint32_t total, uint32_t slot)
-{
-	const uint32_t T = blockDim.x;
-	for(uint32_t k0 = threadIdx.x; k0 < total; k0 += ILP * T) {
-		uint2 s[ILP];
-#pragma unroll
-		for(uint32_t j = 0; j < ILP; ++j) {
-			const uint32_t k = k0 + j * T;
-			if(k < total) {
-				const uint32_t i = find_item(L.off, n, k);
-				s[j] = S.syn[L.adj[i] + k];
-			}
-		}
-#pragma unroll
-		for(uint32_t j = 0; j < ILP; ++j) {
-			if(k0 + j * T < total) {
-				uint32_t d = (s[j].x >> 26) + 1;
-				uint32_t sl = slot + d;
-				sl = sl >= S.D ? sl - S.D : sl;
-				add_current(S.slots + (size_t) sl * S.N + (s[j].x & (MAX_NEURONS - 1)), (int32_t) s[j].y);
-			}
-		}
-	}
-}
-
-// STDP accumulation over the incoming plastic synapses of the CTA's targets
-// (ConnectivityMatrix::accumulateStdp, src/nemo/ConnectivityMatrix.cpp:193-227)
-__device__ __forceinline__ void stdp_phase(const DevSim& S, const WorkList& L, uint32_t n, uint32_t total,
-		const uint64_t* hist)
-{
-	const uint32_t T = blockDim.x;
-	for(uint32_t k0 = threadIdx.x; k0 < total; k0 += ILP * T) {
-		unsigned long long p[ILP];
-		uint32_t sd[ILP];
-		int32_t acc[ILP];
-		uint64_t h[ILP];
-#pragma unroll
-		for(uint32_t j = 0; j < ILP; ++j) {
-			const uint32_t k = k0 + j * T;
-			if(k < total) {
-				const uint32_t i = find_item(L.off, n, k);
-				p[j] = L.adj[i] + k;
-				sd[j] = S.rcmSrc[p[j]];
-				acc[j] = S.rcmAcc[p[j]];
-			}
-		}
-#pragma unroll
-		for(uint32_t j = 0; j < ILP; ++j) {
-			if(k0 + j * T < total) h[j] = hist[sd[j] & (MAX_NEURONS - 1)];
-		}
-#pragma unroll
-		for(uint32_t j = 0; j < ILP; ++j) {
-			if(k0 + j * T < total) {
-				const uint32_t delay = (sd[j] >> 26) + 1;
-				int32_t dw = stdp_weight_change(S.sp, h[j] >> (delay & 63));
-				if(dw != 0) S.rcmAcc[p[j]] = (int32_t) ((uint32_t) acc[j] + (uint32_t) dw);
-			}
-		}
-	}
-}
-
-// warp-aggregated append of the lanes whose flag is set
-__device__ __forceinline__ void append(uint32_t* list, uint32_t* count, bool flag, uint32_t value)
+__device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t x)
 {
 	const uint32_t lane = threadIdx.x & 31;
-	const uint32_t b = __ballot_sync(0xffffffffu, flag);
-	if(!b) return;
-	uint32_t base = 0;
-	if(lane == 0) base = atomicAdd(count, (uint32_t) __popc(b));
-	base = __shfl_sync(0xffffffffu, base, 0);
-	if(flag) list[base + __popc(b & ((1u << lane) - 1u))] = value;
+#pragma unroll
+	for(int o = 1; o < 32; o <<= 1) {
+		uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+		if(lane >= (uint32_t) o) x += y;
+	}
+	return x;
 }
 
-// One simulation step (see kernels.cuh).  CTA c owns the partition of P
-// consecutive neurons starting at c * P (P a multiple of 32, so warps cover
-// whole bit-vector words); its blockDim.x threads loop over them.
-__global__ void __launch_bounds__(1024)
-step_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t slot, uint32_t ring, int stdpPrev)
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long x)
 {
-	extern __shared__ __align__(16) unsigned char smem[];
-	__shared__ uint32_t sNF, sNS, warpTmp[32];
+#pragma unroll
+	for(int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+	return x;
+}
 
+// Reserve nch chunk slots per lane in a global list (one atomic per warp);
+// returns this lane's first slot.
+__device__ __forceinline__ uint32_t reserve_chunks(uint32_t* counter, uint32_t nch)
+{
+	const uint32_t incl = warp_inclusive_scan(nch);
+	const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+	uint32_t base = 0;
+	if(total && (threadIdx.x & 31) == 31) base = atomicAdd(counter, total);
+	base = __shfl_sync(0xffffffffu, base, 31);
+	return base + incl - nch;
+}
+
+__device__ __forceinline__ void write_chunks(uint4* list, uint32_t pos, unsigned long long start,
+		uint32_t count, uint32_t nch, uint32_t tag)
+{
+	for(uint32_t j = 0; j < nch; ++j) {
+		const unsigned long long s = start + (unsigned long long) j * CHUNK;
+		list[pos + j] = make_uint4((uint32_t) s, (uint32_t) (s >> 32), min(CHUNK, count - j * CHUNK), tag);
+	}
+}
+
+// Neuron update of one step (src/nemo/cpu/Simulation.cpp:94-111 minus the
+// delivery and STDP loops).  CTA c owns the partition of P consecutive
+// neurons starting at c * P (P a multiple of 32, so warps cover whole
+// bit-vector words); its blockDim.x threads loop over them.
+__global__ void __launch_bounds__(1024)
+update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t slot, uint32_t ring)
+{
+	__shared__ uint32_t sFired;
+	__shared__ unsigned long long sEvents, sStdp;
 	const uint32_t tid = threadIdx.x, lane = tid & 31;
 	const uint32_t first = blockIdx.x * P;
 	const uint32_t last = min(S.N, first + P);
 	const uint64_t* histPrev = S.hist + (size_t) (cur ^ 1u) * S.N;
 	uint64_t* histCur = S.hist + (size_t) cur * S.N;
-	unsigned char* sp = smem;
-	WorkList LF = carve_list(sp, P);
-	WorkList LS = carve_list(sp, P);
-
-	if(tid == 0) { sNF = 0; sNS = 0; }
+	if(tid == 0) { sFired = 0; sEvents = 0; sStdp = 0; }
 	__syncthreads();
 
-	// 1-3: read-out, update, history, fired bit-vector, compaction
 	for(uint32_t base = first; base < last; base += blockDim.x) {
 		const uint32_t n = base + tid;
-		bool fired = false, stdpTarget = false;
-		uint32_t fw = 0;
+		bool fired = false, target = false;
+		uint32_t fw = 0, outdeg = 0, indeg = 0;
+		unsigned long long ob = 0, rb = 0;
 		if(n < last) {
 			uint32_t k = 0;
 			while(k + 1 < S.ntypes && n >= S.types[k + 1].base) ++k;
 			const TypeRange& T = S.types[k];
 			const uint32_t nl = n - T.base;
+			// this step's synaptic input (deliverSpikes + wfx_toFloat,
+			// src/nemo/cpu/Simulation.cpp:259-288)
 			float cE = 0.0f, cI = 0.0f;
 			if(S.D) {
 				longlong2* a = S.slots + (size_t) slot * S.N + n;
@@ -232,67 +120,167 @@ step_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t slot, uint32_t ri
 				case KIND_POISSON: fired = update_poisson(S, T, nl, n, fs); break;
 				default: fired = fs; break; // Input, src/nemo/cpu/plugins/Input.cpp:17-22
 			}
-			const uint64_t h = histPrev[n];
-			histCur[n] = (h << 1) | (uint64_t) fired;
-			stdpTarget = stdpPrev && (h & S.sp.postFireMask) && S.rcmPtr[n + 1] > S.rcmPtr[n];
+			const uint64_t h = (histPrev[n] << 1) | (uint64_t) fired;
+			histCur[n] = h;
+			if(fired) {
+				ob = S.outPtr[n];
+				outdeg = (uint32_t) (S.outPtr[n + 1] - ob);
+			}
+			// STDP target: fired |post| steps ago (ConnectivityMatrix.cpp:206)
+			if(S.stdp && (h & S.sp.postFireMask)) {
+				rb = S.rcmPtr[n];
+				indeg = (uint32_t) (S.rcmPtr[n + 1] - rb);
+				target = indeg > 0;
+			}
 		}
 		const uint32_t fb = __ballot_sync(0xffffffffu, fired);
 		if(lane == 0 && n < last) {
 			S.firedRing[(size_t) ring * S.W + (n >> 5)] = fb;
 			if(fw) S.fstim[n >> 5] = 0u;
 		}
-		append(LF.item, &sNF, fired, n);
-		append(LS.item, &sNS, stdpTarget, n);
+		// delivery and STDP chunks of this step
+		const uint32_t nchF = (fired && S.D) ? (outdeg + CHUNK - 1) / CHUNK : 0;
+		const uint32_t nchS = target ? (indeg + CHUNK - 1) / CHUNK : 0;
+		if(__any_sync(0xffffffffu, nchF + nchS != 0)) {
+			const uint32_t pos = reserve_chunks(&S.chunkCount[cur], nchF + nchS);
+			write_chunks(S.chunks, pos, ob, outdeg, nchF, 0u);
+			write_chunks(S.chunks, pos + nchF, rb, indeg, nchS, 1u);
+		}
+		// targets touched in this STDP period, for applyStdp
+		const uint32_t tb = __ballot_sync(0xffffffffu, target);
+		if(tb) {
+			uint32_t old = 0;
+			if(lane == 0) old = atomicOr(&S.touchedBits[n >> 5], tb);
+			old = __shfl_sync(0xffffffffu, old, 0);
+			const bool fresh = target && !((old >> lane) & 1u);
+			const uint32_t nchA = fresh ? (indeg + CHUNK - 1) / CHUNK : 0;
+			if(__any_sync(0xffffffffu, fresh)) {
+				const uint32_t pos = reserve_chunks(S.applyChunkCount, nchA);
+				write_chunks(S.applyChunks, pos, rb, indeg, nchA, n);
+			}
+		}
+		if(fb) {
+			const unsigned long long ev = warp_sum(fired ? outdeg : 0);
+			if(lane == 0) {
+				atomicAdd(&sFired, (uint32_t) __popc(fb));
+				atomicAdd(&sEvents, ev);
+			}
+		}
+		if(tb) {
+			const unsigned long long se = warp_sum(target ? indeg : 0);
+			if(lane == 0) atomicAdd(&sStdp, se);
+		}
 	}
 	__syncthreads();
-	const uint32_t nf = sNF, ns = sNS;
-
-	// 4. scatter, 5. STDP of the previous step
-	const uint32_t wf = nf ? build_offsets(LF, nf, S.outPtr, warpTmp) : 0;
-	const uint32_t ws = ns ? build_offsets(LS, ns, S.rcmPtr, warpTmp) : 0;
-	if(S.D && wf) scatter_phase(S, LF, nf, wf, slot);
-	if(ws) stdp_phase(S, LS, ns, ws, histPrev);
-
 	if(tid == 0) {
-		if(nf) atomicAdd(&S.firedCount[ring], nf);
-		if(wf) atomicAdd(&S.eventCount[ring], (unsigned long long) wf);
-		if(ws) atomicAdd(&S.stdpCount[ring], (unsigned long long) ws);
+		if(sFired) atomicAdd(&S.firedCount[ring], sFired);
+		if(sEvents) atomicAdd(&S.eventCount[ring], sEvents);
+		if(sStdp) atomicAdd(&S.stdpCount[ring], sStdp);
 	}
 }
 
-// Pending STDP accumulation of the last completed step (history buffer `par`)
-__global__ void __launch_bounds__(1024)
-stdp_kernel(const DevSim S, uint32_t P, uint32_t par, uint32_t ring)
-{
-	extern __shared__ __align__(16) unsigned char smem[];
-	__shared__ uint32_t sNS, warpTmp[32];
-	const uint32_t tid = threadIdx.x;
-	const uint32_t first = blockIdx.x * P;
-	const uint32_t last = min(S.N, first + P);
-	const uint64_t* hist = S.hist + (size_t) par * S.N;
-	unsigned char* sp = smem;
-	WorkList LS = carve_list(sp, P);
-	if(tid == 0) sNS = 0;
-	__syncthreads();
-	for(uint32_t base = first; base < last; base += blockDim.x) {
-		const uint32_t n = base + tid;
-		bool target = n < last && (hist[n] & S.sp.postFireMask) && S.rcmPtr[n + 1] > S.rcmPtr[n];
-		append(LS.item, &sNS, target, n);
-	}
-	__syncthreads();
-	const uint32_t ns = sNS;
-	const uint32_t ws = ns ? build_offsets(LS, ns, S.rcmPtr, warpTmp) : 0;
-	if(ws) stdp_phase(S, LS, ns, ws, hist);
-	if(tid == 0 && ws) atomicAdd(&S.stdpCount[ring], (unsigned long long) ws);
-}
-
-// applyStdp (src/nemo/ConnectivityMatrix.cpp:241-294): one warp per target,
-// lanes over its incoming plastic synapses.  A weight that changes is
-// written back to the forward matrix, and the spikes already scattered with
-// the old weight but not yet arrived (source fired k < delay steps ago) are
-// corrected in their accumulator slots.
+// Delivery and STDP accumulation of one step over the published chunks.
+// One warp per chunk; lane l handles entries l, l + 32, l + 64, l + 96.
+//  kind 0: add each outgoing synapse into the accumulator slot of its
+//          arrival step (64-bit integer atomics: order-independent sums)
+//  kind 1: STDP accumulation over the incoming plastic synapses of a target
+//          (ConnectivityMatrix::accumulateStdp, ConnectivityMatrix.cpp:193-227)
 __global__ void __launch_bounds__(STEP_THREADS)
-apply_stdp_kernel(const DevSim S, int32_t reward, uint32_t par, uint32_t slot, int fullPass)
+deliver_kernel(const DevSim S, uint32_t cur, uint32_t slot)
+{
+	const uint32_t nch = S.chunkCount[cur];
+	if(blockIdx.x == 0 && threadIdx.x == 0) S.chunkCount[cur ^ 1u] = 0; // next step's list starts empty
+	const uint32_t lane = threadIdx.x & 31;
+	const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+	const uint64_t* hist = S.hist + (size_t) cur * S.N;
+	for(uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nch; c += nw) {
+		const uint4 d = S.chunks[c];
+		const unsigned long long start = (unsigned long long) d.x | ((unsigned long long) d.y << 32);
+		const uint32_t len = d.z;
+		if(d.w == 0) {
+			uint2 s[ILP];
+#pragma unroll
+			for(uint32_t j = 0; j < ILP; ++j) {
+				if(lane + 32 * j < len) s[j] = S.syn[start + lane + 32 * j];
+			}
+#pragma unroll
+			for(uint32_t j = 0; j < ILP; ++j) {
+				if(lane + 32 * j < len) {
+					uint32_t sl = slot + (s[j].x >> 26) + 1;
+					sl = sl >= S.D ? sl - S.D : sl;
+					add_current(S.slots + (size_t) sl * S.N + (s[j].x & (MAX_NEURONS - 1)), (int32_t) s[j].y);
+				}
+			}
+		} else {
+			uint32_t sd[ILP];
+			int32_t acc[ILP];
+			uint64_t h[ILP];
+#pragma unroll
+			for(uint32_t j = 0; j < ILP; ++j) {
+				if(lane + 32 * j < len) {
+					sd[j] = S.rcmSrc[start + lane + 32 * j];
+					acc[j] = S.rcmAcc[start + lane + 32 * j];
+				}
+			}
+#pragma unroll
+			for(uint32_t j = 0; j < ILP; ++j) {
+				if(lane + 32 * j < len) h[j] = hist[sd[j] & (MAX_NEURONS - 1)];
+			}
+#pragma unroll
+			for(uint32_t j = 0; j < ILP; ++j) {
+				if(lane + 32 * j < len) {
+					const uint32_t delay = (sd[j] >> 26) + 1;
+					const int32_t dw = stdp_weight_change(S.sp, h[j] >> (delay & 63));
+					if(dw != 0) S.rcmAcc[start + lane + 32 * j] = (int32_t) ((uint32_t) acc[j] + (uint32_t) dw);
+				}
+			}
+		}
+	}
+}
+
+// applyStdp over the targets touched since the last call (their incoming
+// plastic synapses are the only ones with a nonzero accumulator).  One warp
+// per chunk; d.w of an apply chunk is its target.
+__global__ void __launch_bounds__(STEP_THREADS)
+apply_touched_kernel(const DevSim S, int32_t reward, uint32_t par, uint32_t slot)
+{
+	const uint32_t nch = *S.applyChunkCount;
+	const uint32_t lane = threadIdx.x & 31;
+	const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+	const uint64_t* hist = S.hist + (size_t) par * S.N;
+	for(uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nch; c += nw) {
+		const uint4 d = S.applyChunks[c];
+		const unsigned long long start = (unsigned long long) d.x | ((unsigned long long) d.y << 32);
+		const uint32_t len = d.z, tgt = d.w;
+		int32_t acc[ILP];
+		uint32_t fwd[ILP];
+		int32_t w[ILP];
+#pragma unroll
+		for(uint32_t j = 0; j < ILP; ++j) acc[j] = lane + 32 * j < len ? S.rcmAcc[start + lane + 32 * j] : 0;
+#pragma unroll
+		for(uint32_t j = 0; j < ILP; ++j) if(acc[j]) fwd[j] = S.rcmFwd[start + lane + 32 * j];
+#pragma unroll
+		for(uint32_t j = 0; j < ILP; ++j) if(acc[j]) w[j] = (int32_t) S.syn[fwd[j]].y;
+#pragma unroll
+		for(uint32_t j = 0; j < ILP; ++j) {
+			if(!acc[j]) continue;
+			const unsigned long long p = start + lane + 32 * j;
+			const int32_t nw2 = stdp_updated_weight(S.sp, w[j], fx_mul_dev(reward, acc[j]));
+			if(nw2 != w[j]) {
+				S.syn[fwd[j]].y = (uint32_t) nw2;
+				if(S.D) compensate_inflight(S, hist, S.rcmSrc[p], tgt, slot, w[j], nw2);
+			}
+			S.rcmAcc[p] = 0;
+		}
+	}
+}
+
+// applyStdp (src/nemo/ConnectivityMatrix.cpp:241-294), first call: one warp
+// per target over every incoming plastic synapse, so that weights that
+// start outside their clamp range are clamped as in the reference.  Later
+// calls use apply_touched_kernel.
+__global__ void __launch_bounds__(STEP_THREADS)
+apply_full_kernel(const DevSim S, int32_t reward, uint32_t par, uint32_t slot)
 {
 	const uint32_t lane = threadIdx.x & 31;
 	const uint32_t warpsTotal = gridDim.x * (STEP_THREADS / 32);
@@ -300,34 +288,13 @@ apply_stdp_kernel(const DevSim S, int32_t reward, uint32_t par, uint32_t slot, i
 	for(uint32_t tgt = blockIdx.x * (STEP_THREADS / 32) + (threadIdx.x >> 5); tgt < S.N; tgt += warpsTotal) {
 		unsigned long long b = S.rcmPtr[tgt], e = S.rcmPtr[tgt + 1];
 		for(unsigned long long p = b + lane; p < e; p += 32) {
-			int32_t acc = S.rcmAcc[p];
-			// Once every plastic weight lies within its clamp range (after the
-			// first pass), a zero accumulator leaves the weight unchanged:
-			// updatedWeight(w, 0) == w.
-			if(acc == 0 && !fullPass) continue;
-			uint32_t fwd = S.rcmFwd[p];
-			int32_t w = (int32_t) S.syn[fwd].y;
-			int32_t nw = stdp_updated_weight(S.sp, w, fx_mul_dev(reward, acc));
+			const int32_t acc = S.rcmAcc[p];
+			const uint32_t fwd = S.rcmFwd[p];
+			const int32_t w = (int32_t) S.syn[fwd].y;
+			const int32_t nw = stdp_updated_weight(S.sp, w, fx_mul_dev(reward, acc));
 			if(nw != w) {
 				S.syn[fwd].y = (uint32_t) nw;
-				if(S.D) {
-					uint32_t sd = S.rcmSrc[p];
-					uint32_t src = sd & (MAX_NEURONS - 1);
-					uint32_t delay = (sd >> 26) + 1;
-					uint64_t inflight = hist[src] & ((delay >= 64) ? ~0ull : ((1ull << delay) - 1ull));
-					while(inflight) {
-						uint32_t k = __ffsll((long long) inflight) - 1;
-						inflight &= inflight - 1;
-						// fired k steps before the last step, arrives delay - k steps after it
-						uint32_t sl = (slot + delay - k) % S.D;
-						unsigned long long* a = reinterpret_cast<unsigned long long*>(S.slots + (size_t) sl * S.N + tgt);
-						// remove the old weight from its class (E if >= 0, else I) and
-						// add the new one to its class (deliverSpikesOne,
-						// src/nemo/cpu/Simulation.cpp:297-300)
-						atomicAdd(a + (w < 0 ? 1 : 0), (unsigned long long) (-(long long) w));
-						atomicAdd(a + (nw < 0 ? 1 : 0), (unsigned long long) (long long) nw);
-					}
-				}
+				if(S.D) compensate_inflight(S, hist, S.rcmSrc[p], tgt, slot, w, nw);
 			}
 			if(acc) S.rcmAcc[p] = 0;
 		}
@@ -628,6 +595,21 @@ Simulation::Simulation(const Network& net, const Configuration& conf)
 	auto* dRcmPtr = dalloc<unsigned long long>(N + 1);
 	NB_CUDA(cudaMemcpyAsync(dRcmPtr, rcmPtr.data(), (N + 1) * 8, cudaMemcpyHostToDevice, m_stream));
 	S.rcmPtr = dRcmPtr;
+	// chunk lists: enough for every neuron firing and being an STDP target
+	// in the same step
+	{
+		const uint64_t CH = 128;
+		uint64_t capF = 0, capS = 0;
+		for(unsigned n = 0; n < N; ++n) {
+			capF += (outPtr[n + 1] - outPtr[n] + CH - 1) / CH;
+			capS += (rcmPtr[n + 1] - rcmPtr[n] + CH - 1) / CH;
+		}
+		if(capF + capS >= (1ull << 32)) NB_THROW(NEMO_API_UNSUPPORTED, "network too large for the chunk lists");
+		S.chunks = dalloc<uint4>(capF + capS);
+		S.chunkCount = dalloc<uint32_t>(2);
+		S.applyChunks = dalloc<uint4>(capS);
+		S.applyChunkCount = dalloc<uint32_t>(1);
+	}
 
 	// per-neuron RNG, keyed by local index (src/nemo/cpu/Neurons.cpp:41)
 	std::vector<uint32_t> planes;
@@ -637,6 +619,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf)
 
 	S.hist = dalloc<uint64_t>(2 * (size_t) N);
 	S.fstim = dalloc<uint32_t>(S.W);
+	S.touchedBits = dalloc<uint32_t>(S.W);
 	S.curExt = dalloc<float>(N);
 	// validSpikes = ~(~0 << maxDelay) with x86 shift semantics
 	// (src/nemo/cpu/Simulation.cpp:263): nothing is delivered when the
@@ -652,8 +635,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf)
 
 	if(needCalib) S.calib = device_calibration(m_device);
 	NB_CUDA(cudaDeviceGetAttribute(&m_sms, cudaDevAttrMultiProcessorCount, m_device));
-	NB_CUDA(cudaFuncSetAttribute(step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) stepSmem(MAX_PARTITION)));
-	NB_CUDA(cudaFuncSetAttribute(stdp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) stepSmem(MAX_PARTITION)));
+	m_deliverGrid = (unsigned) m_sms * 8;
 	// default launch shape: two partitions per SM
 	{
 		uint32_t P = (uint32_t) ((N + 2 * m_sms - 1) / (2 * m_sms));
@@ -715,12 +697,6 @@ void Simulation::timedEnd()
 	NB_CUDA(cudaEventRecord(m_evPool[m_evUse.back().second + 1], m_stream));
 }
 
-size_t Simulation::stepSmem(uint32_t P) const
-{
-	size_t list = ((size_t) 8 * P + 4 * P + 4 * (P + 1) + 15) & ~(size_t) 15;
-	return 2 * list;
-}
-
 void Simulation::setLaunch(uint32_t P, uint32_t T)
 {
 	P = std::max<uint32_t>(32, std::min<uint32_t>(MAX_PARTITION, (P + 31) & ~31u));
@@ -738,9 +714,11 @@ void Simulation::launchStep(bool /*fullRecord*/)
 	const uint32_t ring = (uint32_t) (m_cycle % m_dev.R);
 	const unsigned grid = (m_N + m_P - 1) / m_P;
 	timedBegin(K_STEP);
-	step_kernel<<<grid, m_T, stepSmem(m_P), m_stream>>>(m_dev, m_P, cur, slot, ring, m_stdpPending ? 1 : 0);
+	update_kernel<<<grid, m_T, 0, m_stream>>>(m_dev, m_P, cur, slot, ring);
 	timedEnd();
-	m_stdpPending = m_dev.stdp != 0;
+	timedBegin(K_STDP);
+	deliver_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, cur, slot);
+	timedEnd();
 	m_cycle++;
 	m_timerSteps++;
 }
@@ -806,34 +784,27 @@ const std::vector<unsigned>& Simulation::step(const unsigned* fstim, size_t nf,
 	return m_fired;
 }
 
-void Simulation::flushStdp()
-{
-	if(!m_stdpPending) return;
-	const uint32_t par = (uint32_t) ((m_cycle - 1) & 1);
-	const unsigned grid = (m_N + m_P - 1) / m_P;
-	timedBegin(K_STDP);
-	stdp_kernel<<<grid, m_T, stepSmem(m_P) / 2, m_stream>>>(m_dev, m_P, par, (uint32_t) ((m_cycle - 1) % m_dev.R));
-	timedEnd();
-	m_stdpPending = false;
-}
-
 void Simulation::applyStdpDevice(int32_t R)
 {
-	flushStdp();
 	// the last completed step's history and slot; before the first step
 	// the history is all zero, so nothing is in flight
 	const uint64_t last = m_cycle ? m_cycle - 1 : 0;
 	const uint32_t par = (uint32_t) (last & 1);
 	const uint32_t slot = m_dev.D ? (uint32_t) (last % m_dev.D) : 0;
-	int sms = 148;
-	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m_device);
-	unsigned grid = std::min<unsigned>((m_N + 7) / 8, (unsigned) sms * 8);
 	timedBegin(K_APPLY);
-	apply_stdp_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, R, par, slot, m_weightsClamped ? 0 : 1);
+	if(!m_weightsClamped) {
+		unsigned grid = std::min<unsigned>((m_N + 7) / 8, (unsigned) m_sms * 8);
+		apply_full_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, R, par, slot);
+	} else {
+		apply_touched_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, R, par, slot);
+	}
 	timedEnd();
 	// updatedWeight's result always lies within the clamp range of its sign
-	// class, so after one full pass every plastic weight does
+	// class, so after one full pass every plastic weight does, and only the
+	// synapses of touched targets can change
 	m_weightsClamped = true;
+	NB_CUDA(cudaMemsetAsync(m_dev.applyChunkCount, 0, 4, m_stream));
+	NB_CUDA(cudaMemsetAsync(m_dev.touchedBits, 0, (size_t) m_dev.W * 4, m_stream));
 }
 
 /* ConnectivityMatrix::applyStdp argument checks (src/nemo/ConnectivityMatrix.cpp:241-259) */
@@ -950,6 +921,9 @@ float Simulation::autotune(unsigned trialSteps)
 	regions.emplace_back(m_dev.curExt, (size_t) m_N * 4);
 	if(m_dev.D) regions.emplace_back(m_dev.slots, (size_t) m_dev.D * m_N * 16);
 	if(m_dev.stdp) regions.emplace_back(m_dev.rcmAcc, (size_t) lastPlastic * 4);
+	regions.emplace_back(m_dev.chunkCount, 8);
+	regions.emplace_back(m_dev.applyChunkCount, 4);
+	regions.emplace_back(m_dev.touchedBits, (size_t) m_dev.W * 4);
 	std::vector<void*> backup;
 	for(auto& r : regions) {
 		void* p = nullptr;
@@ -963,7 +937,6 @@ float Simulation::autotune(unsigned trialSteps)
 		backup.push_back(p);
 	}
 	const uint64_t cycle = m_cycle;
-	const bool pending = m_stdpPending;
 	const unsigned long timerSteps = m_timerSteps;
 	const bool prof = profiling;
 	profiling = false;
@@ -974,7 +947,6 @@ float Simulation::autotune(unsigned trialSteps)
 			}
 		}
 		m_cycle = cycle;
-		m_stdpPending = pending;
 		m_timerSteps = timerSteps;
 	};
 

@@ -61,6 +61,15 @@ struct DevSim {
 	const uint32_t* rcmSrc;   // source | (delay - 1) << 26
 	const uint32_t* rcmFwd;   // index into syn
 	int32_t* rcmAcc;          // STDP accumulator per incoming plastic synapse
+	// work of the current step, published by update_kernel for deliver_kernel:
+	// {start lo, start hi, length <= 128, 0 = outgoing synapses | 1 = STDP}
+	uint4* chunks;
+	uint32_t* chunkCount;     // [2] by step parity
+	// incoming plastic synapses of the targets touched since the last
+	// applyStdp: {start lo, start hi, length, target}
+	uint4* applyChunks;
+	uint32_t* applyChunkCount;
+	uint32_t* touchedBits;    // [W]
 	StdpParams sp;
 	LibmCalib calib;
 };
@@ -99,7 +108,7 @@ public:
 
 	// timing of the last run(): whole run and, when profiling is on, each
 	// kernel kind (CUDA events around every launch)
-	enum { K_STEP = 0, K_STDP = 1, K_APPLY = 2, K_KINDS = 3 };
+	enum { K_STEP = 0, K_STDP = 1, K_APPLY = 2, K_KINDS = 3 };  // update, deliver, applyStdp
 	float lastRunMs = 0;
 	float kernelMs[K_KINDS] = {0, 0, 0};
 	unsigned kernelLaunches[K_KINDS] = {0, 0, 0};
@@ -130,11 +139,10 @@ private:
 	void locate(unsigned g, const HostType** t, unsigned* i) const;
 	size_t synapseKey(uint64_t id) const;
 	void launchStep(bool fullRecord);
-	size_t stepSmem(uint32_t P) const;
+	unsigned m_deliverGrid = 1184;
 	uint32_t m_P = 256, m_T = 256;
 	uint32_t m_maxOutDeg = 0, m_maxPlasticInDeg = 0;
 	int m_sms = 148;
-	void flushStdp();
 	void applyStdpDevice(int32_t fxReward);
 	void sync();
 
@@ -163,7 +171,6 @@ private:
 
 	// step state
 	uint64_t m_cycle = 0;        // steps since creation (never reset)
-	bool m_stdpPending = false;  // STDP accumulation of step m_cycle-1 not yet run
 	bool m_weightsClamped = false; // every plastic weight within its STDP limits
 	unsigned long m_timerSteps = 0;
 	std::chrono::steady_clock::time_point m_timerStart;
