@@ -226,6 +226,13 @@ NEMO_B200_API nemo_status_t nemo_b200_add_synapses(nemo_network_t, size_t n,
  * (src/examples/random.cpp:63-88), generated in native code. */
 NEMO_B200_API nemo_status_t nemo_b200_example_random(nemo_network_t* net,
 		unsigned ncount, unsigned scount, unsigned dmax, int stdp);
+/* The same generator with its mt19937 seeded by `seed` (the reference uses
+ * the default seed 5489) and the input-noise sigma of the excitatory and
+ * inhibitory neurons as parameters (the reference uses 5 and 2): one member
+ * of a parameter sweep. */
+NEMO_B200_API nemo_status_t nemo_b200_example_random_ex(nemo_network_t* net,
+		unsigned ncount, unsigned scount, unsigned dmax, int stdp,
+		unsigned seed, float sigma_exc, float sigma_inh);
 
 /* Run `steps` unstimulated steps on the device without returning to the
  * host in between.  If stdp_period != 0, applyStdp(reward) is applied after
@@ -239,6 +246,19 @@ NEMO_B200_API nemo_status_t nemo_b200_run(nemo_simulation_t, unsigned steps,
 		unsigned fired_counts[], uint64_t events[],
 		unsigned fired_ids[], size_t fired_cap, size_t* fired_len);
 
+/* A batch: `count` independent networks advanced together, one launch per
+ * step for all of them, under one configuration.  Each network's fire
+ * stream and state are exactly those of its own nemo_new_simulation run.
+ * The batch handle accepts nemo_b200_run (fired_counts then holds steps x
+ * count entries, [step][network], and fired_ids each step's ids network
+ * by network), nemo_apply_stdp, the launch-shape calls and
+ * nemo_b200_batch_get_type_state; per-neuron and per-synapse queries are not
+ * available on it (synapses are write-only).  Networks whose maximum delay
+ * is exactly 64 ms are rejected (NEMO_API_UNSUPPORTED). */
+NEMO_B200_API nemo_simulation_t nemo_b200_new_batch(nemo_network_t nets[], unsigned count, nemo_configuration_t conf);
+NEMO_B200_API nemo_status_t nemo_b200_network_count(nemo_simulation_t, unsigned* count);
+NEMO_B200_API nemo_status_t nemo_b200_batch_get_type_state(nemo_simulation_t, unsigned net, unsigned type,
+		float out[], size_t cap, size_t* len);
 /* Read every synapse weight (raw Q11.20) in network iteration order: source
  * neurons ascending, each source's synapses in insertion order. */
 NEMO_B200_API nemo_status_t nemo_b200_get_weights_fx(nemo_simulation_t, int32_t out[], size_t cap, size_t* len);

@@ -192,11 +192,17 @@ class Network:
         return bool(v.value)
 
 
-def example_random(ncount: int, scount: int, dmax: int, stdp: bool) -> Network:
+def example_random(ncount: int, scount: int, dmax: int, stdp: bool, seed: int | None = None,
+                   sigma_exc: float = 5.0, sigma_inh: float = 2.0) -> Network:
     """The reference's example network random::construct
-    (src/examples/random.cpp:63-88)."""
+    (src/examples/random.cpp:63-88); `seed` and the noise sigmas default to
+    the reference's (5489, 5, 2)."""
     h = C.c_void_p()
-    _check(lib().nemo_b200_example_random(C.byref(h), ncount, scount, dmax, int(stdp)))
+    if seed is None and sigma_exc == 5.0 and sigma_inh == 2.0:
+        _check(lib().nemo_b200_example_random(C.byref(h), ncount, scount, dmax, int(stdp)))
+    else:
+        _check(lib().nemo_b200_example_random_ex(C.byref(h), ncount, scount, dmax, int(stdp),
+                                                 5489 if seed is None else seed, sigma_exc, sigma_inh))
     return Network(h.value)
 
 
@@ -378,6 +384,54 @@ class Simulation:
 
     def reset_timer(self):
         _check(lib().nemo_reset_timer(self._h))
+
+
+class Batch(Simulation):
+    """Independent networks advanced together (an extension).  run() returns
+    fired counts as [step][network] and each step's fired ids network by
+    network; every network's results equal its own Simulation's."""
+
+    def __init__(self, networks, conf: Configuration):
+        arr = (C.c_void_p * len(networks))(*[n._h for n in networks])
+        h = lib().nemo_b200_new_batch(arr, len(networks), conf._h)
+        if not h:
+            raise NemoError(lib().nemo_b200_last_status(), lib().nemo_strerror().decode())
+        self._h = h
+        self.count = len(networks)
+
+    def run(self, steps: int, stdp_period: int = 0, reward: float = 1.0, ids: bool = True,
+            max_ids: int | None = None):
+        counts = np.zeros(max(steps, 1) * self.count, np.uint32)
+        events = np.zeros(max(steps, 1), np.uint64)
+        cap = max_ids if max_ids is not None else steps * 65536
+        buf = np.zeros(max(cap, 1), np.uint32) if ids else None
+        ln = C.c_size_t()
+
+        def ptr(a):
+            return None if a is None else a.ctypes.data_as(C.c_void_p)
+        _check(lib().nemo_b200_run(self._h, steps, stdp_period, reward, ptr(counts), ptr(events), ptr(buf),
+                                   cap if buf is not None else 0, C.byref(ln)))
+        counts = counts[: steps * self.count].reshape(steps, self.count)
+        return counts, events[:steps], (buf[: ln.value].copy() if buf is not None else None)
+
+    def streams(self, counts: np.ndarray, ids: np.ndarray):
+        """Split a run's (counts, ids) into per-network (counts, ids)."""
+        per_counts = [counts[:, k].copy() for k in range(self.count)]
+        per_ids = [[] for _ in range(self.count)]
+        pos = 0
+        for t in range(counts.shape[0]):
+            for k in range(self.count):
+                c = int(counts[t, k])
+                per_ids[k].append(ids[pos:pos + c])
+                pos += c
+        return [(per_counts[k], np.concatenate(per_ids[k]) if per_ids[k] else np.zeros(0, np.uint32))
+                for k in range(self.count)]
+
+    def type_state(self, net: int, ntype: int, nstate: int, n: int) -> np.ndarray:
+        out = np.zeros(max(nstate * n, 1), np.float32)
+        ln = C.c_size_t()
+        _check(lib().nemo_b200_batch_get_type_state(self._h, net, ntype, out, len(out), C.byref(ln)))
+        return out[: ln.value].reshape(nstate, n) if ln.value else np.zeros((nstate, 0), np.float32)
 
 
 def host_nrand(state: np.ndarray) -> float:

@@ -87,7 +87,12 @@ SIGNATURES = {
     "nemo_b200_add_neurons": (st, [vp, C.c_uint, sz, u32p, C.c_uint, f32p]),
     "nemo_b200_add_synapses": (st, [vp, sz, u32p, u32p, u32p, f32p, u8p, u64p]),
     "nemo_b200_example_random": (st, [C.POINTER(vp), C.c_uint, C.c_uint, C.c_uint, C.c_int]),
+    "nemo_b200_example_random_ex": (st, [C.POINTER(vp), C.c_uint, C.c_uint, C.c_uint, C.c_int, C.c_uint,
+                                         C.c_float, C.c_float]),
     "nemo_b200_run": (st, [vp, C.c_uint, C.c_uint, C.c_float, vp, vp, vp, sz, C.POINTER(sz)]),
+    "nemo_b200_new_batch": (vp, [C.POINTER(vp), C.c_uint, vp]),
+    "nemo_b200_network_count": (st, [vp, PU]),
+    "nemo_b200_batch_get_type_state": (st, [vp, C.c_uint, C.c_uint, f32p, sz, C.POINTER(sz)]),
     "nemo_b200_get_weights_fx": (st, [vp, i32p, sz, C.POINTER(sz)]),
     "nemo_b200_get_type_state": (st, [vp, C.c_uint, f32p, sz, C.POINTER(sz)]),
     "nemo_b200_synapse_count": (st, [vp, C.POINTER(C.c_uint64)]),

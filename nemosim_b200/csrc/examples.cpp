@@ -69,12 +69,18 @@ unsigned uniformInt(Mt19937& g, unsigned lo, unsigned hi)
 extern "C" nemo_status_t nemo_b200_example_random(nemo_network_t* out, unsigned ncount, unsigned scount,
 		unsigned dmax, int stdp)
 {
+	return nemo_b200_example_random_ex(out, ncount, scount, dmax, stdp, 5489u, 5.0f, 2.0f);
+}
+
+extern "C" nemo_status_t nemo_b200_example_random_ex(nemo_network_t* out, unsigned ncount, unsigned scount,
+		unsigned dmax, int stdp, unsigned seed, float sigmaExc, float sigmaInh)
+{
 	if(!out) return NEMO_INVALID_INPUT;
 	nemo_network_t net = nemo_new_network();
 	if(!net) return NEMO_ALLOCATION_ERROR;
 	unsigned iz = 0;
 	nemo_status_t r = nemo_add_neuron_type(net, "Izhikevich", &iz);
-	Mt19937 g(5489u);
+	Mt19937 g(seed);
 	std::vector<unsigned> src(scount), tgt(scount), dly(scount);
 	std::vector<float> w(scount);
 	std::vector<unsigned char> pl(scount);
@@ -97,7 +103,7 @@ extern "C" nemo_status_t nemo_b200_example_random(nemo_network_t* out, unsigned 
 			float c = v + 15.0f * r1 * r1;
 			float d = 8.0f - 6.0f * r2 * r2;
 			float u = b * v;
-			float x[7] = { a, b, c, d, 5.0f, u, v };
+			float x[7] = { a, b, c, d, sigmaExc, u, v };
 			for(int i = 0; i < 7; ++i) args[i] = x[i];
 		} else {
 			// addInhibitoryNeuron, random.cpp:46-59
@@ -106,7 +112,7 @@ extern "C" nemo_status_t nemo_b200_example_random(nemo_network_t* out, unsigned 
 			float r2 = (float) uniform01(g);
 			float b = 0.25f - 0.05f * r2;
 			float u = b * v;
-			float x[7] = { a, b, v, 2.0f, 2.0f, u, v };
+			float x[7] = { a, b, v, 2.0f, sigmaInh, u, v };
 			for(int i = 0; i < 7; ++i) args[i] = x[i];
 		}
 		r = nemo_b200_add_neurons(net, iz, 1, &nidx, 7, args);

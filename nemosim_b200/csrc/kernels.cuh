@@ -79,10 +79,33 @@ __device__ __forceinline__ int32_t fx_mul_dev(int32_t a, int32_t b)
 	return (int32_t) (((long long) a * (long long) b) >> FRACTIONAL_BITS);
 }
 
-__device__ __forceinline__ void add_current(longlong2* slot, int32_t w)
+// Fixed-point input sums.  The reference sums E (w >= 0) and I (w < 0)
+// contributions in int64 and clamps once (src/nemo/cpu/Simulation.cpp:297-300,
+// src/nemo/fixedpoint.cpp:40-49).  Here each (step slot, neuron) keeps the
+// low 32 bits of E and of -I in an 8-byte word pair, so the accumulator ring
+// fits in L2; a carry out of (or borrow into) a low word, detected from the
+// value the atomic returns, is added to a signed high-word counter of the
+// same (slot, neuron), and the slot is flagged.  The exact int64 sum is
+// high * 2^32 + low, independent of the order of the atomics.
+__device__ __forceinline__ void acc_add(const DevSim& S, uint32_t sl, uint32_t n, uint32_t cls, int64_t delta)
 {
-	unsigned long long* p = reinterpret_cast<unsigned long long*>(slot) + (w < 0 ? 1 : 0);
-	atomicAdd(p, (unsigned long long) (long long) w);
+	const size_t i = (size_t) sl * S.N + n;
+	uint32_t* lo = reinterpret_cast<uint32_t*>(S.slots + i) + cls;
+	const uint32_t d = (uint32_t) delta;
+	const uint32_t old = atomicAdd(lo, d);
+	const uint32_t now = old + d;
+	const bool wrap = delta >= 0 ? now < old : now > old;
+	if(wrap) {
+		atomicAdd(reinterpret_cast<int*>(S.slotHigh + i) + cls, delta >= 0 ? 1 : -1);
+		S.slotFlag[sl] = 1u;
+	}
+}
+
+// one synaptic weight arriving in slot sl at neuron n
+__device__ __forceinline__ void add_current(const DevSim& S, uint32_t sl, uint32_t n, int32_t w)
+{
+	if(w >= 0) acc_add(S, sl, n, 0, (int64_t) w);
+	else acc_add(S, sl, n, 1, -(int64_t) w);
 }
 
 // Izhikevich, src/nemo/cpu/plugins/Izhikevich.cpp:53-94: the v update is
@@ -188,9 +211,9 @@ __device__ __forceinline__ void compensate_inflight(const DevSim& S, const uint6
 		inflight &= inflight - 1;
 		// emitted k steps before the last step, arrives delay - k steps after it
 		const uint32_t sl = (slot + delay - k) % S.D;
-		unsigned long long* a = reinterpret_cast<unsigned long long*>(S.slots + (size_t) sl * S.N + tgt);
-		atomicAdd(a + (w < 0 ? 1 : 0), (unsigned long long) (-(long long) w));
-		atomicAdd(a + (nw < 0 ? 1 : 0), (unsigned long long) (long long) nw);
+		if(w >= 0) acc_add(S, sl, tgt, 0, -(int64_t) w);
+		else acc_add(S, sl, tgt, 1, (int64_t) w);
+		add_current(S, sl, tgt, nw);
 	}
 }
 

@@ -382,6 +382,52 @@ nemo_simulation_t nemo_new_simulation(nemo_network_t n, nemo_configuration_t c)
 
 void nemo_delete_simulation(nemo_simulation_t s) { delete s; }
 
+nemo_simulation_t nemo_b200_new_batch(nemo_network_t nets[], unsigned count, nemo_configuration_t c)
+{
+	if(!nets || !c || count == 0) {
+		setResult("NULL networks or configuration", NEMO_INVALID_INPUT);
+		return nullptr;
+	}
+	g_lastStatus = NEMO_OK;
+	try {
+		std::vector<const Network*> v;
+		for(unsigned i = 0; i < count; ++i) {
+			if(!nets[i]) NB_THROW(NEMO_INVALID_INPUT, "NULL network %u", i);
+			v.push_back(&nets[i]->net);
+		}
+		auto* s = new nemo_simulation_class();
+		try {
+			s->sim.reset(new Simulation(v, c->conf));
+		} catch(...) {
+			delete s;
+			throw;
+		}
+		return s;
+	} catch(const Error& e) {
+		setResult(e.what(), e.code());
+	} catch(const std::bad_alloc&) {
+		setResult("host memory allocation failed", NEMO_ALLOCATION_ERROR);
+	} catch(const std::exception& e) {
+		setResult(e.what(), NEMO_UNKNOWN_ERROR);
+	}
+	return nullptr;
+}
+
+nemo_status_t nemo_b200_network_count(nemo_simulation_t s, unsigned* count)
+{
+	NULLCHECK(s);
+	NULLCHECK(count);
+	CALL(*count = S(s).networkCount());
+}
+
+nemo_status_t nemo_b200_batch_get_type_state(nemo_simulation_t s, unsigned net, unsigned type, float out[],
+		size_t cap, size_t* len)
+{
+	NULLCHECK(s);
+	NULLCHECK(len);
+	CALL(S(s).getNetTypeState(net, type, out, cap, len));
+}
+
 /* nemo_c.cpp:440-477 */
 nemo_status_t nemo_step(nemo_simulation_t s, unsigned fstim[], size_t nf, unsigned inidx[],
 		float icur[], size_t ni, unsigned* fired[], size_t* nfired)

@@ -7,6 +7,7 @@
 #include <mutex>
 
 #include "kernels.cuh"
+#include "hugevec.hpp"
 #include "libm_calib.hpp"
 
 namespace nemo_b200 {
@@ -87,6 +88,7 @@ update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t slot, uint32_t 
 	const uint32_t last = min(S.N, first + P);
 	const uint64_t* histPrev = S.hist + (size_t) (cur ^ 1u) * S.N;
 	uint64_t* histCur = S.hist + (size_t) cur * S.N;
+	const uint32_t slotFlag = S.D ? S.slotFlag[slot] : 0u;
 	if(tid == 0) { sFired = 0; sEvents = 0; sStdp = 0; }
 	__syncthreads();
 
@@ -104,11 +106,19 @@ update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t slot, uint32_t 
 			// src/nemo/cpu/Simulation.cpp:259-288)
 			float cE = 0.0f, cI = 0.0f;
 			if(S.D) {
-				longlong2* a = S.slots + (size_t) slot * S.N + n;
-				longlong2 acc = *a;
-				if(acc.x | acc.y) *a = make_longlong2(0, 0);
-				cE = wfx_to_float(acc.x);
-				cI = wfx_to_float(acc.y);
+				uint2* a = S.slots + (size_t) slot * S.N + n;
+				const uint2 acc = *a;
+				if(acc.x | acc.y) *a = make_uint2(0, 0);
+				long long e = (long long) acc.x, i = (long long) acc.y;
+				if(slotFlag) {
+					int2* h = S.slotHigh + (size_t) slot * S.N + n;
+					const int2 hi = *h;
+					if(hi.x | hi.y) *h = make_int2(0, 0);
+					e += (long long) hi.x << 32;
+					i += (long long) hi.y << 32;
+				}
+				cE = wfx_to_float(e);
+				cI = wfx_to_float(-i);
 			}
 			float ext = S.curExt[n];
 			if(__float_as_uint(ext) != 0u) S.curExt[n] = 0.0f;
@@ -148,17 +158,7 @@ update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t slot, uint32_t 
 		}
 		// targets touched in this STDP period, for applyStdp
 		const uint32_t tb = __ballot_sync(0xffffffffu, target);
-		if(tb) {
-			uint32_t old = 0;
-			if(lane == 0) old = atomicOr(&S.touchedBits[n >> 5], tb);
-			old = __shfl_sync(0xffffffffu, old, 0);
-			const bool fresh = target && !((old >> lane) & 1u);
-			const uint32_t nchA = fresh ? (indeg + CHUNK - 1) / CHUNK : 0;
-			if(__any_sync(0xffffffffu, fresh)) {
-				const uint32_t pos = reserve_chunks(S.applyChunkCount, nchA);
-				write_chunks(S.applyChunks, pos, rb, indeg, nchA, n);
-			}
-		}
+		if(tb && lane == 0) atomicOr(&S.touchedBits[n >> 5], tb);
 		if(fb) {
 			const unsigned long long ev = warp_sum(fired ? outdeg : 0);
 			if(lane == 0) {
@@ -189,7 +189,11 @@ __global__ void __launch_bounds__(STEP_THREADS)
 deliver_kernel(const DevSim S, uint32_t cur, uint32_t slot)
 {
 	const uint32_t nch = S.chunkCount[cur];
-	if(blockIdx.x == 0 && threadIdx.x == 0) S.chunkCount[cur ^ 1u] = 0; // next step's list starts empty
+	if(blockIdx.x == 0 && threadIdx.x == 0) {
+		S.chunkCount[cur ^ 1u] = 0; // next step's list starts empty
+		// this step's slot was read by update_kernel; no spike arrives in it now
+		if(S.D) S.slotFlag[slot] = 0u;
+	}
 	const uint32_t lane = threadIdx.x & 31;
 	const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
 	const uint64_t* hist = S.hist + (size_t) cur * S.N;
@@ -208,7 +212,7 @@ deliver_kernel(const DevSim S, uint32_t cur, uint32_t slot)
 				if(lane + 32 * j < len) {
 					uint32_t sl = slot + (s[j].x >> 26) + 1;
 					sl = sl >= S.D ? sl - S.D : sl;
-					add_current(S.slots + (size_t) sl * S.N + (s[j].x & (MAX_NEURONS - 1)), (int32_t) s[j].y);
+					add_current(S, sl, s[j].x & (MAX_NEURONS - 1), (int32_t) s[j].y);
 				}
 			}
 		} else {
@@ -235,6 +239,33 @@ deliver_kernel(const DevSim S, uint32_t cur, uint32_t slot)
 				}
 			}
 		}
+	}
+}
+
+// Turns the targets touched since the last applyStdp (a bit-vector) into
+// chunks of their incoming plastic synapses, and clears the bit-vector.
+__global__ void __launch_bounds__(STEP_THREADS)
+collect_touched_kernel(const DevSim S)
+{
+	const uint32_t stride = gridDim.x * blockDim.x;
+	const uint32_t words = (S.W + 31) & ~31u;  // whole warps take part in the reservation
+	for(uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += stride) {
+		const uint32_t bits = w < S.W ? S.touchedBits[w] : 0u;
+		uint32_t nch = 0;
+		for(uint32_t b = bits; b; b &= b - 1) {
+			const uint32_t n = w * 32 + __ffs(b) - 1;
+			nch += (uint32_t) ((S.rcmPtr[n + 1] - S.rcmPtr[n] + CHUNK - 1) / CHUNK);
+		}
+		uint32_t pos = reserve_chunks(S.applyChunkCount, nch);
+		for(uint32_t b = bits; b; b &= b - 1) {
+			const uint32_t n = w * 32 + __ffs(b) - 1;
+			const unsigned long long rb = S.rcmPtr[n];
+			const uint32_t len = (uint32_t) (S.rcmPtr[n + 1] - rb);
+			const uint32_t c = (len + CHUNK - 1) / CHUNK;
+			write_chunks(S.applyChunks, pos, rb, len, c, n);
+			pos += c;
+		}
+		if(bits) S.touchedBits[w] = 0u;
 	}
 }
 
@@ -391,27 +422,51 @@ static void seed_rng(std::vector<uint32_t>& planes, unsigned N)
 	for(unsigned l = 0; l < N; ++l) {
 		for(unsigned p = 0; p < 4; ++p) planes[(size_t) p * N + l] = next() >> 1;
 	}
+	// planes[p * N + l] is word p of the neuron with local index l
 }
 
 static inline uint64_t shl64(uint64_t x, unsigned s) { return x << (s & 63); }
 
-Simulation::Simulation(const Network& net, const Configuration& conf)
+Simulation::Simulation(const Network& net, const Configuration& conf) :
+	Simulation(std::vector<const Network*>{ &net }, conf)
 {
+}
+
+// Builds the device layout of one network or, for a batch, of several
+// independent networks simulated as one: their neurons share the neuron
+// arrays (grouped by neuron kind, so that the step kernel sees at most one
+// range per kind), their synapses never cross networks, and each network's
+// RNG streams and fire stream are those of its own single-network run.
+Simulation::Simulation(const std::vector<const Network*>& nets, const Configuration& conf)
+{
+	if(nets.empty()) NB_THROW(NEMO_INVALID_INPUT, "no network");
+	const bool batch = nets.size() > 1;
 	// checks in the order of nemo::simulationBackend (src/nemo/nemo.cpp:109-134)
 	// and the backend constructor (src/nemo/cpu/Simulation.cpp:36-82)
-	unsigned N = net.neuronCount();
-	if(N == 0) NB_THROW(NEMO_INVALID_INPUT, "Cannot create simulation from empty network");
-	if(conf.stdp && net.maxDelay + conf.postfire.size() > MAX_HISTORY) {
-		NB_THROW(NEMO_INVALID_INPUT, "Max delay + postfire part of STDP function must be <= %u", MAX_HISTORY);
+	size_t totalN = 0;
+	unsigned maxDelay = 0;
+	for(const Network* np : nets) {
+		const Network& net = *np;
+		unsigned n = net.neuronCount();
+		if(n == 0) NB_THROW(NEMO_INVALID_INPUT, "Cannot create simulation from empty network");
+		if(conf.stdp && net.maxDelay + conf.postfire.size() > MAX_HISTORY) {
+			NB_THROW(NEMO_INVALID_INPUT, "Max delay + postfire part of STDP function must be <= %u", MAX_HISTORY);
+		}
+		if(conf.backend != NEMO_BACKEND_CUDA) {
+			NB_THROW(NEMO_API_UNSUPPORTED, "This library provides only the B200 CUDA backend; the CPU backend is not part of it");
+		}
+		if(net.maxDelay > 64) {
+			NB_THROW(NEMO_INVALID_INPUT, "The network has synapses with delay %ums. The B200 backend supports a maximum of 64 ms", net.maxDelay);
+		}
+		if(batch && net.maxDelay == 64) {
+			NB_THROW(NEMO_API_UNSUPPORTED, "A batched network may not have a maximum delay of exactly 64 ms");
+		}
+		if(net.duplicate) NB_THROW(NEMO_INVALID_INPUT, "Duplicate neuron index %u", net.duplicateIdx);
+		totalN += n;
+		maxDelay = std::max(maxDelay, net.maxDelay);
 	}
-	if(conf.backend != NEMO_BACKEND_CUDA) {
-		NB_THROW(NEMO_API_UNSUPPORTED, "This library provides only the B200 CUDA backend; the CPU backend is not part of it");
-	}
-	if(net.maxDelay > 64) {
-		NB_THROW(NEMO_INVALID_INPUT, "The network has synapses with delay %ums. The B200 backend supports a maximum of 64 ms", net.maxDelay);
-	}
-	if(net.duplicate) NB_THROW(NEMO_INVALID_INPUT, "Duplicate neuron index %u", net.duplicateIdx);
-	if(N >= MAX_NEURONS) NB_THROW(NEMO_API_UNSUPPORTED, "The B200 backend supports at most %u neurons", MAX_NEURONS - 1);
+	if(totalN >= MAX_NEURONS) NB_THROW(NEMO_API_UNSUPPORTED, "The B200 backend supports at most %u neurons", MAX_NEURONS - 1);
+	const unsigned N = (unsigned) totalN;
 
 	int ndev = 0;
 	NB_CUDA(cudaGetDeviceCount(&ndev));
@@ -428,46 +483,86 @@ Simulation::Simulation(const Network& net, const Configuration& conf)
 	NB_CUDA(cudaEventCreate(&m_ev1));
 
 	m_N = N;
-	m_maxDelay = net.maxDelay;
-	m_writeOnly = conf.writeOnlySynapses;
+	m_nets = (unsigned) nets.size();
+	m_maxDelay = maxDelay;
+	m_writeOnly = conf.writeOnlySynapses || batch;
 	memset(&m_dev, 0, sizeof m_dev);
 	DevSim& S = m_dev;
 	S.N = N;
 	S.W = (N + 31) / 32;
 
-	// local indices: type order, then insertion order
+	// neuron layout: kinds in order of first appearance (for one network this
+	// is its type order, src/nemo/cpu/Simulation.cpp:58-73), then network
+	// order, then insertion order
+	std::vector<NeuronKind> kinds;
+	for(const Network* np : nets) {
+		for(const NeuronCollection& c : np->types) {
+			if(c.size() && std::find(kinds.begin(), kinds.end(), c.desc->kind) == kinds.end()) kinds.push_back(c.desc->kind);
+		}
+	}
+	if(kinds.size() > MAX_TYPES) NB_THROW(NEMO_API_UNSUPPORTED, "At most %u neuron types", MAX_TYPES);
 	m_l2g.resize(N);
 	m_ltype.resize(N);
-	m_g2l.reserve(N * 2);
+	m_netLocal.resize(N);
+	if(batch) m_netOf.resize(N);
+	m_g2l.assign(nets.size(), std::unordered_map<unsigned, unsigned>());
+	for(size_t i = 0; i < nets.size(); ++i) m_g2l[i].reserve(nets[i]->neuronCount() * 2);
+	m_netTypes.assign(nets.size(), std::vector<NetTypeRange>());
+	// network-local index of the first neuron of each type, per network
+	std::vector<std::vector<unsigned>> localBase(nets.size());
+	for(size_t i = 0; i < nets.size(); ++i) {
+		unsigned b = 0;
+		for(const NeuronCollection& c : nets[i]->types) {
+			localBase[i].push_back(b);
+			b += (unsigned) c.size();
+		}
+		m_netTypes[i].resize(nets[i]->types.size());
+	}
 	unsigned l = 0;
 	bool needCalib = false;
-	for(unsigned t = 0; t < net.types.size(); ++t) {
-		const NeuronCollection& c = net.types[t];
-		if(c.size() == 0) continue;
-		if(m_types.size() >= MAX_TYPES) NB_THROW(NEMO_API_UNSUPPORTED, "At most %u neuron types", MAX_TYPES);
+	for(NeuronKind kind : kinds) {
 		HostType ht;
-		ht.desc = c.desc;
-		ht.netType = t;
+		ht.desc = &NEURON_TYPES[kind];
+		ht.netType = 0;
 		ht.base = l;
-		ht.n = (unsigned) c.size();
-		unsigned np = c.desc->nparam, ns = c.desc->nstate, na = np + ns;
+		ht.n = 0;
+		for(size_t i = 0; i < nets.size(); ++i) {
+			for(size_t t = 0; t < nets[i]->types.size(); ++t) {
+				if(nets[i]->types[t].desc->kind == kind) ht.n += (unsigned) nets[i]->types[t].size();
+			}
+		}
+		const unsigned np = ht.desc->nparam, ns = ht.desc->nstate, na = np + ns;
 		std::vector<float> param((size_t) np * ht.n), state((size_t) ns * ht.n);
-		for(size_t i = 0; i < c.size(); ++i) {
-			for(unsigned p = 0; p < np; ++p) param[(size_t) p * ht.n + i] = c.args[i * na + p];
-			for(unsigned v = 0; v < ns; ++v) state[(size_t) v * ht.n + i] = c.args[i * na + np + v];
-			m_l2g[l + i] = c.gidx[i];
-			m_ltype[l + i] = (uint8_t) m_types.size();
-			if(!m_g2l.emplace(c.gidx[i], l + (unsigned) i).second) {
-				NB_THROW(NEMO_INVALID_INPUT, "Duplicate neuron index %u", c.gidx[i]);
+		unsigned i0 = 0;
+		for(size_t i = 0; i < nets.size(); ++i) {
+			for(size_t t = 0; t < nets[i]->types.size(); ++t) {
+				const NeuronCollection& c = nets[i]->types[t];
+				if(c.desc->kind != kind || c.size() == 0) continue;
+				if(!batch) ht.netType = (unsigned) t;
+				m_netTypes[i][t] = NetTypeRange{ (unsigned) m_types.size(), i0, (unsigned) c.size() };
+				for(size_t j = 0; j < c.size(); ++j) {
+					const unsigned li = i0 + (unsigned) j;
+					for(unsigned p = 0; p < np; ++p) param[(size_t) p * ht.n + li] = c.args[j * na + p];
+					for(unsigned v = 0; v < ns; ++v) state[(size_t) v * ht.n + li] = c.args[j * na + np + v];
+					const unsigned u = l + li;
+					m_l2g[u] = c.gidx[j];
+					m_ltype[u] = (uint8_t) m_types.size();
+					m_netLocal[u] = localBase[i][t] + (unsigned) j;
+					if(batch) m_netOf[u] = (uint32_t) i;
+					if(!m_g2l[i].emplace(c.gidx[j], u).second) {
+						NB_THROW(NEMO_INVALID_INPUT, "Duplicate neuron index %u", c.gidx[j]);
+					}
+				}
+				i0 += (unsigned) c.size();
 			}
 		}
 		ht.dParam = dalloc<float>(param.size());
 		ht.dState = dalloc<float>(state.size());
 		NB_CUDA(cudaMemcpyAsync(ht.dParam, param.data(), param.size() * 4, cudaMemcpyHostToDevice, m_stream));
 		NB_CUDA(cudaMemcpyAsync(ht.dState, state.data(), state.size() * 4, cudaMemcpyHostToDevice, m_stream));
-		if(c.desc->kind == KIND_IZHIKEVICH) needCalib = true;
+		if(kind == KIND_IZHIKEVICH) needCalib = true;
 		TypeRange& tr = S.types[m_types.size()];
-		tr.kind = c.desc->kind;
+		tr.kind = kind;
 		tr.base = ht.base;
 		tr.n = ht.n;
 		tr.param = ht.dParam;
@@ -478,59 +573,74 @@ Simulation::Simulation(const Network& net, const Configuration& conf)
 	}
 	S.ntypes = (uint32_t) m_types.size();
 
+	// synapses of all networks, each mapped through its own network's ids
+	size_t Sn = 0;
+	for(const Network* np : nets) Sn += np->src.size();
+	m_nsyn = Sn;
+	hvector<unsigned> lsrc(Sn), ltgt(Sn), sdelay(Sn);
+	hvector<int32_t> fxw(Sn);
+	hvector<uint8_t> splastic(Sn);
+	{
+		size_t k = 0;
+		for(size_t i = 0; i < nets.size(); ++i) {
+			const Network& net = *nets[i];
+			const auto& g2l = m_g2l[i];
+			for(size_t q = 0; q < net.src.size(); ++q, ++k) {
+				auto is = g2l.find(net.src[q]);
+				if(is == g2l.end()) NB_THROW(NEMO_INVALID_INPUT, "Non-existing neuron index %u", net.src[q]);
+				auto it = g2l.find(net.tgt[q]);
+				if(it == g2l.end()) NB_THROW(NEMO_INVALID_INPUT, "Non-existing neuron index %u", net.tgt[q]);
+				lsrc[k] = is->second;
+				ltgt[k] = it->second;
+				fxw[k] = fx_toFix(net.weight[q]);
+				sdelay[k] = net.delay[q];
+				splastic[k] = net.plastic[q];
+			}
+		}
+	}
+
 	// forward matrix (src/nemo/ConnectivityMatrix.cpp:65-162): outgoing
 	// synapses per local source, sorted by delay, insertion order within a
 	// delay -- the reference's row order
-	const size_t Sn = net.src.size();
-	m_nsyn = Sn;
-	std::vector<unsigned> lsrc(Sn), ltgt(Sn);
-	std::vector<int32_t> fxw(Sn);
-	for(size_t k = 0; k < Sn; ++k) {
-		auto is = m_g2l.find(net.src[k]);
-		if(is == m_g2l.end()) NB_THROW(NEMO_INVALID_INPUT, "Non-existing neuron index %u", net.src[k]);
-		auto it = m_g2l.find(net.tgt[k]);
-		if(it == m_g2l.end()) NB_THROW(NEMO_INVALID_INPUT, "Non-existing neuron index %u", net.tgt[k]);
-		lsrc[k] = is->second;
-		ltgt[k] = it->second;
-		fxw[k] = fx_toFix(net.weight[k]);
-	}
-	// stable counting sort by (local source, delay)
 	const unsigned D = std::max(1u, m_maxDelay);
-	std::vector<uint64_t> rowStart((size_t) N * D + 1, 0);
-	for(size_t k = 0; k < Sn; ++k) rowStart[(size_t) lsrc[k] * D + net.delay[k]]++;
-	for(size_t r = 0; r < (size_t) N * D; ++r) rowStart[r + 1] += rowStart[r];
-	m_pos.resize(Sn);
-	{
-		std::vector<uint64_t> fill(rowStart.begin(), rowStart.end() - 1);
-		for(size_t k = 0; k < Sn; ++k) m_pos[k] = fill[(size_t) lsrc[k] * D + net.delay[k] - 1]++;
-	}
 	std::vector<unsigned long long> outPtr(N + 1);
-	for(unsigned s = 0; s <= N; ++s) outPtr[s] = rowStart[(size_t) s * D];
+	hvector<uint64_t> pos(Sn);
+	{
+		hvector<uint64_t> rowStart((size_t) N * D + 1, 0);
+		for(size_t k = 0; k < Sn; ++k) rowStart[(size_t) lsrc[k] * D + sdelay[k]]++;
+		for(size_t r = 0; r < (size_t) N * D; ++r) rowStart[r + 1] += rowStart[r];
+		for(unsigned s = 0; s <= N; ++s) outPtr[s] = rowStart[(size_t) s * D];
+		for(size_t k = 0; k < Sn; ++k) pos[k] = rowStart[(size_t) lsrc[k] * D + sdelay[k] - 1]++;
+	}
 	m_outDegree.resize(N);
 	for(unsigned s = 0; s < N; ++s) {
 		m_outDegree[s] = (uint32_t) (outPtr[s + 1] - outPtr[s]);
 		m_maxOutDeg = std::max(m_maxOutDeg, m_outDegree[s]);
 	}
-	std::vector<uint2> syn(Sn);
-	for(size_t k = 0; k < Sn; ++k) {
-		syn[m_pos[k]] = make_uint2(ltgt[k] | ((net.delay[k] - 1) << 26), (uint32_t) fxw[k]);
+	{
+		hvector<uint2> syn(Sn);
+		for(size_t k = 0; k < Sn; ++k) {
+			syn[pos[k]] = make_uint2(ltgt[k] | ((sdelay[k] - 1) << 26), (uint32_t) fxw[k]);
+		}
+		auto* dOut = dalloc<unsigned long long>(N + 1);
+		auto* dSyn = dalloc<uint2>(Sn);
+		NB_CUDA(cudaMemcpyAsync(dOut, outPtr.data(), (N + 1) * 8, cudaMemcpyHostToDevice, m_stream));
+		NB_CUDA(cudaMemcpyAsync(dSyn, syn.data(), Sn * 8, cudaMemcpyHostToDevice, m_stream));
+		S.outPtr = dOut;
+		S.syn = dSyn;
+		NB_CUDA(cudaStreamSynchronize(m_stream));
 	}
-	rowStart.clear();
-	rowStart.shrink_to_fit();
-	auto* dOut = dalloc<unsigned long long>(N + 1);
-	auto* dSyn = dalloc<uint2>(Sn);
-	NB_CUDA(cudaMemcpyAsync(dOut, outPtr.data(), (N + 1) * 8, cudaMemcpyHostToDevice, m_stream));
-	NB_CUDA(cudaMemcpyAsync(dSyn, syn.data(), Sn * 8, cudaMemcpyHostToDevice, m_stream));
-	S.outPtr = dOut;
-	S.syn = dSyn;
 
-	// query tables: per local source, its synapses by per-source index
+	// query tables of one network: per local source, its synapses by
+	// per-source index
 	if(!m_writeOnly) {
+		const Network& net = *nets[0];
 		m_srcStart.assign(N + 1, 0);
 		for(size_t k = 0; k < Sn; ++k) m_srcStart[lsrc[k] + 1]++;
 		for(unsigned s = 0; s < N; ++s) m_srcStart[s + 1] += m_srcStart[s];
 		m_srcOrder.resize(Sn);
 		for(size_t k = 0; k < Sn; ++k) m_srcOrder[m_srcStart[lsrc[k]] + net.sid[k]] = k;
+		m_pos.assign(pos.begin(), pos.end());
 		m_synDelay.assign(net.delay.begin(), net.delay.end());
 		m_synPlastic.assign(net.plastic.begin(), net.plastic.end());
 		m_synTarget.assign(net.tgt.begin(), net.tgt.end());
@@ -567,20 +677,20 @@ Simulation::Simulation(const Network& net, const Configuration& conf)
 		sp.postPreBits = ~shl64(~0ull, sp.npost);
 		sp.postFireMask = shl64(1ull, sp.npost);
 
-		for(size_t k = 0; k < Sn; ++k) if(net.plastic[k]) rcmPtr[ltgt[k] + 1]++;
+		for(size_t k = 0; k < Sn; ++k) if(splastic[k]) rcmPtr[ltgt[k] + 1]++;
 		for(unsigned t = 0; t < N; ++t) {
 			m_maxPlasticInDeg = std::max(m_maxPlasticInDeg, (uint32_t) rcmPtr[t + 1]);
 			rcmPtr[t + 1] += rcmPtr[t];
 		}
 		size_t P = rcmPtr[N];
-		std::vector<uint32_t> rsrc(P), rfwd(P);
+		hvector<uint32_t> rsrc(P), rfwd(P);
 		std::vector<unsigned long long> fill(rcmPtr.begin(), rcmPtr.end() - 1);
 		for(size_t k = 0; k < Sn; ++k) {
-			if(!net.plastic[k]) continue;
+			if(!splastic[k]) continue;
 			size_t p = fill[ltgt[k]]++;
-			rsrc[p] = lsrc[k] | ((net.delay[k] - 1) << 26);
-			if(m_pos[k] > 0xffffffffull) NB_THROW(NEMO_API_UNSUPPORTED, "too many synapses for STDP");
-			rfwd[p] = (uint32_t) m_pos[k];
+			rsrc[p] = lsrc[k] | ((sdelay[k] - 1) << 26);
+			if(pos[k] > 0xffffffffull) NB_THROW(NEMO_API_UNSUPPORTED, "too many synapses for STDP");
+			rfwd[p] = (uint32_t) pos[k];
 		}
 		auto* dRsrc = dalloc<uint32_t>(P);
 		auto* dRfwd = dalloc<uint32_t>(P);
@@ -611,11 +721,21 @@ Simulation::Simulation(const Network& net, const Configuration& conf)
 		S.applyChunkCount = dalloc<uint32_t>(1);
 	}
 
-	// per-neuron RNG, keyed by local index (src/nemo/cpu/Neurons.cpp:41)
-	std::vector<uint32_t> planes;
-	seed_rng(planes, N);
-	S.rng = dalloc<uint32_t>(4 * (size_t) N);
-	NB_CUDA(cudaMemcpyAsync(S.rng, planes.data(), planes.size() * 4, cudaMemcpyHostToDevice, m_stream));
+	// per-neuron RNG, keyed by the network-local index
+	// (src/nemo/cpu/Neurons.cpp:41)
+	{
+		unsigned maxLocal = 0;
+		for(const Network* np : nets) maxLocal = std::max(maxLocal, np->neuronCount());
+		std::vector<uint32_t> stream;
+		seed_rng(stream, maxLocal);
+		std::vector<uint32_t> planes(4 * (size_t) N);
+		for(unsigned u = 0; u < N; ++u) {
+			for(unsigned p = 0; p < 4; ++p) planes[(size_t) p * N + u] = stream[(size_t) p * maxLocal + m_netLocal[u]];
+		}
+		S.rng = dalloc<uint32_t>(4 * (size_t) N);
+		NB_CUDA(cudaMemcpyAsync(S.rng, planes.data(), planes.size() * 4, cudaMemcpyHostToDevice, m_stream));
+		NB_CUDA(cudaStreamSynchronize(m_stream));
+	}
 
 	S.hist = dalloc<uint64_t>(2 * (size_t) N);
 	S.fstim = dalloc<uint32_t>(S.W);
@@ -625,7 +745,9 @@ Simulation::Simulation(const Network& net, const Configuration& conf)
 	// (src/nemo/cpu/Simulation.cpp:263): nothing is delivered when the
 	// maximum delay is 0 or 64
 	S.D = (m_maxDelay >= 1 && m_maxDelay <= 63) ? m_maxDelay + 1 : 0;
-	S.slots = S.D ? dalloc<longlong2>((size_t) S.D * N) : nullptr;
+	S.slots = S.D ? dalloc<uint2>((size_t) S.D * N) : nullptr;
+	S.slotHigh = S.D ? dalloc<int2>((size_t) S.D * N) : nullptr;
+	S.slotFlag = dalloc<uint32_t>(std::max(1u, S.D));
 	S.R = (uint32_t) std::max<size_t>(16, std::min<size_t>(1024, (64u << 20) / ((size_t) S.W * 4)));
 	S.firedRing = dalloc<uint32_t>((size_t) S.R * S.W);
 	S.firedCount = dalloc<uint32_t>(S.R);
@@ -666,8 +788,9 @@ void Simulation::sync()
 
 unsigned Simulation::localIdx(unsigned g) const
 {
-	auto it = m_g2l.find(g);
-	if(it == m_g2l.end()) NB_THROW(NEMO_INVALID_INPUT, "Non-existing neuron index %u", g);
+	if(m_nets > 1) NB_THROW(NEMO_API_UNSUPPORTED, "per-neuron access is not available on a batch of networks");
+	auto it = m_g2l[0].find(g);
+	if(it == m_g2l[0].end()) NB_THROW(NEMO_INVALID_INPUT, "Non-existing neuron index %u", g);
 	return it->second;
 }
 
@@ -791,11 +914,14 @@ void Simulation::applyStdpDevice(int32_t R)
 	const uint64_t last = m_cycle ? m_cycle - 1 : 0;
 	const uint32_t par = (uint32_t) (last & 1);
 	const uint32_t slot = m_dev.D ? (uint32_t) (last % m_dev.D) : 0;
+	const bool fullPassDone = m_weightsClamped;
 	timedBegin(K_APPLY);
 	if(!m_weightsClamped) {
 		unsigned grid = std::min<unsigned>((m_N + 7) / 8, (unsigned) m_sms * 8);
 		apply_full_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, R, par, slot);
 	} else {
+		unsigned cgrid = std::max(1u, std::min<unsigned>((m_dev.W + STEP_THREADS - 1) / STEP_THREADS, (unsigned) m_sms * 4));
+		collect_touched_kernel<<<cgrid, STEP_THREADS, 0, m_stream>>>(m_dev);
 		apply_touched_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, R, par, slot);
 	}
 	timedEnd();
@@ -804,7 +930,7 @@ void Simulation::applyStdpDevice(int32_t R)
 	// synapses of touched targets can change
 	m_weightsClamped = true;
 	NB_CUDA(cudaMemsetAsync(m_dev.applyChunkCount, 0, 4, m_stream));
-	NB_CUDA(cudaMemsetAsync(m_dev.touchedBits, 0, (size_t) m_dev.W * 4, m_stream));
+	if(!fullPassDone) NB_CUDA(cudaMemsetAsync(m_dev.touchedBits, 0, (size_t) m_dev.W * 4, m_stream));
 }
 
 /* ConnectivityMatrix::applyStdp argument checks (src/nemo/ConnectivityMatrix.cpp:241-259) */
@@ -862,7 +988,7 @@ void Simulation::run(unsigned steps, unsigned stdpPeriod, float reward, unsigned
 		NB_CUDA(cudaMemcpyAsync(hc.data(), m_dev.firedCount, m_dev.R * 4, cudaMemcpyDeviceToHost, m_stream));
 		NB_CUDA(cudaMemcpyAsync(he.data(), m_dev.eventCount, m_dev.R * 8, cudaMemcpyDeviceToHost, m_stream));
 		NB_CUDA(cudaMemcpyAsync(hs.data(), m_dev.stdpCount, m_dev.R * 8, cudaMemcpyDeviceToHost, m_stream));
-		if(ids) {
+		if(ids || (m_nets > 1 && counts)) {
 			NB_CUDA(cudaMemcpyAsync(m_hFired, m_dev.firedRing, (size_t) m_dev.R * m_dev.W * 4,
 					cudaMemcpyDeviceToHost, m_stream));
 		}
@@ -882,29 +1008,68 @@ void Simulation::run(unsigned steps, unsigned stdpPeriod, float reward, unsigned
 		for(uint32_t r = 0; r < m_dev.R; ++r) lastStdpEntries += hs[r];
 		for(unsigned i = 0; i < chunk; ++i) {
 			uint32_t r = (uint32_t) ((first + i) % m_dev.R);
-			if(counts) counts[done + i] = hc[r];
 			if(events) events[done + i] = he[r];
 			lastFired += hc[r];
 			lastEvents += he[r];
-			if(ids) {
-				const uint32_t* words = m_hFired + (size_t) r * m_dev.W;
-				for(uint32_t w = 0; w < m_dev.W; ++w) {
-					uint32_t bits = words[w];
-					while(bits) {
-						uint32_t b = __builtin_ctz(bits);
-						bits &= bits - 1;
-						if(total >= cap) NB_THROW(NEMO_BUFFER_OVERFLOW, "fired id buffer too small");
-						ids[total++] = m_l2g[w * 32 + b];
+			if(m_nets == 1) {
+				if(counts) counts[done + i] = hc[r];
+				if(ids) {
+					const uint32_t* words = m_hFired + (size_t) r * m_dev.W;
+					for(uint32_t w = 0; w < m_dev.W; ++w) {
+						uint32_t bits = words[w];
+						while(bits) {
+							uint32_t b = __builtin_ctz(bits);
+							bits &= bits - 1;
+							if(total >= cap) NB_THROW(NEMO_BUFFER_OVERFLOW, "fired id buffer too small");
+							ids[total++] = m_l2g[w * 32 + b];
+						}
 					}
+				} else {
+					total += hc[r];
 				}
 			} else {
-				total += hc[r];
+				total += decodeBatchStep(r, done + i, counts, ids, total, cap);
 			}
 		}
 		done += chunk;
 	}
 	if(len) *len = total;
 	lastRunMs = runMs;
+}
+
+// Fired neurons of ring position r, split by network: per network in its
+// own local order (as its single-network run reports them), networks in
+// order.  Writes counts[step * nets + net] and appends to ids when given.
+size_t Simulation::decodeBatchStep(uint32_t r, unsigned step, unsigned* counts, unsigned* ids, size_t pos, size_t cap)
+{
+	std::vector<std::vector<uint32_t>>& per = m_batchScratch;
+	per.resize(m_nets);
+	for(auto& v : per) v.clear();
+	const uint32_t* words = m_hFired + (size_t) r * m_dev.W;
+	for(uint32_t w = 0; w < m_dev.W; ++w) {
+		uint32_t bits = words[w];
+		while(bits) {
+			uint32_t b = __builtin_ctz(bits);
+			bits &= bits - 1;
+			const uint32_t u = w * 32 + b;
+			per[m_netOf[u]].push_back(u);
+		}
+	}
+	size_t n = 0;
+	for(unsigned k = 0; k < m_nets; ++k) {
+		auto& v = per[k];
+		if(!std::is_sorted(v.begin(), v.end(), [&](uint32_t a, uint32_t b) { return m_netLocal[a] < m_netLocal[b]; })) {
+			std::sort(v.begin(), v.end(), [&](uint32_t a, uint32_t b) { return m_netLocal[a] < m_netLocal[b]; });
+		}
+		if(counts) counts[(size_t) step * m_nets + k] = (unsigned) v.size();
+		if(ids) {
+			if(pos + n + v.size() > cap) NB_THROW(NEMO_BUFFER_OVERFLOW, "fired id buffer too small");
+			for(uint32_t u : v) ids[pos + n++] = m_l2g[u];
+		} else {
+			n += v.size();
+		}
+	}
+	return n;
 }
 
 float Simulation::autotune(unsigned trialSteps)
@@ -919,7 +1084,11 @@ float Simulation::autotune(unsigned trialSteps)
 	regions.emplace_back(m_dev.hist, (size_t) 2 * m_N * 8);
 	regions.emplace_back(m_dev.fstim, (size_t) m_dev.W * 4);
 	regions.emplace_back(m_dev.curExt, (size_t) m_N * 4);
-	if(m_dev.D) regions.emplace_back(m_dev.slots, (size_t) m_dev.D * m_N * 16);
+	if(m_dev.D) {
+		regions.emplace_back(m_dev.slots, (size_t) m_dev.D * m_N * 8);
+		regions.emplace_back(m_dev.slotHigh, (size_t) m_dev.D * m_N * 8);
+		regions.emplace_back(m_dev.slotFlag, (size_t) m_dev.D * 4);
+	}
 	if(m_dev.stdp) regions.emplace_back(m_dev.rcmAcc, (size_t) lastPlastic * 4);
 	regions.emplace_back(m_dev.chunkCount, 8);
 	regions.emplace_back(m_dev.applyChunkCount, 4);
@@ -1070,8 +1239,8 @@ void Simulation::setNeuronParameter(unsigned g, unsigned p, float v)
 const std::vector<uint64_t>& Simulation::getSynapsesFrom(unsigned source)
 {
 	if(m_writeOnly) NB_THROW(NEMO_INVALID_INPUT, "Cannot read synapse state if simulation configured with write-only synapses");
-	auto it = m_g2l.find(source);
-	if(it == m_g2l.end()) NB_THROW(NEMO_INVALID_INPUT, "Non-existing source neuron id (%u) in synapse id query", source);
+	auto it = m_g2l[0].find(source);
+	if(it == m_g2l[0].end()) NB_THROW(NEMO_INVALID_INPUT, "Non-existing source neuron id (%u) in synapse id query", source);
 	uint64_t n = m_srcStart[it->second + 1] - m_srcStart[it->second];
 	m_queried.resize(n);
 	for(uint64_t i = 0; i < n; ++i) m_queried[i] = ((uint64_t) source << 32) | i;
@@ -1084,8 +1253,8 @@ size_t Simulation::synapseKey(uint64_t id) const
 	if(m_writeOnly) NB_THROW(NEMO_INVALID_INPUT, "Cannot read synapse state if simulation configured with write-only synapses");
 	unsigned source = (unsigned) (id >> 32);
 	uint32_t s = (uint32_t) (id & 0xffffffffu);
-	auto it = m_g2l.find(source);
-	if(it == m_g2l.end() || m_srcStart[it->second + 1] == m_srcStart[it->second]) {
+	auto it = m_g2l[0].find(source);
+	if(it == m_g2l[0].end() || m_srcStart[it->second + 1] == m_srcStart[it->second]) {
 		NB_THROW(NEMO_INVALID_INPUT, "Non-existing neuron id (%u) in synapse query", source);
 	}
 	uint64_t n = m_srcStart[it->second + 1] - m_srcStart[it->second];
@@ -1130,17 +1299,26 @@ void Simulation::getWeightsFx(int32_t* out, size_t cap, size_t* len)
 
 void Simulation::getTypeState(unsigned netType, float* out, size_t cap, size_t* len)
 {
-	for(const HostType& t : m_types) {
-		if(t.netType != netType) continue;
-		size_t n = (size_t) t.n * t.desc->nstate;
-		if(cap < n) NB_THROW(NEMO_BUFFER_OVERFLOW, "state buffer too small");
-		NB_CUDA(cudaSetDevice(m_device));
-		NB_CUDA(cudaMemcpyAsync(out, t.dState, n * 4, cudaMemcpyDeviceToHost, m_stream));
-		sync();
-		*len = n;
-		return;
-	}
+	getNetTypeState(0, netType, out, cap, len);
+}
+
+void Simulation::getNetTypeState(unsigned net, unsigned netType, float* out, size_t cap, size_t* len)
+{
+	if(net >= m_nets) NB_THROW(NEMO_INVALID_INPUT, "Invalid network index %u", net);
 	*len = 0;
+	if(netType >= m_netTypes[net].size()) return;
+	const NetTypeRange& r = m_netTypes[net][netType];
+	if(r.count == 0) return;
+	const HostType& t = m_types[r.hostType];
+	size_t n = (size_t) r.count * t.desc->nstate;
+	if(cap < n) NB_THROW(NEMO_BUFFER_OVERFLOW, "state buffer too small");
+	NB_CUDA(cudaSetDevice(m_device));
+	for(unsigned v = 0; v < t.desc->nstate; ++v) {
+		NB_CUDA(cudaMemcpyAsync(out + (size_t) v * r.count, t.dState + (size_t) v * t.n + r.offset,
+				(size_t) r.count * 4, cudaMemcpyDeviceToHost, m_stream));
+	}
+	sync();
+	*len = n;
 }
 
 unsigned long Simulation::elapsedWallclock() const

@@ -49,7 +49,9 @@ struct DevSim {
 	uint64_t* hist;           // [2][N] firing history, double-buffered by step parity
 	uint32_t* fstim;          // [W] pending firing stimulus
 	float* curExt;            // [N] pending current stimulus
-	longlong2* slots;         // [D][N] (E, I) fixed-point sums per delivery step
+	uint2* slots;             // [D][N] low words of the E and -I fixed-point sums per delivery step
+	int2* slotHigh;           // [D][N] their high words (touched only on carry/borrow)
+	uint32_t* slotFlag;       // [D] set when a slot holds a nonzero high word
 	const unsigned long long* outPtr; // [N+1] outgoing synapses per source
 	uint2* syn;               // [S] {target | (delay - 1) << 26, weight}
 	uint32_t* firedRing;      // [R][W] fired bit-vector per step
@@ -77,7 +79,11 @@ struct DevSim {
 class Simulation {
 public:
 	Simulation(const Network& net, const Configuration& conf);
+	// a batch of independent networks advanced together (each network's
+	// results are those of its own single-network simulation)
+	Simulation(const std::vector<const Network*>& nets, const Configuration& conf);
 	~Simulation();
+	unsigned networkCount() const { return m_nets; }
 
 	const std::vector<unsigned>& step(const unsigned* fstim, size_t nf,
 			const unsigned* inidx, const float* icur, size_t ni);
@@ -100,6 +106,7 @@ public:
 
 	void getWeightsFx(int32_t* out, size_t cap, size_t* len);
 	void getTypeState(unsigned netType, float* out, size_t cap, size_t* len);
+	void getNetTypeState(unsigned net, unsigned netType, float* out, size_t cap, size_t* len);
 	uint64_t synapseCount() const { return m_nsyn; }
 
 	unsigned long elapsedWallclock() const;
@@ -139,6 +146,8 @@ private:
 	void locate(unsigned g, const HostType** t, unsigned* i) const;
 	size_t synapseKey(uint64_t id) const;
 	void launchStep(bool fullRecord);
+	size_t decodeBatchStep(uint32_t r, unsigned step, unsigned* counts, unsigned* ids, size_t pos, size_t cap);
+	std::vector<std::vector<uint32_t>> m_batchScratch;
 	unsigned m_deliverGrid = 1184;
 	uint32_t m_P = 256, m_T = 256;
 	uint32_t m_maxOutDeg = 0, m_maxPlasticInDeg = 0;
@@ -155,7 +164,12 @@ private:
 	std::vector<HostType> m_types;
 	std::vector<unsigned> m_l2g;
 	std::vector<uint8_t> m_ltype;
-	std::unordered_map<unsigned, unsigned> m_g2l;
+	std::vector<unsigned> m_netLocal;  // index within its own network's local order
+	std::vector<uint32_t> m_netOf;     // network of each neuron (batches only)
+	std::vector<std::unordered_map<unsigned, unsigned>> m_g2l;  // per network: global id -> index
+	struct NetTypeRange { unsigned hostType, offset, count; };
+	std::vector<std::vector<NetTypeRange>> m_netTypes;  // per network and type id
+	unsigned m_nets = 1;
 
 	// synapse bookkeeping for queries: for local source l, the synapse with
 	// per-source index i is m_srcOrder[m_srcStart[l] + i] (an insertion-order

@@ -1242,12 +1242,19 @@ static double uniform_01(mt19937* g) { return (double) mt_next(g) / 4294967296.0
 int nemo_oracle_example_random(nemo_oracle_network** out, unsigned ncount, unsigned scount,
 		unsigned dmax, int stdp)
 {
+	return nemo_oracle_example_random_ex(out, ncount, scount, dmax, stdp, 5489u, 5.0f, 2.0f);
+}
+
+/* the same with the generator seed and the two noise sigmas as parameters */
+int nemo_oracle_example_random_ex(nemo_oracle_network** out, unsigned ncount, unsigned scount,
+		unsigned dmax, int stdp, unsigned seed, float sigmaExc, float sigmaInh)
+{
 	nemo_oracle_network* net = nemo_oracle_new_network();
 	if(!net) return fail(NEMO_ALLOCATION_ERROR, "allocation failed");
 	unsigned iz;
 	nemo_oracle_add_neuron_type(net, "Izhikevich", &iz);
 	mt19937 g;
-	mt_seed(&g, 5489u);
+	mt_seed(&g, seed);
 	unsigned* tgt = malloc((scount ? scount : 1) * sizeof(unsigned));
 	unsigned* dly = malloc((scount ? scount : 1) * sizeof(unsigned));
 	unsigned* src = malloc((scount ? scount : 1) * sizeof(unsigned));
@@ -1266,7 +1273,7 @@ int nemo_oracle_example_random(nemo_oracle_network** out, unsigned ncount, unsig
 			float c = v + 15.0f * r1 * r1;
 			float d = 8.0f - 6.0f * r2 * r2;
 			float u = b * v;
-			float sigma = 5.0f;
+			float sigma = sigmaExc;
 			float x[7] = { a, b, c, d, sigma, u, v };
 			memcpy(args, x, sizeof x);
 		} else {
@@ -1278,7 +1285,7 @@ int nemo_oracle_example_random(nemo_oracle_network** out, unsigned ncount, unsig
 			float c = v;
 			float d = 2.0f;
 			float u = b * v;
-			float sigma = 2.0f;
+			float sigma = sigmaInh;
 			float x[7] = { a, b, c, d, sigma, u, v };
 			memcpy(args, x, sizeof x);
 		}

@@ -99,6 +99,8 @@ int nemo_oracle_reset_timer(nemo_oracle_simulation*);
 /* The reference's example network (src/examples/random.cpp:63-88) */
 int nemo_oracle_example_random(nemo_oracle_network** out, unsigned ncount, unsigned scount,
 		unsigned dmax, int stdp);
+int nemo_oracle_example_random_ex(nemo_oracle_network** out, unsigned ncount, unsigned scount,
+		unsigned dmax, int stdp, unsigned seed, float sigma_exc, float sigma_inh);
 size_t nemo_oracle_network_synapse_count(nemo_oracle_network*);
 int nemo_oracle_network_synapses(nemo_oracle_network*, size_t cap,
 		unsigned* source, unsigned* target, unsigned* delay, float* weight,

@@ -78,6 +78,8 @@ def lib():
                 "nemo_oracle_nrand": (C.c_float, [u32p]),
                 "nemo_oracle_seed_states": (None, [C.c_uint, C.c_uint, u32p]),
                 "nemo_oracle_example_random": (i, [C.POINTER(vp), C.c_uint, C.c_uint, C.c_uint, C.c_int]),
+                "nemo_oracle_example_random_ex": (i, [C.POINTER(vp), C.c_uint, C.c_uint, C.c_uint, C.c_int, C.c_uint,
+                                                      C.c_float, C.c_float]),
                 "nemo_oracle_network_synapse_count": (sz, [vp]),
                 "nemo_oracle_network_synapses": (i, [vp, sz, u32p, u32p, u32p, f32p, u8p, C.POINTER(sz)]),
             }
@@ -184,10 +186,12 @@ class Network:
         return out
 
 
-def example_random(ncount: int, scount: int, dmax: int, stdp: bool) -> Network:
+def example_random(ncount: int, scount: int, dmax: int, stdp: bool, seed: int | None = None,
+                   sigma_exc: float = 5.0, sigma_inh: float = 2.0) -> Network:
     """The reference's random::construct (src/examples/random.cpp:63-88)."""
     h = C.c_void_p()
-    _check(lib().nemo_oracle_example_random(C.byref(h), ncount, scount, dmax, int(stdp)))
+    _check(lib().nemo_oracle_example_random_ex(C.byref(h), ncount, scount, dmax, int(stdp),
+                                               5489 if seed is None else seed, sigma_exc, sigma_inh))
     return Network(h.value)
 
 
