@@ -251,6 +251,8 @@ def run_b200(args, rank, world, local):
     conf.set_cuda_backend(local)
     sim = nb.Simulation(net, conf)
     del net
+    if args.no_graphs:
+        sim.set_graphs(False)
     build_s = time.perf_counter() - t0
     W = args.window
 
@@ -349,7 +351,8 @@ def run_b200(args, rank, world, local):
             "gpu_launches": args.steps * (2 * W + 1),
             "clocks": clk.summary(),
             "build_s": build_s,
-            "launch": {"partition": launch[0], "threads": launch[1], "autotuned_us_per_step": tuned_us},
+            "launch": {"partition": launch[0], "threads": launch[1], "autotuned_us_per_step": tuned_us,
+                       "cuda_graphs": not args.no_graphs},
             "spikes_per_neuron_s": st["fired"] / args.neurons / (args.steps * W / 1e3),
         }
         print(json.dumps(line), flush=True)
@@ -372,6 +375,7 @@ def main():
     ap.add_argument("--cpu-warm-ms", type=int, default=50)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-graphs", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

@@ -272,6 +272,9 @@ NEMO_B200_API nemo_status_t nemo_b200_get_type_state(nemo_simulation_t, unsigned
 NEMO_B200_API nemo_status_t nemo_b200_synapse_count(nemo_simulation_t, uint64_t* count);
 /* Turn per-launch CUDA-event timing of nemo_b200_run's kernels on or off. */
 NEMO_B200_API nemo_status_t nemo_b200_set_profiling(nemo_simulation_t, int on);
+/* Turn the CUDA-graph replay of nemo_b200_run's step loop (blocks of 100
+ * steps, captured once per launch shape) on (the default) or off. */
+NEMO_B200_API nemo_status_t nemo_b200_set_graphs(nemo_simulation_t, int on);
 /* Statistics of the last nemo_b200_run: its device time in ms (CUDA events
  * on the simulation's stream), and per kernel kind (0 = step kernel,
  * 1 = pending STDP accumulation, 2 = applyStdp) the summed device time and

@@ -334,6 +334,10 @@ class Simulation:
     def set_profiling(self, on: bool = True):
         _check(lib().nemo_b200_set_profiling(self._h, int(on)))
 
+    def set_graphs(self, on: bool = True):
+        """CUDA-graph replay of run()'s step loop (an extension; on by default)."""
+        _check(lib().nemo_b200_set_graphs(self._h, int(on)))
+
     def run_stats(self) -> dict:
         """Statistics of the last run() (an extension): device ms, per-kernel
         ms and launches (when profiling), spikes, events, STDP entries walked

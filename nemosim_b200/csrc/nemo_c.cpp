@@ -597,6 +597,12 @@ nemo_status_t nemo_b200_set_profiling(nemo_simulation_t s, int on)
 	CALL(S(s).profiling = on != 0);
 }
 
+nemo_status_t nemo_b200_set_graphs(nemo_simulation_t s, int on)
+{
+	NULLCHECK(s);
+	CALL(S(s).useGraphs = on != 0);
+}
+
 nemo_status_t nemo_b200_run_stats(nemo_simulation_t s, float* runMs, float kernelMs[3], unsigned launches[3],
 		uint64_t* fired, uint64_t* events, uint64_t* stdpEntries, uint64_t* plastic)
 {

@@ -33,6 +33,21 @@ namespace nemo_b200 {
 // independent loads in flight.
 
 constexpr uint32_t CHUNK = 128;  // entries per chunk: 4 per lane of a warp
+
+// Inside a CUDA graph the step's cycle comes from a device counter (the
+// graph is replayed at different cycles): cycle = *cycleDev + offset.
+__device__ __forceinline__ void step_indices(const DevSim& S, uint32_t offset, uint32_t& cur, uint32_t& slot, uint32_t& ring)
+{
+	const unsigned long long c = *S.cycleDev + offset;
+	cur = (uint32_t) (c & 1);
+	slot = S.D ? (uint32_t) (c % S.D) : 0u;
+	ring = (uint32_t) (c % S.R);
+}
+
+__global__ void advance_cycle_kernel(unsigned long long* cycle, uint32_t by)
+{
+	*cycle += by;
+}
 constexpr uint32_t ILP = CHUNK / 32;
 
 __device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t x)
@@ -79,8 +94,9 @@ __device__ __forceinline__ void write_chunks(uint4* list, uint32_t pos, unsigned
 // neurons starting at c * P (P a multiple of 32, so warps cover whole
 // bit-vector words); its blockDim.x threads loop over them.
 __global__ void __launch_bounds__(1024)
-update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t slot, uint32_t ring)
+update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t slot, uint32_t ring, uint32_t offset, int fromDev)
 {
+	if(fromDev) step_indices(S, offset, cur, slot, ring);
 	__shared__ uint32_t sFired;
 	__shared__ unsigned long long sEvents, sStdp;
 	const uint32_t tid = threadIdx.x, lane = tid & 31;
@@ -186,8 +202,12 @@ update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t slot, uint32_t 
 //  kind 1: STDP accumulation over the incoming plastic synapses of a target
 //          (ConnectivityMatrix::accumulateStdp, ConnectivityMatrix.cpp:193-227)
 __global__ void __launch_bounds__(STEP_THREADS)
-deliver_kernel(const DevSim S, uint32_t cur, uint32_t slot)
+deliver_kernel(const DevSim S, uint32_t cur, uint32_t slot, uint32_t offset, int fromDev)
 {
+	if(fromDev) {
+		uint32_t ring;
+		step_indices(S, offset, cur, slot, ring);
+	}
 	const uint32_t nch = S.chunkCount[cur];
 	if(blockIdx.x == 0 && threadIdx.x == 0) {
 		S.chunkCount[cur ^ 1u] = 0; // next step's list starts empty
@@ -205,7 +225,7 @@ deliver_kernel(const DevSim S, uint32_t cur, uint32_t slot)
 			uint2 s[ILP];
 #pragma unroll
 			for(uint32_t j = 0; j < ILP; ++j) {
-				if(lane + 32 * j < len) s[j] = S.syn[start + lane + 32 * j];
+				if(lane + 32 * j < len) s[j] = __ldcs(S.syn + start + lane + 32 * j);
 			}
 #pragma unroll
 			for(uint32_t j = 0; j < ILP; ++j) {
@@ -222,8 +242,8 @@ deliver_kernel(const DevSim S, uint32_t cur, uint32_t slot)
 #pragma unroll
 			for(uint32_t j = 0; j < ILP; ++j) {
 				if(lane + 32 * j < len) {
-					sd[j] = S.rcmSrc[start + lane + 32 * j];
-					acc[j] = S.rcmAcc[start + lane + 32 * j];
+					sd[j] = __ldcs(S.rcmSrc + start + lane + 32 * j);
+					acc[j] = __ldcs(S.rcmAcc + start + lane + 32 * j);
 				}
 			}
 #pragma unroll
@@ -235,7 +255,7 @@ deliver_kernel(const DevSim S, uint32_t cur, uint32_t slot)
 				if(lane + 32 * j < len) {
 					const uint32_t delay = (sd[j] >> 26) + 1;
 					const int32_t dw = stdp_weight_change(S.sp, h[j] >> (delay & 63));
-					if(dw != 0) S.rcmAcc[start + lane + 32 * j] = (int32_t) ((uint32_t) acc[j] + (uint32_t) dw);
+					if(dw != 0) __stcs(S.rcmAcc + start + lane + 32 * j, (int32_t) ((uint32_t) acc[j] + (uint32_t) dw));
 				}
 			}
 		}
@@ -287,9 +307,9 @@ apply_touched_kernel(const DevSim S, int32_t reward, uint32_t par, uint32_t slot
 		uint32_t fwd[ILP];
 		int32_t w[ILP];
 #pragma unroll
-		for(uint32_t j = 0; j < ILP; ++j) acc[j] = lane + 32 * j < len ? S.rcmAcc[start + lane + 32 * j] : 0;
+		for(uint32_t j = 0; j < ILP; ++j) acc[j] = lane + 32 * j < len ? __ldcs(S.rcmAcc + start + lane + 32 * j) : 0;
 #pragma unroll
-		for(uint32_t j = 0; j < ILP; ++j) if(acc[j]) fwd[j] = S.rcmFwd[start + lane + 32 * j];
+		for(uint32_t j = 0; j < ILP; ++j) if(acc[j]) fwd[j] = __ldcs(S.rcmFwd + start + lane + 32 * j);
 #pragma unroll
 		for(uint32_t j = 0; j < ILP; ++j) if(acc[j]) w[j] = (int32_t) S.syn[fwd[j]].y;
 #pragma unroll
@@ -748,6 +768,8 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	S.slots = S.D ? dalloc<uint2>((size_t) S.D * N) : nullptr;
 	S.slotHigh = S.D ? dalloc<int2>((size_t) S.D * N) : nullptr;
 	S.slotFlag = dalloc<uint32_t>(std::max(1u, S.D));
+	S.cycleDev = dalloc<unsigned long long>(1);
+	NB_CUDA(cudaMallocHost(&m_hCycle, 8));
 	S.R = (uint32_t) std::max<size_t>(16, std::min<size_t>(1024, (64u << 20) / ((size_t) S.W * 4)));
 	S.firedRing = dalloc<uint32_t>((size_t) S.R * S.W);
 	S.firedCount = dalloc<uint32_t>(S.R);
@@ -772,6 +794,8 @@ Simulation::~Simulation()
 	cudaSetDevice(m_device);
 	if(m_stream) cudaStreamSynchronize(m_stream);
 	for(void* p : m_allocs) cudaFree(p);
+	if(m_graph) cudaGraphExecDestroy(m_graph);
+	if(m_hCycle) cudaFreeHost(m_hCycle);
 	if(m_hFired) cudaFreeHost(m_hFired);
 	if(m_hStim) cudaFreeHost(m_hStim);
 	if(m_dStim) cudaFree(m_dStim);
@@ -837,13 +861,62 @@ void Simulation::launchStep(bool /*fullRecord*/)
 	const uint32_t ring = (uint32_t) (m_cycle % m_dev.R);
 	const unsigned grid = (m_N + m_P - 1) / m_P;
 	timedBegin(K_STEP);
-	update_kernel<<<grid, m_T, 0, m_stream>>>(m_dev, m_P, cur, slot, ring);
+	update_kernel<<<grid, m_T, 0, m_stream>>>(m_dev, m_P, cur, slot, ring, 0, 0);
 	timedEnd();
 	timedBegin(K_STDP);
-	deliver_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, cur, slot);
+	deliver_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, cur, slot, 0, 0);
 	timedEnd();
 	m_cycle++;
 	m_timerSteps++;
+}
+
+// n consecutive steps: whole CUDA graphs of GRAPH_STEPS steps (captured once
+// per launch shape and replayed from a device cycle counter), then single
+// launches for the rest
+void Simulation::launchSteps(unsigned n)
+{
+	if(!useGraphs || profiling || n < GRAPH_STEPS) {
+		for(unsigned i = 0; i < n; ++i) launchStep(false);
+		return;
+	}
+	if(!m_graph || m_graphP != m_P || m_graphT != m_T) buildGraph();
+	*m_hCycle = m_cycle;
+	NB_CUDA(cudaMemcpyAsync(m_dev.cycleDev, m_hCycle, 8, cudaMemcpyHostToDevice, m_stream));
+	while(n >= GRAPH_STEPS) {
+		NB_CUDA(cudaGraphLaunch(m_graph, m_stream));
+		m_cycle += GRAPH_STEPS;
+		m_timerSteps += GRAPH_STEPS;
+		n -= GRAPH_STEPS;
+	}
+	// the pinned cycle value must not change before the copy above ran
+	NB_CUDA(cudaStreamSynchronize(m_stream));
+	for(unsigned i = 0; i < n; ++i) launchStep(false);
+}
+
+void Simulation::buildGraph()
+{
+	if(m_graph) {
+		cudaGraphExecDestroy(m_graph);
+		m_graph = nullptr;
+	}
+	sync();
+	const unsigned grid = (m_N + m_P - 1) / m_P;
+	cudaGraph_t g;
+	NB_CUDA(cudaStreamBeginCapture(m_stream, cudaStreamCaptureModeThreadLocal));
+	for(unsigned k = 0; k < GRAPH_STEPS; ++k) {
+		update_kernel<<<grid, m_T, 0, m_stream>>>(m_dev, m_P, 0, 0, 0, k, 1);
+		deliver_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, 0, 0, k, 1);
+	}
+	advance_cycle_kernel<<<1, 1, 0, m_stream>>>(m_dev.cycleDev, GRAPH_STEPS);
+	NB_CUDA(cudaStreamEndCapture(m_stream, &g));
+	cudaError_t err = cudaGraphInstantiate(&m_graph, g, 0);
+	cudaGraphDestroy(g);
+	if(err != cudaSuccess) {
+		m_graph = nullptr;
+		NB_THROW(NEMO_CUDA_ERROR, "CUDA graph instantiation failed: %s", cudaGetErrorString(err));
+	}
+	m_graphP = m_P;
+	m_graphT = m_T;
 }
 
 const std::vector<unsigned>& Simulation::step(const unsigned* fstim, size_t nf,
@@ -978,9 +1051,12 @@ void Simulation::run(unsigned steps, unsigned stdpPeriod, float reward, unsigned
 		m_evUse.clear();
 		m_evNext = 0;
 		NB_CUDA(cudaEventRecord(m_ev0, m_stream));
-		for(unsigned i = 0; i < chunk; ++i) {
-			launchStep(false);
-			if(stdpPeriod && (done + i + 1) % stdpPeriod == 0) applyStdpDevice(R);
+		for(unsigned i = 0; i < chunk;) {
+			const unsigned untilApply = stdpPeriod ? stdpPeriod - (done + i) % stdpPeriod : chunk - i;
+			const unsigned seg = std::min(chunk - i, untilApply);
+			launchSteps(seg);
+			i += seg;
+			if(stdpPeriod && (done + i) % stdpPeriod == 0) applyStdpDevice(R);
 		}
 		NB_CUDA(cudaEventRecord(m_ev1, m_stream));
 		std::vector<uint32_t> hc(m_dev.R);

@@ -72,6 +72,7 @@ struct DevSim {
 	uint4* applyChunks;
 	uint32_t* applyChunkCount;
 	uint32_t* touchedBits;    // [W]
+	unsigned long long* cycleDev; // step counter read by kernels replayed from a CUDA graph
 	StdpParams sp;
 	LibmCalib calib;
 };
@@ -121,6 +122,7 @@ public:
 	unsigned kernelLaunches[K_KINDS] = {0, 0, 0};
 	uint64_t lastFired = 0, lastEvents = 0, lastStdpEntries = 0, lastPlastic = 0;
 	bool profiling = false;
+	bool useGraphs = true;  // replay the step loop from CUDA graphs in run()
 
 	// partition size (neurons per CTA) and threads per CTA of the step
 	// kernel; results do not depend on them
@@ -146,6 +148,12 @@ private:
 	void locate(unsigned g, const HostType** t, unsigned* i) const;
 	size_t synapseKey(uint64_t id) const;
 	void launchStep(bool fullRecord);
+	void launchSteps(unsigned n);
+	void buildGraph();
+	static constexpr unsigned GRAPH_STEPS = 100;
+	cudaGraphExec_t m_graph = nullptr;
+	uint32_t m_graphP = 0, m_graphT = 0;
+	unsigned long long* m_hCycle = nullptr;
 	size_t decodeBatchStep(uint32_t r, unsigned step, unsigned* counts, unsigned* ids, size_t pos, size_t cap);
 	std::vector<std::vector<uint32_t>> m_batchScratch;
 	unsigned m_deliverGrid = 1184;

@@ -166,6 +166,24 @@ def test_launch_shape_does_not_change_results(shape):
     assert np.array_equal(ref.weights_fx(450000), sim.weights_fx(450000))
 
 
+def test_graph_replay_matches_single_launches():
+    """run() replays 100-step CUDA graphs from a device cycle counter; the
+    results equal single launches, across applyStdp calls and remainders."""
+    a = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
+    b = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
+    b.set_graphs(False)
+    for steps, period in [(537, 100), (250, 0), (333, 70)]:
+        ra = a.run(steps, period, 1.0)
+        rb = b.run(steps, period, 1.0)
+        assert np.array_equal(ra[0], rb[0]) and np.array_equal(ra[2], rb[2])
+    a.set_launch(64, 64)  # the graph is rebuilt for the new shape
+    b.set_launch(64, 64)
+    ra = a.run(300, 100, 1.0)
+    rb = b.run(300, 100, 1.0)
+    assert np.array_equal(ra[2], rb[2])
+    assert np.array_equal(a.weights_fx(450000), b.weights_fx(450000))
+
+
 def test_autotune_restores_state():
     """The autotuner's trial steps leave the simulation exactly as it was."""
     ref = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
