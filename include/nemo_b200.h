@@ -309,6 +309,34 @@ NEMO_B200_API nemo_status_t nemo_b200_libm_calibration(uint64_t* log_flips, uint
  * (nemo_new_simulation and the like) that report failure only by returning
  * NULL. */
 NEMO_B200_API nemo_status_t nemo_b200_last_status(void);
+/* Differentiable float32 mode.  A network of `neurons` Izhikevich neurons
+ * with `synapses` delayed synapses (source[], target[], delay[] in 1..;
+ * ordered by source; synapse e has weight w[e]) run for `ms` milliseconds of
+ * 4 Euler sub-steps on `trials` independent noise inputs.  The loss is the
+ * mean squared error between the exp(-t/20 ms)-filtered spike trains of
+ * neurons 0..readout-1 and target rates; the backward pass is a hand-written
+ * BPTT adjoint with a fast-sigmoid surrogate (slope 10) for the threshold,
+ * replaying `checkpoint_ms`-long segments from state checkpoints.  smooth = 1
+ * replaces the threshold by the fast sigmoid itself in the forward pass.
+ * The float arrays of forward/backward are DEVICE pointers: w[synapses],
+ * a, b, c, d [neurons], noise [ms][trials][neurons] (the input current noise
+ * itself), target [ms][trials][readout], loss a device scalar, gradients
+ * dw[synapses], da, db [neurons]; `stream` is a cudaStream_t (NULL = default).
+ * backward differentiates the most recent forward call. */
+struct nemo_b200_bptt_class;
+typedef struct nemo_b200_bptt_class* nemo_b200_bptt_t;
+NEMO_B200_API nemo_b200_bptt_t nemo_b200_bptt_new(unsigned neurons, unsigned trials, unsigned ms, unsigned readout,
+		unsigned checkpoint_ms, size_t synapses, const unsigned source[], const unsigned target[],
+		const unsigned delay[], int smooth, int device);
+NEMO_B200_API void nemo_b200_bptt_delete(nemo_b200_bptt_t);
+NEMO_B200_API nemo_status_t nemo_b200_bptt_forward(nemo_b200_bptt_t, const float* w, const float* a, const float* b,
+		const float* c, const float* d, const float* noise, const float* target, float* loss, void* stream);
+/* The filtered readout spike trains of the most recent forward call, as a
+ * device array [ms][trials][readout] (e.g. the targets made by a teacher). */
+NEMO_B200_API nemo_status_t nemo_b200_bptt_readout(nemo_b200_bptt_t, float* out, void* stream);
+NEMO_B200_API nemo_status_t nemo_b200_bptt_backward(nemo_b200_bptt_t, const float* w, const float* a, const float* b,
+		const float* c, const float* d, const float* noise, const float* target, float* dw, float* da, float* db,
+		void* stream);
 /* Host build of the device's glibc-exact nrand (for tests): advances the
  * xorshift state in place and returns the normal deviate. */
 NEMO_B200_API float nemo_b200_host_nrand(unsigned state[4]);

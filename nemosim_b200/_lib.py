@@ -107,6 +107,12 @@ SIGNATURES = {
     "nemo_b200_neuron_type_name": (C.c_char_p, [C.c_uint]),
     "nemo_b200_libm_calibration": (st, [C.POINTER(C.c_uint64)] * 3),
     "nemo_b200_last_status": (st, []),
+    "nemo_b200_bptt_new": (vp, [C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_uint, sz, u32p, u32p, u32p,
+                                C.c_int, C.c_int]),
+    "nemo_b200_bptt_delete": (None, [vp]),
+    "nemo_b200_bptt_forward": (st, [vp] + [vp] * 8 + [vp]),
+    "nemo_b200_bptt_backward": (st, [vp] + [vp] * 10 + [vp]),
+    "nemo_b200_bptt_readout": (st, [vp, vp, vp]),
     "nemo_b200_host_nrand": (C.c_float, [u32p]),
 }
 

@@ -14,6 +14,7 @@
 
 #include "../../include/nemo_b200.h"
 #include "libm_calib.hpp"
+#include "bptt.hpp"
 #include "handles.hpp"
 #include "network.hpp"
 #include "simulation.hpp"
@@ -667,6 +668,53 @@ nemo_status_t nemo_b200_libm_calibration(uint64_t* logFlips, uint64_t* sinFlips,
 }
 
 nemo_status_t nemo_b200_last_status(void) { return g_lastStatus; }
+
+nemo_b200_bptt_t nemo_b200_bptt_new(unsigned neurons, unsigned trials, unsigned ms, unsigned readout,
+		unsigned checkpoint_ms, size_t synapses, const unsigned source[], const unsigned target[],
+		const unsigned delay[], int smooth, int device)
+{
+	g_lastStatus = NEMO_OK;
+	try {
+		auto* h = new nemo_b200_bptt_class();
+		try {
+			h->impl.reset(new Bptt(neurons, trials, ms, readout, checkpoint_ms, synapses, source, target, delay,
+					smooth, device));
+		} catch(...) {
+			delete h;
+			throw;
+		}
+		return h;
+	} catch(const Error& e) {
+		setResult(e.what(), e.code());
+	} catch(const std::exception& e) {
+		setResult(e.what(), NEMO_UNKNOWN_ERROR);
+	}
+	return nullptr;
+}
+
+void nemo_b200_bptt_delete(nemo_b200_bptt_t h) { delete h; }
+
+nemo_status_t nemo_b200_bptt_forward(nemo_b200_bptt_t h, const float* w, const float* a, const float* b,
+		const float* c, const float* d, const float* noise, const float* target, float* loss, void* stream)
+{
+	NULLCHECK(h);
+	CALL(h->impl->forward(BpttParams{ w, a, b, c, d, noise, target }, loss, stream));
+}
+
+nemo_status_t nemo_b200_bptt_readout(nemo_b200_bptt_t h, float* out, void* stream)
+{
+	NULLCHECK(h);
+	NULLCHECK(out);
+	CALL(h->impl->readout(out, stream));
+}
+
+nemo_status_t nemo_b200_bptt_backward(nemo_b200_bptt_t h, const float* w, const float* a, const float* b,
+		const float* c, const float* d, const float* noise, const float* target, float* dw, float* da, float* db,
+		void* stream)
+{
+	NULLCHECK(h);
+	CALL(h->impl->backward(BpttParams{ w, a, b, c, d, noise, target }, dw, da, db, stream));
+}
 
 float nemo_b200_host_nrand(unsigned state[4])
 {
