@@ -21,8 +21,10 @@ wall second.
            buffers: a one-neuron firing stimulus goes host->device and the
            fired bit-vector comes back every step (src/examples/common.cpp
            --fstim), plus nemo_apply_stdp every 100 ms
-  roofline the step kernel's algorithmic bytes per launch / its measured
-           average duration, against the measured HBM copy bandwidth
+  roofline the step loop's algorithmic bytes per launch / its measured
+           average duration (CUDA events around each launch), against the
+           measured HBM copy bandwidth; the persistent loop runs one period
+           per launch
   --impl reference  the CPU oracle (a restatement of the reference CPU
            backend; the reference itself cannot be built here) on the host
 
@@ -95,33 +97,42 @@ def measured_peak_gbs():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """nvidia-smi clocks and throttle reasons during the timed region: the
+    sampler is running (its first row has arrived) before the region starts,
+    and only rows that arrive inside the region are summarised."""
 
     FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    INTERVAL_MS = 50
 
     def __init__(self, gpu: int):
         self.gpu = gpu
-        self.rows = []
+        self.rows = []  # (arrival time, fields)
         self.proc = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+                 "-lms", str(self.INTERVAL_MS)], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.monotonic() + 10
+            while not self.rows and time.monotonic() < deadline and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
+        self.t0 = time.monotonic()
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            self.rows.append((time.monotonic(), [x.strip() for x in line.split(",")]))
 
     def __exit__(self, *exc):
+        self.t1 = time.monotonic()
         if self.proc:
             self.proc.terminate()
             try:
@@ -131,18 +142,19 @@ class ClockSampler:
             self.t.join(timeout=2)
 
     def summary(self) -> dict:
-        if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["not sampled"]}
-        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        inside = [r for t, r in self.rows if self.t0 <= t <= self.t1]
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["not sampled"], "samples": 0}
+        sm = [float(r[1]) for r in inside if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in inside if len(r) > 2 and r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
-        for r in self.rows:
+        for r in inside:
             for k, n in enumerate(names):
                 if len(r) > 5 + k and r[5 + k].lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+                "reasons": sorted(reasons), "samples": len(inside), "interval_ms": self.INTERVAL_MS}
 
 
 def dist_setup(args):
@@ -253,6 +265,8 @@ def run_b200(args, rank, world, local):
     del net
     if args.no_graphs:
         sim.set_graphs(False)
+    if args.no_persistent:
+        sim.set_persistent(False)
     build_s = time.perf_counter() - t0
     W = args.window
 
@@ -279,13 +293,22 @@ def run_b200(args, rank, world, local):
     sim.run(W * kp, W, 1.0, ids=False)
     sim.set_profiling(False)
     ps = sim.run_stats()
-    nsteps_p = max(1, ps["kernel_launches"]["step"])
-    upd_ms = ps["kernel_ms"]["step"] / nsteps_p
-    dlv_ms = ps["kernel_ms"]["stdp"] / max(1, ps["kernel_launches"]["stdp"])
-    # algorithmic bytes per launch of each kernel of the step
-    upd_bytes = (args.neurons * B_NEURON * nsteps_p + ps["fired"] * B_FIRED) / nsteps_p
-    dlv_bytes = (ps["events"] * B_EVENT + ps["stdp_entries"] * B_STDP) / nsteps_p
-    kernels = {"update_kernel": (upd_bytes, upd_ms), "deliver_kernel": (dlv_bytes, dlv_ms)}
+    steps_p = kp * W
+    persistent = ps["kernel_launches"]["run"] > 0
+    if persistent:
+        # one launch of the persistent step loop per STDP period
+        nl = ps["kernel_launches"]["run"]
+        run_bytes = (args.neurons * B_NEURON * steps_p + ps["fired"] * B_FIRED + ps["events"] * B_EVENT
+                     + ps["stdp_entries"] * B_STDP) / nl
+        kernels = {"run_kernel": (run_bytes, ps["kernel_ms"]["run"] / nl)}
+    else:
+        nsteps_p = max(1, ps["kernel_launches"]["step"])
+        upd_ms = ps["kernel_ms"]["step"] / nsteps_p
+        dlv_ms = ps["kernel_ms"]["stdp"] / max(1, ps["kernel_launches"]["stdp"])
+        # algorithmic bytes per launch of each kernel of the step
+        upd_bytes = (args.neurons * B_NEURON * nsteps_p + ps["fired"] * B_FIRED) / nsteps_p
+        dlv_bytes = (ps["events"] * B_EVENT + ps["stdp_entries"] * B_STDP) / nsteps_p
+        kernels = {"update_kernel": (upd_bytes, upd_ms), "deliver_kernel": (dlv_bytes, dlv_ms)}
     dominant = max(kernels, key=lambda k: kernels[k][1])
     alg_bytes, step_ms = kernels[dominant]
     achieved = alg_bytes / (step_ms / 1e3) / 1e9
@@ -348,11 +371,15 @@ def run_b200(args, rank, world, local):
             "e2e": {"value": e2e_events / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 4 * W,
                     "d2h_bytes_per_step": 4 * words * W, "api": "nemo_step + nemo_apply_stdp (C ABI)",
                     "sim_ms_per_s": ke * W / e2e_s},
-            "gpu_launches": args.steps * (2 * W + 1),
+            # per period: the persistent loop (or 100 update + deliver launches,
+            # plus the graph's cycle-counter kernel), then applyStdp's collect
+            # and apply kernels
+            "gpu_launches": args.steps * ((1 if persistent else 2 * W + (W // 100)) + 2),
             "clocks": clk.summary(),
             "build_s": build_s,
             "launch": {"partition": launch[0], "threads": launch[1], "autotuned_us_per_step": tuned_us,
-                       "cuda_graphs": not args.no_graphs},
+                       "step_loop": "persistent cooperative launch per period" if persistent
+                       else "two launches per step" + ("" if args.no_graphs else ", CUDA graphs of 100 steps")},
             "spikes_per_neuron_s": st["fired"] / args.neurons / (args.steps * W / 1e3),
         }
         print(json.dumps(line), flush=True)
@@ -365,7 +392,7 @@ def run_b200(args, rank, world, local):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--neurons", type=int, default=NEURONS)
@@ -376,6 +403,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-graphs", action="store_true")
+    ap.add_argument("--no-persistent", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

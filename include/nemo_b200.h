@@ -272,21 +272,29 @@ NEMO_B200_API nemo_status_t nemo_b200_get_type_state(nemo_simulation_t, unsigned
 NEMO_B200_API nemo_status_t nemo_b200_synapse_count(nemo_simulation_t, uint64_t* count);
 /* Turn per-launch CUDA-event timing of nemo_b200_run's kernels on or off. */
 NEMO_B200_API nemo_status_t nemo_b200_set_profiling(nemo_simulation_t, int on);
-/* Turn the CUDA-graph replay of nemo_b200_run's step loop (blocks of 100
- * steps, captured once per launch shape) on (the default) or off. */
+/* Turn the CUDA-graph replay of nemo_b200_run's two-launch step loop
+ * (blocks of 100 steps, captured once per launch shape) on (the default) or
+ * off. */
 NEMO_B200_API nemo_status_t nemo_b200_set_graphs(nemo_simulation_t, int on);
+/* Choose how nemo_b200_run advances the steps between applyStdp calls: one
+ * persistent cooperative launch per segment, its update and delivery phases
+ * separated by grid barriers (on, the default), or two launches per step
+ * (off).  nemo_step always uses two launches.  Results are identical. */
+NEMO_B200_API nemo_status_t nemo_b200_set_persistent(nemo_simulation_t, int on);
 /* Statistics of the last nemo_b200_run: its device time in ms (CUDA events
- * on the simulation's stream), and per kernel kind (0 = step kernel,
- * 1 = pending STDP accumulation, 2 = applyStdp) the summed device time and
- * launch count when profiling is on; the spikes, synaptic events and STDP
- * reverse-matrix entries walked in the run; and the number of plastic
- * synapses.  Any output pointer may be NULL. */
+ * on the simulation's stream), and per kernel kind (0 = update kernel and
+ * 1 = deliver kernel of the two-launch step, 2 = applyStdp, 3 = persistent
+ * step loop) the summed device time and launch count when profiling is on;
+ * the spikes, synaptic events and STDP reverse-matrix entries walked in the
+ * run; and the number of plastic synapses.  Any output pointer may be NULL. */
 NEMO_B200_API nemo_status_t nemo_b200_run_stats(nemo_simulation_t, float* run_ms,
-		float kernel_ms[3], unsigned kernel_launches[3],
+		float kernel_ms[4], unsigned kernel_launches[4],
 		uint64_t* fired, uint64_t* events, uint64_t* stdp_entries, uint64_t* plastic_synapses);
-/* Launch shape of the per-step kernel: neurons per CTA ("partition",
- * rounded up to a multiple of 32, at most 2048) and threads per CTA (a
- * multiple of 32, at most 1024).  Results are identical for every shape. */
+/* Launch shape of the active step loop: neurons per partition (rounded up
+ * to a multiple of 32; at most 2048 for the two-launch step, where a CTA
+ * owns one partition; a CTA of the persistent loop owns one or more) and
+ * threads per CTA (a multiple of 32, at most 1024; 64 to 384 for the
+ * persistent loop).  Results are identical for every shape. */
 NEMO_B200_API nemo_status_t nemo_b200_set_launch(nemo_simulation_t, unsigned partition, unsigned threads);
 NEMO_B200_API nemo_status_t nemo_b200_get_launch(nemo_simulation_t, unsigned* partition, unsigned* threads);
 /* Autotuner: times candidate launch shapes on `trial_steps` steps each,
@@ -316,8 +324,14 @@ NEMO_B200_API nemo_status_t nemo_b200_last_status(void);
  * mean squared error between the exp(-t/20 ms)-filtered spike trains of
  * neurons 0..readout-1 and target rates; the backward pass is a hand-written
  * BPTT adjoint with a fast-sigmoid surrogate (slope 10) for the threshold,
- * replaying `checkpoint_ms`-long segments from state checkpoints.  smooth = 1
- * replaces the threshold by the fast sigmoid itself in the forward pass.
+ * replaying `checkpoint_ms`-long segments from state checkpoints.
+ * `options` is a bit set: NEMO_B200_BPTT_SMOOTH replaces the threshold by the
+ * fast sigmoid itself in the forward pass; NEMO_B200_BPTT_FP64_STATE keeps
+ * the neuron state, the stored trajectories and the adjoints in float64
+ * (inputs and gradients stay float32), which reproduces a float64
+ * evaluation of the gradient; without it they are float32, and the
+ * gradient's rounding error is that of a float32 evaluation (about 1e-2
+ * relative on chaotic spiking networks).
  * The float arrays of forward/backward are DEVICE pointers: w[synapses],
  * a, b, c, d [neurons], noise [ms][trials][neurons] (the input current noise
  * itself), target [ms][trials][readout], loss a device scalar, gradients
@@ -325,9 +339,11 @@ NEMO_B200_API nemo_status_t nemo_b200_last_status(void);
  * backward differentiates the most recent forward call. */
 struct nemo_b200_bptt_class;
 typedef struct nemo_b200_bptt_class* nemo_b200_bptt_t;
+#define NEMO_B200_BPTT_SMOOTH 1
+#define NEMO_B200_BPTT_FP64_STATE 2
 NEMO_B200_API nemo_b200_bptt_t nemo_b200_bptt_new(unsigned neurons, unsigned trials, unsigned ms, unsigned readout,
 		unsigned checkpoint_ms, size_t synapses, const unsigned source[], const unsigned target[],
-		const unsigned delay[], int smooth, int device);
+		const unsigned delay[], int options, int device);
 NEMO_B200_API void nemo_b200_bptt_delete(nemo_b200_bptt_t);
 NEMO_B200_API nemo_status_t nemo_b200_bptt_forward(nemo_b200_bptt_t, const float* w, const float* a, const float* b,
 		const float* c, const float* d, const float* noise, const float* target, float* loss, void* stream);

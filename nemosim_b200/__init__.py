@@ -338,16 +338,24 @@ class Simulation:
         """CUDA-graph replay of run()'s step loop (an extension; on by default)."""
         _check(lib().nemo_b200_set_graphs(self._h, int(on)))
 
+    def set_persistent(self, on: bool = True):
+        """run()'s step loop as one persistent cooperative launch per segment
+        between applyStdp calls (an extension; on by default) or as two
+        launches per step."""
+        _check(lib().nemo_b200_set_persistent(self._h, int(on)))
+
     def run_stats(self) -> dict:
         """Statistics of the last run() (an extension): device ms, per-kernel
-        ms and launches (when profiling), spikes, events, STDP entries walked
-        and the number of plastic synapses."""
+        ms and launches (when profiling; "step" and "stdp" are the update and
+        deliver kernels of the two-launch step, "run" the persistent loop),
+        spikes, events, STDP entries walked and the number of plastic
+        synapses."""
         run_ms = C.c_float()
-        kms = (C.c_float * 3)()
-        kl = (C.c_uint * 3)()
+        kms = (C.c_float * 4)()
+        kl = (C.c_uint * 4)()
         vals = [C.c_uint64() for _ in range(4)]
         _check(lib().nemo_b200_run_stats(self._h, C.byref(run_ms), kms, kl, *[C.byref(v) for v in vals]))
-        names = ("step", "stdp", "apply")
+        names = ("step", "stdp", "apply", "run")
         return {"run_ms": run_ms.value,
                 "kernel_ms": {n: kms[i] for i, n in enumerate(names)},
                 "kernel_launches": {n: kl[i] for i, n in enumerate(names)},

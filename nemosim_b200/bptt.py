@@ -1,5 +1,9 @@
 """Differentiable float32 mode: the hand-written BPTT adjoint of the native
 library (nemosim_b200/csrc/bptt.cu) behind a ``torch.autograd.Function``.
+Weights, parameters, noise, targets and gradients are float32 tensors; the
+neuron state and adjoints are float32 or, with ``state_dtype=torch.float64``,
+float64 (the gradient of a spiking network amplifies rounding, so only the
+latter matches a float64 evaluation to 1e-4).
 
 The model: Izhikevich neurons with 4 Euler sub-steps per ms (as
 src/nemo/cpu/plugins/Izhikevich.cpp), a reset after every sub-step, delayed
@@ -76,25 +80,33 @@ class DifferentiableNetwork:
         return (torch.tensor(self.c, device=device, dtype=dtype), torch.tensor(self.d, device=device, dtype=dtype))
 
     def model(self, trials: int, ms: int, readout: int, checkpoint_ms: int = 50, smooth: bool = False,
-              device: int | None = None) -> "BpttModel":
-        return BpttModel(self, trials, ms, readout, checkpoint_ms, smooth, device)
+              device: int | None = None, state_dtype: torch.dtype = torch.float32) -> "BpttModel":
+        """``state_dtype=torch.float64`` keeps neuron state, trajectories and
+        adjoints in float64 (inputs and gradients stay float32)."""
+        return BpttModel(self, trials, ms, readout, checkpoint_ms, smooth, device, state_dtype)
 
 
 class BpttModel:
     """Device buffers of one differentiable network configuration (the
     native handle of nemo_b200_bptt_new)."""
 
+    SMOOTH, FP64_STATE = 1, 2  # option bits of nemo_b200_bptt_new
+
     def __init__(self, net: DifferentiableNetwork, trials: int, ms: int, readout: int, checkpoint_ms: int,
-                 smooth: bool, device: int | None):
+                 smooth: bool, device: int | None, state_dtype: torch.dtype = torch.float32):
+        if state_dtype not in (torch.float32, torch.float64):
+            raise ValueError("state_dtype must be torch.float32 or torch.float64")
         self.net = net
         self.trials, self.ms, self.readout = trials, ms, readout
+        self.state_dtype = state_dtype
         dev = torch.cuda.current_device() if device is None else device
         self.device = torch.device("cuda", dev)
         src = np.ascontiguousarray(net.source, np.uint32)
         tgt = np.ascontiguousarray(net.target, np.uint32)
         dly = np.ascontiguousarray(net.delay, np.uint32)
+        options = (self.SMOOTH if smooth else 0) | (self.FP64_STATE if state_dtype == torch.float64 else 0)
         h = lib().nemo_b200_bptt_new(net.neurons, trials, ms, readout, checkpoint_ms, len(src), src, tgt, dly,
-                                     int(smooth), dev)
+                                     options, dev)
         if not h:
             raise NemoError(lib().nemo_b200_last_status(), lib().nemo_strerror().decode())
         self._h = h
@@ -121,7 +133,7 @@ class BpttModel:
         _check(lib().nemo_b200_bptt_forward(self._h, *self._ptrs(W, a, b, self.c, self.d, noise, target, loss), stream))
         return loss
 
-    def readout(self, W, a, b, noise) -> torch.Tensor:
+    def readout_trains(self, W, a, b, noise) -> torch.Tensor:
         """Forward pass without a target; returns the filtered readout spike
         trains [ms, trials, readout] (a teacher's targets)."""
         target = torch.zeros((self.ms, self.trials, self.readout), device=self.device, dtype=torch.float32)

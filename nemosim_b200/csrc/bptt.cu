@@ -1,6 +1,6 @@
-// bptt.cu -- differentiable float32 mode: a network of Izhikevich neurons
-// with delayed synapses, run forward with checkpoints and differentiated by
-// a hand-written backpropagation-through-time adjoint.
+// bptt.cu -- differentiable mode: a network of Izhikevich neurons with
+// delayed synapses, run forward with checkpoints and differentiated by a
+// hand-written backpropagation-through-time adjoint.
 //
 // Model (per trial b, neuron n, millisecond t; 4 Euler sub-steps per ms as
 // in src/nemo/cpu/plugins/Izhikevich.cpp, with a reset after every sub-step
@@ -17,16 +17,25 @@
 // and g(x) = f'(x) = k / (2 (1 + k|x|)^2) is the surrogate derivative used
 // for H in the backward pass.  Initial state v = -65, u = b v.
 //
-// Layouts (float32): spikes S and input adjoints lambda_I as [n][t][b];
-// states [n][b]; noise and targets as PyTorch tensors [T][B][N] and [T][B][R].
-// One thread per (neuron, trial); 16 trials of one neuron are 64 contiguous
-// bytes.  Checkpoints of (v, u) every `ckpt` ms; the backward pass replays
-// each segment from its checkpoint and keeps the per-ms start states and
-// synaptic inputs of that segment.
+// Every kernel is a template over the state type Real (float or double):
+// the caller's weights, parameters, noise, targets, loss and gradients are
+// float32 either way; Real is the type of the neuron state, the stored
+// trajectories and the adjoints.  Gradients of this model are sensitive to
+// rounding (the spike upstroke amplifies a state perturbation many times
+// over), so float32 state gives gradients within about 1e-2 of the exact
+// ones, while float64 state reproduces a float64 evaluation.
+//
+// Layouts: spikes S and input adjoints lambda_I as [n][t][b]; states [n][b];
+// noise and targets as PyTorch tensors [T][B][N] and [T][B][R].  One thread
+// per (neuron, trial); the 16 trials of one neuron are contiguous.
+// Checkpoints of (v, u) every `ckpt` ms; the backward pass replays each
+// segment from its checkpoint and keeps the per-ms start states and synaptic
+// inputs of that segment.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "../../include/nemo_b200.h"
@@ -43,258 +52,268 @@ namespace nemo_b200 {
 		}                                                                          \
 	} while(0)
 
-constexpr float BP_K = 10.0f;
-
-__device__ __forceinline__ float spike_fn(float x, int smooth)
+template<typename Real>
+__device__ __forceinline__ Real spike_fn(Real x, int smooth)
 {
-	if(smooth) return 0.5f * (1.0f + BP_K * x / (1.0f + BP_K * fabsf(x)));
-	return x >= 0.0f ? 1.0f : 0.0f;
+	const Real k = Real(10);
+	if(smooth) return Real(0.5) * (Real(1) + k * x / (Real(1) + k * fabs(x)));
+	return x >= Real(0) ? Real(1) : Real(0);
 }
 
-__device__ __forceinline__ float spike_grad(float x)
+template<typename Real>
+__device__ __forceinline__ Real spike_grad(Real x)
 {
-	const float q = 1.0f + BP_K * fabsf(x);
-	return 0.5f * BP_K / (q * q);
+	const Real q = Real(1) + Real(10) * fabs(x);
+	return Real(0.5) * Real(10) / (q * q);
 }
 
 // synaptic input of (n, b) at ms t from the stored spikes
-__device__ __forceinline__ float syn_input(const BpttDev& D, const float* W, int n, int b, int t)
+template<typename Real>
+__device__ __forceinline__ Real syn_input(const BpttDev& D, const BpttState<Real>& X, const float* W, int n, int b, int t)
 {
-	float syn = 0.0f;
+	Real syn = Real(0);
 	for(int e = D.inStart[n]; e < D.inStart[n + 1]; ++e) {
 		const int dl = D.inDelay[e];
-		if(t >= dl) syn = fmaf(W[D.inSyn[e]], D.S[((size_t) D.inSrc[e] * D.T + (t - dl)) * D.B + b], syn);
+		if(t >= dl) syn = fma((Real) W[D.inSyn[e]], X.S[((size_t) D.inSrc[e] * D.T + (t - dl)) * D.B + b], syn);
 	}
 	return syn;
 }
 
-// the four sub-steps of one ms; returns S(t)
-__device__ __forceinline__ float substeps(float& v, float& u, float I, float a, float b, float c, float d, int smooth)
+// one Euler sub-step and its reset; returns s
+template<typename Real>
+__device__ __forceinline__ Real substep(Real& v, Real& u, Real& v1, Real I, Real a, Real b, Real c, Real d, int smooth)
 {
-	float St = 0.0f;
+	v1 = v + Real(0.25) * (Real(0.04) * v * v + Real(5) * v + Real(140) - u + I);
+	const Real u1 = u + Real(0.25) * a * (b * v1 - u);
+	const Real s = spike_fn(v1 - Real(30), smooth);
+	v = v1 + s * (c - v1);
+	u = u1 + s * d;
+	return s;
+}
+
+// the four sub-steps of one ms; returns S(t)
+template<typename Real>
+__device__ __forceinline__ Real substeps(Real& v, Real& u, Real I, Real a, Real b, Real c, Real d, int smooth)
+{
+	Real St = Real(0), v1;
 #pragma unroll
-	for(int k = 0; k < 4; ++k) {
-		const float v1 = v + 0.25f * (0.04f * v * v + 5.0f * v + 140.0f - u + I);
-		const float u1 = u + 0.25f * a * (b * v1 - u);
-		const float s = spike_fn(v1 - 30.0f, smooth);
-		v = v1 + s * (c - v1);
-		u = u1 + s * d;
-		St += s;
-	}
+	for(int k = 0; k < 4; ++k) St += substep(v, u, v1, I, a, b, c, d, smooth);
 	return St;
 }
 
-__global__ void bptt_init_kernel(BpttDev D, BpttParams P)
+template<typename Real>
+__global__ void bptt_init_kernel(BpttDev D, BpttState<Real> X, BpttParams P)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if(i >= D.N * D.B) return;
 	const int n = i / D.B, b = i % D.B;
-	D.v[i] = -65.0f;
-	D.u[i] = P.b[n] * -65.0f;
-	D.lossPart[i] = 0.0f;
-	D.lamV[i] = 0.0f;
-	D.lamU[i] = 0.0f;
-	D.gA[i] = 0.0f;
-	D.gB[i] = 0.0f;
-	if(n < D.R) {
-		D.r[n * D.B + b] = 0.0f;
-		D.lamR[n * D.B + b] = 0.0f;
-	}
+	X.v[i] = Real(-65);
+	X.u[i] = (Real) P.b[n] * Real(-65);
+	X.lossPart[i] = Real(0);
+	if(n < D.R) X.r[n * D.B + b] = Real(0);
 }
 
 // forward: one ms for every (neuron, trial)
-__global__ void bptt_forward_kernel(BpttDev D, BpttParams P, int t)
+template<typename Real>
+__global__ void bptt_forward_kernel(BpttDev D, BpttState<Real> X, BpttParams P, int t)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if(i >= D.N * D.B) return;
 	const int n = i / D.B, b = i % D.B;
-	float v = D.v[i], u = D.u[i];
+	Real v = X.v[i], u = X.u[i];
 	if(t % D.ckpt == 0) {
 		const size_t k = (size_t) (t / D.ckpt) * D.N * D.B + i;
-		D.ckV[k] = v;
-		D.ckU[k] = u;
+		X.ckV[k] = v;
+		X.ckU[k] = u;
 	}
-	const float I = syn_input(D, P.W, n, b, t) + P.noise[((size_t) t * D.B + b) * D.N + n];
-	const float St = substeps(v, u, I, P.a[n], P.b[n], P.c[n], P.d[n], D.smooth);
-	D.S[((size_t) n * D.T + t) * D.B + b] = St;
-	D.v[i] = v;
-	D.u[i] = u;
+	const Real I = syn_input(D, X, P.W, n, b, t) + (Real) P.noise[((size_t) t * D.B + b) * D.N + n];
+	const Real St = substeps(v, u, I, (Real) P.a[n], (Real) P.b[n], (Real) P.c[n], (Real) P.d[n], D.smooth);
+	X.S[((size_t) n * D.T + t) * D.B + b] = St;
+	X.v[i] = v;
+	X.u[i] = u;
 	if(n < D.R) {
-		const float r = D.alpha * D.r[n * D.B + b] + St;
-		D.r[n * D.B + b] = r;
-		D.rHist[((size_t) n * D.T + t) * D.B + b] = r;
-		const float diff = r - P.target[((size_t) t * D.B + b) * D.R + n];
-		D.lossPart[i] += diff * diff;
+		const Real r = X.alpha * X.r[n * D.B + b] + St;
+		X.r[n * D.B + b] = r;
+		X.rHist[((size_t) n * D.T + t) * D.B + b] = r;
+		const Real diff = r - (Real) P.target[((size_t) t * D.B + b) * D.R + n];
+		X.lossPart[i] += diff * diff;
 	}
 }
 
-// deterministic final reduction of the loss (one block)
-__global__ void bptt_loss_kernel(BpttDev D, float* loss)
+// deterministic final reduction of the loss (one block of 1024 threads)
+template<typename Real>
+__global__ void bptt_loss_kernel(BpttDev D, BpttState<Real> X, float* loss)
 {
-	__shared__ float part[1024];
-	float s = 0.0f;
-	for(int i = threadIdx.x; i < D.R * D.B; i += blockDim.x) s += D.lossPart[i];
+	__shared__ Real part[1024];
+	Real s = Real(0);
+	for(int i = threadIdx.x; i < D.R * D.B; i += blockDim.x) s += X.lossPart[i];
 	part[threadIdx.x] = s;
 	__syncthreads();
 	for(int o = blockDim.x / 2; o > 0; o >>= 1) {
 		if((int) threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
 		__syncthreads();
 	}
-	if(threadIdx.x == 0) *loss = part[0] * D.lossScale;
+	if(threadIdx.x == 0) *loss = (float) (part[0] * X.lossScale);
 }
 
 // backward, segment replay: ms t of the segment starting at t0 (identical
 // arithmetic to the forward pass), keeping its start state and input
-__global__ void bptt_replay_kernel(BpttDev D, BpttParams P, int t, int t0)
+template<typename Real>
+__global__ void bptt_replay_kernel(BpttDev D, BpttState<Real> X, BpttParams P, int t, int t0)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if(i >= D.N * D.B) return;
 	const int n = i / D.B, b = i % D.B;
-	float v, u;
+	Real v, u;
 	if(t == t0) {
 		const size_t k = (size_t) (t0 / D.ckpt) * D.N * D.B + i;
-		v = D.ckV[k];
-		u = D.ckU[k];
+		v = X.ckV[k];
+		u = X.ckU[k];
 	} else {
-		v = D.v[i];
-		u = D.u[i];
+		v = X.v[i];
+		u = X.u[i];
 	}
-	const float syn = syn_input(D, P.W, n, b, t);
+	const Real syn = syn_input(D, X, P.W, n, b, t);
 	const size_t s = (size_t) (t - t0) * D.N * D.B + i;
-	D.segV[s] = v;
-	D.segU[s] = u;
-	D.segSyn[s] = syn;
-	substeps(v, u, syn + P.noise[((size_t) t * D.B + b) * D.N + n], P.a[n], P.b[n], P.c[n], P.d[n], D.smooth);
-	D.v[i] = v;
-	D.u[i] = u;
+	X.segV[s] = v;
+	X.segU[s] = u;
+	X.segSyn[s] = syn;
+	substeps(v, u, syn + (Real) P.noise[((size_t) t * D.B + b) * D.N + n], (Real) P.a[n], (Real) P.b[n],
+			(Real) P.c[n], (Real) P.d[n], D.smooth);
+	X.v[i] = v;
+	X.u[i] = u;
 }
 
 // backward: adjoint of ms t for every (neuron, trial)
-__global__ void bptt_backward_kernel(BpttDev D, BpttParams P, int t, int t0)
+template<typename Real>
+__global__ void bptt_backward_kernel(BpttDev D, BpttState<Real> X, BpttParams P, int t, int t0)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if(i >= D.N * D.B) return;
 	const int n = i / D.B, b = i % D.B;
 
 	// dL/dS(t): readout trace and the inputs S(t) drives d ms later
-	float lamS = 0.0f;
+	Real lamS = Real(0);
 	if(n < D.R) {
-		const float r = D.rHist[((size_t) n * D.T + t) * D.B + b];
-		const float diff = r - P.target[((size_t) t * D.B + b) * D.R + n];
-		const float lr = 2.0f * D.lossScale * diff + D.alpha * D.lamR[n * D.B + b];
-		D.lamR[n * D.B + b] = lr;
+		const Real r = X.rHist[((size_t) n * D.T + t) * D.B + b];
+		const Real diff = r - (Real) P.target[((size_t) t * D.B + b) * D.R + n];
+		const Real lr = Real(2) * X.lossScale * diff + X.alpha * X.lamR[n * D.B + b];
+		X.lamR[n * D.B + b] = lr;
 		lamS = lr;
 	}
 	for(int e = D.outStart[n]; e < D.outStart[n + 1]; ++e) {
 		const int tt = t + D.outDelay[e];
-		if(tt < D.T) lamS = fmaf(P.W[e], D.lamI[((size_t) D.outTgt[e] * D.T + tt) * D.B + b], lamS);
+		if(tt < D.T) lamS = fma((Real) P.W[e], X.lamI[((size_t) D.outTgt[e] * D.T + tt) * D.B + b], lamS);
 	}
 
 	// replay the sub-steps of ms t
-	const float a = P.a[n], bb = P.b[n], c = P.c[n], d = P.d[n];
+	const Real a = P.a[n], bb = P.b[n], c = P.c[n], d = P.d[n];
 	const size_t s = (size_t) (t - t0) * D.N * D.B + i;
-	const float I = D.segSyn[s] + P.noise[((size_t) t * D.B + b) * D.N + n];
-	float vk[4], uk[4], v1k[4], sk[4];
+	const Real I = X.segSyn[s] + (Real) P.noise[((size_t) t * D.B + b) * D.N + n];
+	Real vk[4], uk[4], v1k[4], sk[4];
 	{
-		float v = D.segV[s], u = D.segU[s];
+		Real v = X.segV[s], u = X.segU[s];
 #pragma unroll
 		for(int k = 0; k < 4; ++k) {
 			vk[k] = v;
 			uk[k] = u;
-			const float v1 = v + 0.25f * (0.04f * v * v + 5.0f * v + 140.0f - u + I);
-			const float u1 = u + 0.25f * a * (bb * v1 - u);
-			const float sp = spike_fn(v1 - 30.0f, D.smooth);
-			v1k[k] = v1;
-			sk[k] = sp;
-			v = v1 + sp * (c - v1);
-			u = u1 + sp * d;
+			sk[k] = substep(v, u, v1k[k], I, a, bb, c, d, D.smooth);
 		}
 	}
 
 	// reverse through the sub-steps
-	float lamV = D.lamV[i], lamU = D.lamU[i];
-	float lamI = 0.0f, ga = D.gA[i], gb = D.gB[i];
+	Real lamV = X.lamV[i], lamU = X.lamU[i];
+	Real lamI = Real(0), ga = X.gA[i], gb = X.gB[i];
 #pragma unroll
 	for(int k = 3; k >= 0; --k) {
-		const float v = vk[k], u = uk[k], v1 = v1k[k], sp = sk[k];
+		const Real v = vk[k], u = uk[k], v1 = v1k[k], sp = sk[k];
 		// v' = v1 + s (c - v1), u' = u1 + s d
-		const float lams = lamS + lamV * (c - v1) + lamU * d;
-		float lamV1 = lamV * (1.0f - sp) + lams * spike_grad(v1 - 30.0f);
-		const float lamU1 = lamU;
+		const Real lams = lamS + lamV * (c - v1) + lamU * d;
+		Real lamV1 = lamV * (Real(1) - sp) + lams * spike_grad(v1 - Real(30));
+		const Real lamU1 = lamU;
 		// u1 = u + a/4 (b v1 - u)
-		lamV1 += lamU1 * 0.25f * a * bb;
-		float lamUin = lamU1 * (1.0f - 0.25f * a);
-		ga += lamU1 * 0.25f * (bb * v1 - u);
-		gb += lamU1 * 0.25f * a * v1;
+		lamV1 += lamU1 * Real(0.25) * a * bb;
+		const Real lamUin = lamU1 * (Real(1) - Real(0.25) * a);
+		ga += lamU1 * Real(0.25) * (bb * v1 - u);
+		gb += lamU1 * Real(0.25) * a * v1;
 		// v1 = v + 1/4 (0.04 v^2 + 5 v + 140 - u + I)
-		lamV = lamV1 * (1.0f + 0.25f * (0.08f * v + 5.0f));
-		lamU = lamUin - 0.25f * lamV1;
-		lamI += 0.25f * lamV1;
+		lamV = lamV1 * (Real(1) + Real(0.25) * (Real(0.08) * v + Real(5)));
+		lamU = lamUin - Real(0.25) * lamV1;
+		lamI += Real(0.25) * lamV1;
 	}
-	D.lamV[i] = lamV;
-	D.lamU[i] = lamU;
-	D.gA[i] = ga;
-	D.gB[i] = gb;
-	D.lamI[((size_t) n * D.T + t) * D.B + b] = lamI;
+	X.lamV[i] = lamV;
+	X.lamU[i] = lamU;
+	X.gA[i] = ga;
+	X.gB[i] = gb;
+	X.lamI[((size_t) n * D.T + t) * D.B + b] = lamI;
 }
 
 // readout traces of the last forward pass as [T][B][R]
-__global__ void bptt_readout_kernel(BpttDev D, float* out)
+template<typename Real>
+__global__ void bptt_readout_kernel(BpttDev D, BpttState<Real> X, float* out)
 {
 	const size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x;
 	const size_t total = (size_t) D.T * D.B * D.R;
 	if(i >= total) return;
 	const int n = (int) (i % D.R), b = (int) ((i / D.R) % D.B), t = (int) (i / ((size_t) D.R * D.B));
-	out[i] = D.rHist[((size_t) n * D.T + t) * D.B + b];
+	out[i] = (float) X.rHist[((size_t) n * D.T + t) * D.B + b];
 }
 
 // parameter gradients: sum over trials, plus u(0) = b v(0) with v(0) = -65
-__global__ void bptt_param_grad_kernel(BpttDev D, float* da, float* db)
+template<typename Real>
+__global__ void bptt_param_grad_kernel(BpttDev D, BpttState<Real> X, float* da, float* db)
 {
 	const int n = blockIdx.x * blockDim.x + threadIdx.x;
 	if(n >= D.N) return;
-	float sa = 0.0f, sb = 0.0f;
+	Real sa = Real(0), sb = Real(0);
 	for(int b = 0; b < D.B; ++b) {
-		sa += D.gA[n * D.B + b];
-		sb += D.gB[n * D.B + b] + D.lamU[n * D.B + b] * -65.0f;
+		sa += X.gA[n * D.B + b];
+		sb += X.gB[n * D.B + b] + X.lamU[n * D.B + b] * Real(-65);
 	}
-	da[n] = sa;
-	db[n] = sb;
+	da[n] = (float) sa;
+	db[n] = (float) sb;
 }
 
 // dL/dW[e] = sum_t,b S_src(t - d) lambda_I,tgt(t): one CTA per source, its
 // spike train in shared memory, one warp per outgoing synapse
-__global__ void bptt_weight_grad_kernel(BpttDev D, float* dW)
+template<typename Real>
+__global__ void bptt_weight_grad_kernel(BpttDev D, BpttState<Real> X, float* dW)
 {
-	extern __shared__ float sS[];
+	extern __shared__ __align__(16) unsigned char sRaw[];
+	Real* sS = reinterpret_cast<Real*>(sRaw);
 	const int j = blockIdx.x;
 	const int TB = D.T * D.B;
-	for(int k = threadIdx.x; k < TB; k += blockDim.x) sS[k] = D.S[(size_t) j * TB + k];
+	for(int k = threadIdx.x; k < TB; k += blockDim.x) sS[k] = X.S[(size_t) j * TB + k];
 	__syncthreads();
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 	for(int e = D.outStart[j] + warp; e < D.outStart[j + 1]; e += nw) {
 		const int dl = D.outDelay[e];
-		const float* lam = D.lamI + (size_t) D.outTgt[e] * TB + (size_t) dl * D.B;
+		const Real* lam = X.lamI + (size_t) D.outTgt[e] * TB + (size_t) dl * D.B;
 		const int len = (D.T - dl) * D.B;
-		float acc = 0.0f;
-		for(int k = lane; k < len; k += 32) acc = fmaf(sS[k], lam[k], acc);
+		Real acc = Real(0);
+		for(int k = lane; k < len; k += 32) acc = fma(sS[k], lam[k], acc);
 #pragma unroll
 		for(int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-		if(lane == 0) dW[e] = acc;
+		if(lane == 0) dW[e] = (float) acc;
 	}
 }
 
 Bptt::Bptt(unsigned N, unsigned B, unsigned T, unsigned R, unsigned ckpt, size_t M, const unsigned* src,
-		const unsigned* tgt, const unsigned* delay, int smooth, int device)
+		const unsigned* tgt, const unsigned* delay, bool smooth, bool fp64, int device)
 {
 	if(N == 0 || B == 0 || T == 0 || ckpt == 0) NB_THROW(NEMO_INVALID_INPUT, "empty differentiable network");
 	if(R > N) NB_THROW(NEMO_INVALID_INPUT, "more readout neurons than neurons");
+	const size_t realSize = fp64 ? 8 : 4;
+	if((size_t) T * B * realSize > 227 * 1024) {
+		NB_THROW(NEMO_API_UNSUPPORTED, "ms x trials too large for the weight-gradient kernel (%zu bytes of shared memory)",
+				(size_t) T * B * realSize);
+	}
+	if((size_t) N * B > (size_t) INT32_MAX) NB_THROW(NEMO_API_UNSUPPORTED, "neurons x trials too large");
 	m_device = device;
 	if(device >= 0) BP_CUDA(cudaSetDevice(device));
 	else BP_CUDA(cudaGetDevice(&m_device));
-	D.N = (int) N; D.B = (int) B; D.T = (int) T; D.R = (int) R; D.ckpt = (int) ckpt; D.smooth = smooth;
-	D.alpha = expf(-1.0f / 20.0f);
-	D.lossScale = 1.0f / ((float) T * (float) R * (float) B);
+	D.N = (int) N; D.B = (int) B; D.T = (int) T; D.R = (int) R; D.ckpt = (int) ckpt; D.smooth = smooth ? 1 : 0;
+	m_fp64 = fp64;
 	m_M = M;
 	// synapses are given source-major: synapse e's weight is W[e]
 	std::vector<int> outStart(N + 1, 0), inStart(N + 1, 0);
@@ -326,86 +345,125 @@ Bptt::Bptt(unsigned N, unsigned B, unsigned T, unsigned R, unsigned ckpt, size_t
 	D.outStart = upload(outStart);
 	D.outTgt = upload(outTgt);
 	D.outDelay = upload(outDelay);
-	const size_t NB = (size_t) N * B;
-	const size_t nck = (T + ckpt - 1) / ckpt;
-	D.S = alloc(NB * T);
-	D.v = alloc(NB);
-	D.u = alloc(NB);
-	D.ckV = alloc(NB * nck);
-	D.ckU = alloc(NB * nck);
-	D.r = alloc((size_t) std::max(1u, R) * B);
-	D.rHist = alloc((size_t) std::max(1u, R) * T * B);
-	D.lossPart = alloc(NB);
-	D.segV = alloc(NB * ckpt);
-	D.segU = alloc(NB * ckpt);
-	D.segSyn = alloc(NB * ckpt);
-	D.lamV = alloc(NB);
-	D.lamU = alloc(NB);
-	D.lamR = alloc((size_t) std::max(1u, R) * B);
-	D.lamI = alloc(NB * T);
-	D.gA = alloc(NB);
-	D.gB = alloc(NB);
-	BP_CUDA(cudaFuncSetAttribute(bptt_weight_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			(int) std::min<size_t>(227 * 1024, (size_t) T * B * 4)));
-	if((size_t) T * B * 4 > 227 * 1024) NB_THROW(NEMO_API_UNSUPPORTED, "T x trials too large for the weight-gradient kernel");
+	if(fp64) {
+		allocState(X64);
+		BP_CUDA(cudaFuncSetAttribute(bptt_weight_grad_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				(int) ((size_t) T * B * 8)));
+	} else {
+		allocState(X32);
+		BP_CUDA(cudaFuncSetAttribute(bptt_weight_grad_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+				(int) ((size_t) T * B * 4)));
+	}
 }
 
+template<typename Real>
+void Bptt::allocState(BpttState<Real>& X)
+{
+	const size_t NB = (size_t) D.N * D.B, R = (size_t) std::max(1, D.R), B = D.B, T = D.T;
+	const size_t nck = (T + D.ckpt - 1) / D.ckpt, seg = (size_t) std::min(D.ckpt, D.T);
+	auto a = [&](size_t n) { return static_cast<Real*>(alloc(n * sizeof(Real))); };
+	X.alpha = (Real) std::exp(-1.0 / 20.0);
+	X.lossScale = Real(1) / ((Real) T * (Real) D.R * (Real) B);
+	X.S = a(NB * T);
+	X.v = a(NB);
+	X.u = a(NB);
+	X.ckV = a(NB * nck);
+	X.ckU = a(NB * nck);
+	X.r = a(R * B);
+	X.rHist = a(R * T * B);
+	X.lossPart = a(NB);
+	X.segV = a(NB * seg);
+	X.segU = a(NB * seg);
+	X.segSyn = a(NB * seg);
+	X.lamV = a(NB);
+	X.lamU = a(NB);
+	X.lamR = a(R * B);
+	X.lamI = a(NB * T);
+	X.gA = a(NB);
+	X.gB = a(NB);
+}
 
 Bptt::~Bptt()
 {
 	for(void* p : m_allocs) cudaFree(p);
 }
 
-void Bptt::forward(const BpttParams& P, float* loss, void* stream)
+template<typename Real>
+void Bptt::forwardT(BpttState<Real>& X, const BpttParams& P, float* loss, void* stream)
 {
 	cudaStream_t st = static_cast<cudaStream_t>(stream);
-BP_CUDA(cudaSetDevice(m_device));
 	const int threads = 256, blocks = (D.N * D.B + threads - 1) / threads;
-	bptt_init_kernel<<<blocks, threads, 0, st>>>(D, P);
-	for(int t = 0; t < D.T; ++t) bptt_forward_kernel<<<blocks, threads, 0, st>>>(D, P, t);
-	bptt_loss_kernel<<<1, 1024, 0, st>>>(D, loss);
+	bptt_init_kernel<Real><<<blocks, threads, 0, st>>>(D, X, P);
+	for(int t = 0; t < D.T; ++t) bptt_forward_kernel<Real><<<blocks, threads, 0, st>>>(D, X, P, t);
+	bptt_loss_kernel<Real><<<1, 1024, 0, st>>>(D, X, loss);
 	BP_CUDA(cudaGetLastError());
+}
+
+template<typename Real>
+void Bptt::backwardT(BpttState<Real>& X, const BpttParams& P, float* dW, float* da, float* db, void* stream)
+{
+	cudaStream_t st = static_cast<cudaStream_t>(stream);
+	const int threads = 256, blocks = (D.N * D.B + threads - 1) / threads;
+	const size_t NB = (size_t) D.N * D.B * sizeof(Real);
+	// lamV, lamU, lamR, gA, gB start at zero
+	BP_CUDA(cudaMemsetAsync(X.lamV, 0, NB, st));
+	BP_CUDA(cudaMemsetAsync(X.lamU, 0, NB, st));
+	BP_CUDA(cudaMemsetAsync(X.lamR, 0, (size_t) std::max(1, D.R) * D.B * sizeof(Real), st));
+	BP_CUDA(cudaMemsetAsync(X.gA, 0, NB, st));
+	BP_CUDA(cudaMemsetAsync(X.gB, 0, NB, st));
+	const int nseg = (D.T + D.ckpt - 1) / D.ckpt;
+	for(int seg = nseg - 1; seg >= 0; --seg) {
+		const int t0 = seg * D.ckpt, t1 = std::min(D.T, t0 + D.ckpt);
+		for(int t = t0; t < t1; ++t) bptt_replay_kernel<Real><<<blocks, threads, 0, st>>>(D, X, P, t, t0);
+		for(int t = t1 - 1; t >= t0; --t) bptt_backward_kernel<Real><<<blocks, threads, 0, st>>>(D, X, P, t, t0);
+	}
+	bptt_param_grad_kernel<Real><<<(D.N + 255) / 256, 256, 0, st>>>(D, X, da, db);
+	bptt_weight_grad_kernel<Real><<<D.N, 256, (size_t) D.T * D.B * sizeof(Real), st>>>(D, X, dW);
+	BP_CUDA(cudaGetLastError());
+}
+
+template<typename Real>
+void Bptt::readoutT(BpttState<Real>& X, float* out, void* stream)
+{
+	const size_t total = (size_t) D.T * D.B * D.R;
+	if(total) {
+		bptt_readout_kernel<Real><<<(unsigned) ((total + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(D,
+				X, out);
+	}
+	BP_CUDA(cudaGetLastError());
+}
+
+void Bptt::forward(const BpttParams& P, float* loss, void* stream)
+{
+	BP_CUDA(cudaSetDevice(m_device));
+	if(m_fp64) forwardT(X64, P, loss, stream);
+	else forwardT(X32, P, loss, stream);
 }
 
 void Bptt::backward(const BpttParams& P, float* dW, float* da, float* db, void* stream)
 {
-	cudaStream_t st = static_cast<cudaStream_t>(stream);
-BP_CUDA(cudaSetDevice(m_device));
-	const int threads = 256, blocks = (D.N * D.B + threads - 1) / threads;
-	// lamV, lamU, lamR, gA, gB start at zero
-	BP_CUDA(cudaMemsetAsync(D.lamV, 0, (size_t) D.N * D.B * 4, st));
-	BP_CUDA(cudaMemsetAsync(D.lamU, 0, (size_t) D.N * D.B * 4, st));
-	BP_CUDA(cudaMemsetAsync(D.lamR, 0, (size_t) std::max(1, D.R) * D.B * 4, st));
-	BP_CUDA(cudaMemsetAsync(D.gA, 0, (size_t) D.N * D.B * 4, st));
-	BP_CUDA(cudaMemsetAsync(D.gB, 0, (size_t) D.N * D.B * 4, st));
-	const int nseg = (D.T + D.ckpt - 1) / D.ckpt;
-	for(int seg = nseg - 1; seg >= 0; --seg) {
-		const int t0 = seg * D.ckpt, t1 = std::min(D.T, t0 + D.ckpt);
-		for(int t = t0; t < t1; ++t) bptt_replay_kernel<<<blocks, threads, 0, st>>>(D, P, t, t0);
-		for(int t = t1 - 1; t >= t0; --t) bptt_backward_kernel<<<blocks, threads, 0, st>>>(D, P, t, t0);
-	}
-	bptt_param_grad_kernel<<<(D.N + 255) / 256, 256, 0, st>>>(D, da, db);
-	bptt_weight_grad_kernel<<<D.N, 256, (size_t) D.T * D.B * 4, st>>>(D, dW);
-	BP_CUDA(cudaGetLastError());
+	BP_CUDA(cudaSetDevice(m_device));
+	if(m_fp64) backwardT(X64, P, dW, da, db, stream);
+	else backwardT(X32, P, dW, da, db, stream);
 }
 
 void Bptt::readout(float* out, void* stream)
 {
 	BP_CUDA(cudaSetDevice(m_device));
-	const size_t total = (size_t) D.T * D.B * D.R;
-	if(total) bptt_readout_kernel<<<(unsigned) ((total + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(D, out);
-	BP_CUDA(cudaGetLastError());
+	if(m_fp64) readoutT(X64, out, stream);
+	else readoutT(X32, out, stream);
 }
 
-float* Bptt::alloc(size_t n)
+void* Bptt::alloc(size_t bytes)
 {
 	void* p = nullptr;
-	if(cudaMalloc(&p, std::max<size_t>(n, 1) * 4) != cudaSuccess) {
-		NB_THROW(NEMO_CUDA_MEMORY_ERROR, "failed to allocate %zu bytes of device memory", n * 4);
+	bytes = std::max<size_t>(bytes, 4);
+	if(cudaMalloc(&p, bytes) != cudaSuccess) {
+		NB_THROW(NEMO_CUDA_MEMORY_ERROR, "failed to allocate %zu bytes of device memory", bytes);
 	}
 	m_allocs.push_back(p);
-	BP_CUDA(cudaMemset(p, 0, std::max<size_t>(n, 1) * 4));
-	return static_cast<float*>(p);
+	BP_CUDA(cudaMemset(p, 0, bytes));
+	return p;
 }
 
 const int* Bptt::upload(const std::vector<int>& v)
@@ -420,4 +478,3 @@ const int* Bptt::upload(const std::vector<int>& v)
 }
 
 } // namespace nemo_b200
-

@@ -1,29 +1,7 @@
-// kernels.cuh -- sm_100a kernels of the simulation step.
-//
-// One launch of step_kernel advances the whole network by one millisecond.
-// It fuses what the reference does in four passes
-// (src/nemo/cpu/Simulation.cpp:94-111 on the CPU; gather, update, scatter and
-// updateStdp kernels on the reference CUDA backend):
-//
-//   1. current read-out: each neuron reads its (E, I) 64-bit fixed-point sums
-//      for this step from the accumulator slot ring and clears them;
-//   2. neuron update: the type's plugin arithmetic, in the reference's
-//      operation order with IEEE-rounded intrinsics (no contraction);
-//   3. firing bookkeeping: the history word, the fired bit-vector, and a
-//      ballot/popc compaction of the CTA's fired neurons into shared memory;
-//   4. spike scatter: the CTA's warps stream the fired neurons' outgoing
-//      synapses (pre-sorted by delay, 8 bytes each) and add every weight into
-//      the accumulator slot of the step at which it arrives, with 64-bit
-//      integer atomics (order-independent, hence bit-exact);
-//   5. STDP accumulation for the previous step (the reference does it at the
-//      end of the same step; it only needs the previous step's history, which
-//      the double-buffered history keeps intact).
-//
-// Scattering at firing time instead of gathering at arrival time makes one
-// kernel boundary per step sufficient.  It delivers the weight a synapse has
-// when the spike is emitted; applyStdp compensates in-flight spikes of every
-// synapse whose weight it changes, so the arrival-time weight is what is
-// delivered, as in the reference.
+// kernels.cuh -- device functions of the simulation step (sm_100a): the
+// fixed-point and STDP arithmetic of the reference and the neuron-type
+// plugins.  The step's phases (delivery at arrival, neuron update, STDP
+// accumulation) are the kernels of simulation.cu.
 #pragma once
 
 #include "simulation.hpp"
@@ -79,53 +57,73 @@ __device__ __forceinline__ int32_t fx_mul_dev(int32_t a, int32_t b)
 	return (int32_t) (((long long) a * (long long) b) >> FRACTIONAL_BITS);
 }
 
-// Fixed-point input sums.  The reference sums E (w >= 0) and I (w < 0)
-// contributions in int64 and clamps once (src/nemo/cpu/Simulation.cpp:297-300,
-// src/nemo/fixedpoint.cpp:40-49).  Here each (step slot, neuron) keeps the
-// low 32 bits of E and of -I in an 8-byte word pair, so the accumulator ring
-// fits in L2; a carry out of (or borrow into) a low word, detected from the
-// value the atomic returns, is added to a signed high-word counter of the
-// same (slot, neuron), and the slot is flagged.  The exact int64 sum is
-// high * 2^32 + low, independent of the order of the atomics.
-__device__ __forceinline__ void acc_add(const DevSim& S, uint32_t sl, uint32_t n, uint32_t cls, int64_t delta)
+// The neuron-type plugins, each split into a load of the neuron's
+// parameters, state and RNG words into registers, the update arithmetic on
+// those registers, and the store of what changed.  The step issues every
+// load of a neuron before its first store, so that none of them waits for
+// another.
+struct NeuronRegs {
+	float p[9];     // parameters
+	float x[4];     // state
+	uint32_t r[4];  // xorshift words
+};
+
+__device__ __forceinline__ void load_rng(const DevSim& S, uint32_t n, NeuronRegs& R)
 {
-	const size_t i = (size_t) sl * S.N + n;
-	uint32_t* lo = reinterpret_cast<uint32_t*>(S.slots + i) + cls;
-	const uint32_t d = (uint32_t) delta;
-	const uint32_t old = atomicAdd(lo, d);
-	const uint32_t now = old + d;
-	const bool wrap = delta >= 0 ? now < old : now > old;
-	if(wrap) {
-		atomicAdd(reinterpret_cast<int*>(S.slotHigh + i) + cls, delta >= 0 ? 1 : -1);
-		S.slotFlag[sl] = 1u;
-	}
+	R.r[0] = S.rng[n];
+	R.r[1] = S.rng[S.N + n];
+	R.r[2] = S.rng[2 * S.N + n];
+	R.r[3] = S.rng[3 * S.N + n];
 }
 
-// one synaptic weight arriving in slot sl at neuron n
-__device__ __forceinline__ void add_current(const DevSim& S, uint32_t sl, uint32_t n, int32_t w)
+__device__ __forceinline__ void store_rng(const DevSim& S, uint32_t n, const NeuronRegs& R)
 {
-	if(w >= 0) acc_add(S, sl, n, 0, (int64_t) w);
-	else acc_add(S, sl, n, 1, -(int64_t) w);
+	S.rng[n] = R.r[0];
+	S.rng[S.N + n] = R.r[1];
+	S.rng[2 * S.N + n] = R.r[2];
+	S.rng[3 * S.N + n] = R.r[3];
+}
+
+// parameters and state of neuron nl of type T (the plugin layouts of
+// src/nemo/plugins/Izhikevich.h, IF_curr_exp.h, PoissonSource.h)
+__device__ __forceinline__ void load_neuron(const DevSim& S, const TypeRange& T, uint32_t nl, uint32_t n, NeuronRegs& R)
+{
+	const float* P = T.param;
+	const float* X = T.state;
+	const uint32_t nn = T.n;
+	switch(T.kind) {
+		case KIND_IZHIKEVICH:
+#pragma unroll
+			for(int k = 0; k < 5; ++k) R.p[k] = P[k * nn + nl];  // a, b, c, d, sigma
+			R.x[0] = X[nl];       // u
+			R.x[1] = X[nn + nl];  // v
+			load_rng(S, n, R);
+			break;
+		case KIND_IF_CURR_EXP:
+#pragma unroll
+			for(int k = 0; k < 9; ++k) R.p[k] = P[k * nn + nl];
+#pragma unroll
+			for(int k = 0; k < 4; ++k) R.x[k] = X[k * nn + nl];  // v, Ie, Ii, lastfired
+			break;
+		case KIND_POISSON:
+			R.p[0] = P[nl];  // rate
+			load_rng(S, n, R);
+			break;
+		default:
+			break;
+	}
 }
 
 // Izhikevich, src/nemo/cpu/plugins/Izhikevich.cpp:53-94: the v update is
 // evaluated in double (0.04, 5.0 and 140.0 are double literals there), u in
 // float; both round exactly as the x86-64 SSE build does.
-__device__ __forceinline__ bool update_izhikevich(const DevSim& S, const TypeRange& T, uint32_t nl, uint32_t n,
-		float cE, float cI, float ext, bool fs)
+__device__ __forceinline__ bool update_izhikevich(const LibmCalib& calib, NeuronRegs& R, float cE, float cI, float ext,
+		bool fs)
 {
-	const float* P = T.param;
-	float* X = T.state;
-	const uint32_t nn = T.n;
+	const float a = R.p[0], b = R.p[1], sigma = R.p[4];
 	float I = __fadd_rn(__fadd_rn(cE, cI), ext);
-	float sigma = P[4 * nn + nl];
-	if(sigma != 0.0f) {
-		uint32_t s0 = S.rng[n], s1 = S.rng[S.N + n], s2 = S.rng[2 * S.N + n], s3 = S.rng[3 * S.N + n];
-		I = __fadd_rn(I, __fmul_rn(sigma, nb_nrand(S.calib, s0, s1, s2, s3)));
-		S.rng[n] = s0; S.rng[S.N + n] = s1; S.rng[2 * S.N + n] = s2; S.rng[3 * S.N + n] = s3;
-	}
-	float a = P[nl], b = P[nn + nl];
-	float u = X[nl], v = X[nn + nl];
+	if(sigma != 0.0f) I = __fadd_rn(I, __fmul_rn(sigma, nb_nrand(calib, R.r[0], R.r[1], R.r[2], R.r[3])));
+	float u = R.x[0], v = R.x[1];
 	const double dI = (double) I;
 	bool fired = false;
 #pragma unroll
@@ -143,77 +141,84 @@ __device__ __forceinline__ bool update_izhikevich(const DevSim& S, const TypeRan
 	}
 	fired = fired || fs;
 	if(fired) {
-		v = P[2 * nn + nl];
-		u = __fadd_rn(u, P[3 * nn + nl]);
+		v = R.p[2];
+		u = __fadd_rn(u, R.p[3]);
 	}
-	X[nl] = u;
-	X[nn + nl] = v;
+	R.x[0] = u;
+	R.x[1] = v;
 	return fired;
 }
 
 // IF_curr_exp, src/nemo/cpu/plugins/IF_curr_exp.cpp:74-121 with the header
 // parameter order (src/nemo/plugins/IF_curr_exp.h:4-20).
-__device__ __forceinline__ bool update_if_curr_exp(const TypeRange& T, uint32_t nl,
-		float cE, float cI, float ext, bool fs)
+__device__ __forceinline__ bool update_if_curr_exp(NeuronRegs& R, float cE, float cI, float ext, bool fs)
 {
-	const float* P = T.param;
-	float* X = T.state;
-	const uint32_t nn = T.n;
-	float v_rest = P[nl], v_reset = P[nn + nl], c_m = P[2 * nn + nl], tau_m = P[3 * nn + nl];
-	float tau_refrac = P[4 * nn + nl], tau_E = P[5 * nn + nl], tau_I = P[6 * nn + nl];
-	float v_thresh = P[7 * nn + nl], i_offset = P[8 * nn + nl];
-	float Ie = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, __fdiv_rn(1.0f, tau_E)), X[nn + nl]), cE);
-	float Ii = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, __fdiv_rn(1.0f, tau_I)), X[2 * nn + nl]), cI);
-	float I = __fadd_rn(__fadd_rn(__fadd_rn(Ie, Ii), ext), i_offset);
-	X[nn + nl] = Ie;
-	X[2 * nn + nl] = Ii;
-	float v = X[nl];
-	float lastfired = X[3 * nn + nl];
-	bool refractory = lastfired <= tau_refrac;
+	const float v_rest = R.p[0], v_reset = R.p[1], c_m = R.p[2], tau_m = R.p[3];
+	const float tau_refrac = R.p[4], tau_E = R.p[5], tau_I = R.p[6];
+	const float v_thresh = R.p[7], i_offset = R.p[8];
+	const float Ie = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, __fdiv_rn(1.0f, tau_E)), R.x[1]), cE);
+	const float Ii = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, __fdiv_rn(1.0f, tau_I)), R.x[2]), cI);
+	const float I = __fadd_rn(__fadd_rn(__fadd_rn(Ie, Ii), ext), i_offset);
+	R.x[1] = Ie;
+	R.x[2] = Ii;
+	float v = R.x[0];
+	const float lastfired = R.x[3];
+	const bool refractory = lastfired <= tau_refrac;
 	if(!refractory) {
 		v = __fadd_rn(v, __fadd_rn(__fdiv_rn(I, c_m), __fdiv_rn(__fsub_rn(v_rest, v), tau_m)));
 	}
-	bool fired = (!refractory && v > v_thresh) || fs;
+	const bool fired = (!refractory && v > v_thresh) || fs;
 	if(fired) {
-		X[3 * nn + nl] = 1.0f;
-		X[nl] = v_reset;
+		R.x[3] = 1.0f;
+		R.x[0] = v_reset;
 	} else {
-		X[3 * nn + nl] = __fadd_rn(lastfired, 1.0f);
-		X[nl] = v;
+		R.x[3] = __fadd_rn(lastfired, 1.0f);
+		R.x[0] = v;
 	}
 	return fired;
 }
 
 // PoissonSource, src/nemo/cpu/plugins/PoissonSource.cpp:6-30
-__device__ __forceinline__ bool update_poisson(const DevSim& S, const TypeRange& T, uint32_t nl, uint32_t n, bool fs)
+__device__ __forceinline__ bool update_poisson(NeuronRegs& R, bool fs)
 {
-	uint32_t p0 = x86_f2u32(__fmul_rn(T.param[nl], 65536.0f));
-	uint32_t s0 = S.rng[n], s1 = S.rng[S.N + n], s2 = S.rng[2 * S.N + n], s3 = S.rng[3 * S.N + n];
-	uint32_t p1 = nb_urand(s0, s1, s2, s3) & 0xffffu;
-	S.rng[n] = s0; S.rng[S.N + n] = s1; S.rng[2 * S.N + n] = s2; S.rng[3 * S.N + n] = s3;
+	const uint32_t p0 = x86_f2u32(__fmul_rn(R.p[0], 65536.0f));
+	const uint32_t p1 = nb_urand(R.r[0], R.r[1], R.r[2], R.r[3]) & 0xffffu;
 	return p1 < p0 || fs;
 }
 
-// A weight that applyStdp changes was already scattered, with its old value,
-// for the spikes its source emitted k < delay steps before the last step and
-// that have not arrived yet.  The reference reads the weight on arrival
-// (deliverSpikesOne, src/nemo/cpu/Simulation.cpp:293-307), so move each such
-// contribution from the old weight's class (E if >= 0, else I) to the new
-// weight's class with the new value.
-__device__ __forceinline__ void compensate_inflight(const DevSim& S, const uint64_t* hist, uint32_t sd,
-		uint32_t tgt, uint32_t slot, int32_t w, int32_t nw)
+// One step of neuron nl (local index n) of type T; returns whether it fired.
+__device__ __forceinline__ bool update_neuron(const DevSim& S, const TypeRange& T, NeuronRegs& R, float cE, float cI,
+		float ext, bool fs)
 {
-	const uint32_t src = sd & (MAX_NEURONS - 1);
-	const uint32_t delay = (sd >> 26) + 1;
-	uint64_t inflight = hist[src] & ((delay >= 64) ? ~0ull : ((1ull << delay) - 1ull));
-	while(inflight) {
-		const uint32_t k = __ffsll((long long) inflight) - 1;
-		inflight &= inflight - 1;
-		// emitted k steps before the last step, arrives delay - k steps after it
-		const uint32_t sl = (slot + delay - k) % S.D;
-		if(w >= 0) acc_add(S, sl, tgt, 0, -(int64_t) w);
-		else acc_add(S, sl, tgt, 1, (int64_t) w);
-		add_current(S, sl, tgt, nw);
+	switch(T.kind) {
+		case KIND_IZHIKEVICH: return update_izhikevich(S.calib, R, cE, cI, ext, fs);
+		case KIND_IF_CURR_EXP: return update_if_curr_exp(R, cE, cI, ext, fs);
+		case KIND_POISSON: return update_poisson(R, fs);
+		default: return fs;  // Input, src/nemo/cpu/plugins/Input.cpp:17-22
+	}
+}
+
+// the state and RNG words that update_neuron changed
+__device__ __forceinline__ void store_neuron(const DevSim& S, const TypeRange& T, uint32_t nl, uint32_t n,
+		const NeuronRegs& R)
+{
+	float* X = T.state;
+	const uint32_t nn = T.n;
+	switch(T.kind) {
+		case KIND_IZHIKEVICH:
+			X[nl] = R.x[0];
+			X[nn + nl] = R.x[1];
+			if(R.p[4] != 0.0f) store_rng(S, n, R);
+			break;
+		case KIND_IF_CURR_EXP:
+#pragma unroll
+			for(int k = 0; k < 4; ++k) X[k * nn + nl] = R.x[k];
+			break;
+		case KIND_POISSON:
+			store_rng(S, n, R);
+			break;
+		default:
+			break;
 	}
 }
 

@@ -604,14 +604,20 @@ nemo_status_t nemo_b200_set_graphs(nemo_simulation_t s, int on)
 	CALL(S(s).useGraphs = on != 0);
 }
 
-nemo_status_t nemo_b200_run_stats(nemo_simulation_t s, float* runMs, float kernelMs[3], unsigned launches[3],
+nemo_status_t nemo_b200_set_persistent(nemo_simulation_t s, int on)
+{
+	NULLCHECK(s);
+	CALL(S(s).usePersistent = on != 0);
+}
+
+nemo_status_t nemo_b200_run_stats(nemo_simulation_t s, float* runMs, float kernelMs[4], unsigned launches[4],
 		uint64_t* fired, uint64_t* events, uint64_t* stdpEntries, uint64_t* plastic)
 {
 	NULLCHECK(s);
 	CALL({
 		Simulation& sim = S(s);
 		if(runMs) *runMs = sim.lastRunMs;
-		for(int k = 0; k < 3; ++k) {
+		for(int k = 0; k < Simulation::K_KINDS; ++k) {
 			if(kernelMs) kernelMs[k] = sim.kernelMs[k];
 			if(launches) launches[k] = sim.kernelLaunches[k];
 		}
@@ -671,14 +677,17 @@ nemo_status_t nemo_b200_last_status(void) { return g_lastStatus; }
 
 nemo_b200_bptt_t nemo_b200_bptt_new(unsigned neurons, unsigned trials, unsigned ms, unsigned readout,
 		unsigned checkpoint_ms, size_t synapses, const unsigned source[], const unsigned target[],
-		const unsigned delay[], int smooth, int device)
+		const unsigned delay[], int options, int device)
 {
 	g_lastStatus = NEMO_OK;
 	try {
 		auto* h = new nemo_b200_bptt_class();
 		try {
+			if(options & ~(NEMO_B200_BPTT_SMOOTH | NEMO_B200_BPTT_FP64_STATE)) {
+				NB_THROW(NEMO_INVALID_INPUT, "unknown differentiable-mode option bits 0x%x", (unsigned) options);
+			}
 			h->impl.reset(new Bptt(neurons, trials, ms, readout, checkpoint_ms, synapses, source, target, delay,
-					smooth, device));
+					(options & NEMO_B200_BPTT_SMOOTH) != 0, (options & NEMO_B200_BPTT_FP64_STATE) != 0, device));
 		} catch(...) {
 			delete h;
 			throw;

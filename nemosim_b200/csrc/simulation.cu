@@ -24,23 +24,34 @@ namespace nemo_b200 {
 // ---------------------------------------------------------------------------
 // kernels
 
-// The step is two launches.  update_kernel advances every neuron and, for
-// each fired neuron and each STDP target, publishes the CSR span of work it
-// implies (its outgoing synapses; its incoming plastic synapses) as chunks of
-// at most CHUNK entries in a global list.  deliver_kernel then spreads those
-// chunks over all warps of the GPU.  The work of a step is therefore balanced
-// across the device however the spikes fall, and every lane keeps ILP
-// independent loads in flight.
+// A step has two phases, in the reference's order (src/nemo/cpu/
+// Simulation.cpp:94-111, deliverSpikes at :259-288):
+//
+//  - the pre-phase of step t delivers the spikes that arrive at t: every
+//    (source, delay d) group whose source fired at t - d, published by the
+//    update of step t - 1, adds its weights -- read now, at arrival, as the
+//    reference does -- into each target's accumulator; it also runs the
+//    STDP accumulation of step t - 1;
+//  - the update of step t advances every neuron and publishes, as chunks of
+//    at most CHUNK synapses in global lists, the delay groups that arrive
+//    at t + 1 and the incoming plastic synapses of this step's STDP targets.
+//
+// All warps of the GPU share the chunks of a phase, so its work is balanced
+// however the spikes fall.  The phases run as two kernels per step
+// (deliver_kernel, update_kernel) or inside the persistent step loop
+// (run_kernel), one cooperative launch for many steps.  STDP accumulation
+// of the last step runs before applyStdp (stdp_flush); deliveries stay
+// pending until the next step, so they read the weights applyStdp leaves.
 
 constexpr uint32_t CHUNK = 128;  // entries per chunk: 4 per lane of a warp
+constexpr uint32_t ILP = CHUNK / 32;
 
 // Inside a CUDA graph the step's cycle comes from a device counter (the
 // graph is replayed at different cycles): cycle = *cycleDev + offset.
-__device__ __forceinline__ void step_indices(const DevSim& S, uint32_t offset, uint32_t& cur, uint32_t& slot, uint32_t& ring)
+__device__ __forceinline__ void step_indices(const DevSim& S, uint32_t offset, uint32_t& cur, uint32_t& ring)
 {
 	const unsigned long long c = *S.cycleDev + offset;
 	cur = (uint32_t) (c & 1);
-	slot = S.D ? (uint32_t) (c % S.D) : 0u;
 	ring = (uint32_t) (c % S.R);
 }
 
@@ -48,7 +59,6 @@ __global__ void advance_cycle_kernel(unsigned long long* cycle, uint32_t by)
 {
 	*cycle += by;
 }
-constexpr uint32_t ILP = CHUNK / 32;
 
 __device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t x)
 {
@@ -89,73 +99,106 @@ __device__ __forceinline__ void write_chunks(uint4* list, uint32_t pos, unsigned
 	}
 }
 
-// Neuron update of one step (src/nemo/cpu/Simulation.cpp:94-111 minus the
-// delivery and STDP loops).  CTA c owns the partition of P consecutive
-// neurons starting at c * P (P a multiple of 32, so warps cover whole
-// bit-vector words); its blockDim.x threads loop over them.
-__global__ void __launch_bounds__(1024)
-update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t slot, uint32_t ring, uint32_t offset, int fromDev)
+constexpr uint32_t BUCKET = 32;  // entries per bucket of a work list
+
+// Reserve ng groups and ne entries per lane in a work list (one atomic per
+// warp); returns this lane's first group and first entry.
+__device__ __forceinline__ void reserve_groups(unsigned long long* counter, uint32_t ng, uint32_t ne, uint32_t& g,
+		uint32_t& e)
 {
-	if(fromDev) step_indices(S, offset, cur, slot, ring);
-	__shared__ uint32_t sFired;
-	__shared__ unsigned long long sEvents, sStdp;
+	const uint32_t ig = warp_inclusive_scan(ng), ie = warp_inclusive_scan(ne);
+	const uint32_t tg = __shfl_sync(0xffffffffu, ig, 31), te = __shfl_sync(0xffffffffu, ie, 31);
+	unsigned long long base = 0;
+	if((tg | te) && (threadIdx.x & 31) == 31) base = atomicAdd(counter, ((unsigned long long) tg << 32) | te);
+	base = __shfl_sync(0xffffffffu, base, 31);
+	g = (uint32_t) (base >> 32) + ig - ng;
+	e = (uint32_t) base + ie - ne;
+}
+
+// group g = entries [e, e + len) = [start, start + len) of the list's array
+__device__ __forceinline__ void write_group(const WorkList& L, uint32_t g, uint32_t e, unsigned long long start,
+		uint32_t len)
+{
+	L.group[g] = make_uint4((uint32_t) start, (uint32_t) (start >> 32), len, e);
+	for(uint32_t b = (e + BUCKET - 1) / BUCKET; b * BUCKET < e + len; ++b) L.bucket[b] = g;
+}
+
+// End of source n's delay-d group (its synapses of delay <= d) within its
+// row, which holds the synapses sorted by delay.
+__device__ __forceinline__ uint32_t delay_end(const DevSim& S, uint32_t n, uint32_t d)
+{
+	if(d == 0) return 0;
+	const size_t i = (size_t) n * S.dStride + (d - 1);
+	return S.dEnd16 ? (uint32_t) S.dEnd16[i] : S.dEnd32[i];
+}
+
+// CTA-level counters of one step, added to the per-step ring counters once
+// per CTA
+struct CtaCounters {
+	uint32_t fired;
+	unsigned long long events, stdp;
+};
+
+// Neuron update of step t (src/nemo/cpu/Simulation.cpp:94-111 minus the
+// delivery and STDP loops) for the neurons [first, last) of one CTA (first a
+// multiple of 32, so warps cover whole bit-vector words); the CTA's
+// blockDim.x threads loop over them.  Every thread of the CTA calls it.
+// cur = t & 1.
+__device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, uint32_t last, uint32_t cur,
+		uint32_t ring, CtaCounters& C)
+{
 	const uint32_t tid = threadIdx.x, lane = tid & 31;
-	const uint32_t first = blockIdx.x * P;
-	const uint32_t last = min(S.N, first + P);
 	const uint64_t* histPrev = S.hist + (size_t) (cur ^ 1u) * S.N;
 	uint64_t* histCur = S.hist + (size_t) cur * S.N;
-	const uint32_t slotFlag = S.D ? S.slotFlag[slot] : 0u;
-	if(tid == 0) { sFired = 0; sEvents = 0; sStdp = 0; }
-	__syncthreads();
 
 	for(uint32_t base = first; base < last; base += blockDim.x) {
 		const uint32_t n = base + tid;
 		bool fired = false, target = false;
 		uint32_t fw = 0, outdeg = 0, indeg = 0;
 		unsigned long long ob = 0, rb = 0;
+		uint64_t pend = 0;
 		if(n < last) {
 			uint32_t k = 0;
 			while(k + 1 < S.ntypes && n >= S.types[k + 1].base) ++k;
 			const TypeRange& T = S.types[k];
 			const uint32_t nl = n - T.base;
-			// this step's synaptic input (deliverSpikes + wfx_toFloat,
-			// src/nemo/cpu/Simulation.cpp:259-288)
-			float cE = 0.0f, cI = 0.0f;
-			if(S.D) {
-				uint2* a = S.slots + (size_t) slot * S.N + n;
-				const uint2 acc = *a;
-				if(acc.x | acc.y) *a = make_uint2(0, 0);
-				long long e = (long long) acc.x, i = (long long) acc.y;
-				if(slotFlag) {
-					int2* h = S.slotHigh + (size_t) slot * S.N + n;
-					const int2 hi = *h;
-					if(hi.x | hi.y) *h = make_int2(0, 0);
-					e += (long long) hi.x << 32;
-					i += (long long) hi.y << 32;
-				}
-				cE = wfx_to_float(e);
-				cI = wfx_to_float(-i);
-			}
-			float ext = S.curExt[n];
-			if(__float_as_uint(ext) != 0u) S.curExt[n] = 0.0f;
+			// every load of this neuron before its first store: this step's
+			// synaptic input, stimulus, history, CSR spans, delay groups,
+			// parameters, state and RNG words
+			const ulonglong2 acc = S.slot[n];
+			const float ext = S.curExt[n];
 			fw = S.fstim[n >> 5];
+			const uint64_t hp = histPrev[n];
+			const unsigned long long o0 = S.outPtr[n], o1 = S.outPtr[n + 1];
+			const uint64_t dm = S.delayMask[n];
+			unsigned long long r0 = 0, r1 = 0;
+			if(S.stdp) {
+				r0 = S.rcmPtr[n];
+				r1 = S.rcmPtr[n + 1];
+			}
+			NeuronRegs R;
+			load_neuron(S, T, nl, n, R);
+
+			if(acc.x | acc.y) S.slot[n] = make_ulonglong2(0, 0);
+			if(__float_as_uint(ext) != 0u) S.curExt[n] = 0.0f;
+			// wfx_toFloat of the int64 sums (src/nemo/fixedpoint.cpp:40-49)
+			const float cE = wfx_to_float((long long) acc.x);
+			const float cI = wfx_to_float((long long) acc.y);
 			const bool fs = (fw >> lane) & 1u;
-			switch(T.kind) {
-				case KIND_IZHIKEVICH: fired = update_izhikevich(S, T, nl, n, cE, cI, ext, fs); break;
-				case KIND_IF_CURR_EXP: fired = update_if_curr_exp(T, nl, cE, cI, ext, fs); break;
-				case KIND_POISSON: fired = update_poisson(S, T, nl, n, fs); break;
-				default: fired = fs; break; // Input, src/nemo/cpu/plugins/Input.cpp:17-22
-			}
-			const uint64_t h = (histPrev[n] << 1) | (uint64_t) fired;
+			fired = update_neuron(S, T, R, cE, cI, ext, fs);
+			store_neuron(S, T, nl, n, R);
+			const uint64_t h = (hp << 1) | (uint64_t) fired;
 			histCur[n] = h;
-			if(fired) {
-				ob = S.outPtr[n];
-				outdeg = (uint32_t) (S.outPtr[n + 1] - ob);
-			}
+			ob = o0;
+			if(fired) outdeg = (uint32_t) (o1 - o0);
+			// groups arriving next step: delay d of a source that fired d - 1
+			// steps ago (bit d - 1 of the history; dm holds only the delays
+			// the source has and deliverSpikes accepts)
+			pend = h & dm;
 			// STDP target: fired |post| steps ago (ConnectivityMatrix.cpp:206)
 			if(S.stdp && (h & S.sp.postFireMask)) {
-				rb = S.rcmPtr[n];
-				indeg = (uint32_t) (S.rcmPtr[n + 1] - rb);
+				rb = r0;
+				indeg = (uint32_t) (r1 - r0);
 				target = indeg > 0;
 			}
 		}
@@ -164,13 +207,28 @@ update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t slot, uint32_t 
 			S.firedRing[(size_t) ring * S.W + (n >> 5)] = fb;
 			if(fw) S.fstim[n >> 5] = 0u;
 		}
-		// delivery and STDP chunks of this step
-		const uint32_t nchF = (fired && S.D) ? (outdeg + CHUNK - 1) / CHUNK : 0;
-		const uint32_t nchS = target ? (indeg + CHUNK - 1) / CHUNK : 0;
-		if(__any_sync(0xffffffffu, nchF + nchS != 0)) {
-			const uint32_t pos = reserve_chunks(&S.chunkCount[cur], nchF + nchS);
-			write_chunks(S.chunks, pos, ob, outdeg, nchF, 0u);
-			write_chunks(S.chunks, pos + nchF, rb, indeg, nchS, 1u);
+		// the delay groups that arrive next step
+		if(__any_sync(0xffffffffu, pend != 0)) {
+			uint32_t ng = 0, ne = 0;
+			for(uint64_t b = pend; b; b &= b - 1) {
+				const uint32_t d = (uint32_t) __ffsll((long long) b);
+				ne += delay_end(S, n, d) - delay_end(S, n, d - 1);
+				++ng;
+			}
+			uint32_t g, e;
+			reserve_groups(&S.dlvWork.count[cur], ng, ne, g, e);
+			for(uint64_t b = pend; b; b &= b - 1) {
+				const uint32_t d = (uint32_t) __ffsll((long long) b);
+				const uint32_t e0 = delay_end(S, n, d - 1), len = delay_end(S, n, d) - e0;
+				write_group(S.dlvWork, g++, e, ob + e0, len);
+				e += len;
+			}
+		}
+		// the incoming plastic synapses of this step's STDP targets
+		if(__any_sync(0xffffffffu, target)) {
+			uint32_t g, e;
+			reserve_groups(&S.stdpWork.count[cur], target ? 1u : 0u, target ? indeg : 0u, g, e);
+			if(target) write_group(S.stdpWork, g, e, rb, indeg);
 		}
 		// targets touched in this STDP period, for applyStdp
 		const uint32_t tb = __ballot_sync(0xffffffffu, target);
@@ -178,87 +236,256 @@ update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t slot, uint32_t 
 		if(fb) {
 			const unsigned long long ev = warp_sum(fired ? outdeg : 0);
 			if(lane == 0) {
-				atomicAdd(&sFired, (uint32_t) __popc(fb));
-				atomicAdd(&sEvents, ev);
+				atomicAdd(&C.fired, (uint32_t) __popc(fb));
+				atomicAdd(&C.events, ev);
 			}
 		}
 		if(tb) {
 			const unsigned long long se = warp_sum(target ? indeg : 0);
-			if(lane == 0) atomicAdd(&sStdp, se);
+			if(lane == 0) atomicAdd(&C.stdp, se);
 		}
-	}
-	__syncthreads();
-	if(tid == 0) {
-		if(sFired) atomicAdd(&S.firedCount[ring], sFired);
-		if(sEvents) atomicAdd(&S.eventCount[ring], sEvents);
-		if(sStdp) atomicAdd(&S.stdpCount[ring], sStdp);
 	}
 }
 
-// Delivery and STDP accumulation of one step over the published chunks.
-// One warp per chunk; lane l handles entries l, l + 32, l + 64, l + 96.
-//  kind 0: add each outgoing synapse into the accumulator slot of its
-//          arrival step (64-bit integer atomics: order-independent sums)
-//  kind 1: STDP accumulation over the incoming plastic synapses of a target
-//          (ConnectivityMatrix::accumulateStdp, ConnectivityMatrix.cpp:193-227)
-__global__ void __launch_bounds__(STEP_THREADS)
-deliver_kernel(const DevSim S, uint32_t cur, uint32_t slot, uint32_t offset, int fromDev)
+// Adds the CTA's counters to those of ring position `ring` and clears them
+// (after a __syncthreads that follows the last update_range of the step).
+__device__ __forceinline__ void flush_counters(const DevSim& S, uint32_t ring, CtaCounters& C)
 {
-	if(fromDev) {
-		uint32_t ring;
-		step_indices(S, offset, cur, slot, ring);
+	if(threadIdx.x == 0) {
+		if(C.fired) atomicAdd(&S.firedCount[ring], C.fired);
+		if(C.events) atomicAdd(&S.eventCount[ring], C.events);
+		if(C.stdp) atomicAdd(&S.stdpCount[ring], C.stdp);
+		C.fired = 0;
+		C.events = 0;
+		C.stdp = 0;
 	}
-	const uint32_t nch = S.chunkCount[cur];
-	if(blockIdx.x == 0 && threadIdx.x == 0) {
-		S.chunkCount[cur ^ 1u] = 0; // next step's list starts empty
-		// this step's slot was read by update_kernel; no spike arrives in it now
-		if(S.D) S.slotFlag[slot] = 0u;
-	}
+}
+
+// One step's neuron update: CTA c owns the partition of P consecutive
+// neurons starting at c * P (P a multiple of 32).
+__global__ void __launch_bounds__(1024)
+update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t ring, uint32_t offset, int fromDev)
+{
+	if(fromDev) step_indices(S, offset, cur, ring);
+	__shared__ CtaCounters sC;
+	if(threadIdx.x == 0) sC = CtaCounters{ 0, 0, 0 };
+	__syncthreads();
+	const uint32_t first = blockIdx.x * P;
+	update_range(S, first, min(S.N, first + P), cur, ring, sC);
+	__syncthreads();
+	flush_counters(S, ring, sC);
+}
+
+// 64-bit integer reduction into an accumulator word (its result unused)
+__device__ __forceinline__ void red_add_u64(unsigned long long* p, unsigned long long v)
+{
+	asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
+
+// One warp's share of a work list: the entries [E0, E1) of the list's
+// ne entries, in rounds of 32 x K, each lane finding the group of its entry
+// by a binary search over 32 consecutive group descriptors (one per lane).
+//  KIND 0 (delivery): add each synapse's weight into its target's
+//          accumulator: the E (w >= 0) or I (w < 0) int64 sum, as
+//          deliverSpikesOne (src/nemo/cpu/Simulation.cpp:293-307); integer
+//          addition is associative, so the sums do not depend on the order
+//          of the reductions
+//  KIND 1 (STDP): accumulation over the incoming plastic synapses of a
+//          target (ConnectivityMatrix::accumulateStdp,
+//          ConnectivityMatrix.cpp:193-227) with the history `hist` of the
+//          step that published the list
+template<int KIND, int K>
+__device__ __forceinline__ void process_list(const DevSim& S, const WorkList& L, uint32_t ng, uint32_t ne,
+		const uint64_t* hist, uint32_t warp, uint32_t nwarps)
+{
+	if(ne == 0) return;
 	const uint32_t lane = threadIdx.x & 31;
-	const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-	const uint64_t* hist = S.hist + (size_t) cur * S.N;
-	for(uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nch; c += nw) {
-		const uint4 d = S.chunks[c];
-		const unsigned long long start = (unsigned long long) d.x | ((unsigned long long) d.y << 32);
-		const uint32_t len = d.z;
-		if(d.w == 0) {
-			uint2 s[ILP];
+	const uint32_t per = (ne + nwarps - 1) / nwarps;
+	const uint32_t E0 = warp * per;
+	if(E0 >= ne) return;
+	const uint32_t E1 = min(ne, E0 + per);
+	uint32_t g = L.bucket[E0 / BUCKET];
+	for(;;) {
+		// descriptors g .. g + 31; lanes past the last group hold an offset
+		// above every entry
+		const bool valid = g + lane < ng;
+		const uint4 d = valid ? L.group[g + lane] : make_uint4(0, 0, 0, 0xffffffffu);
+		const uint32_t lastLane = min(31u, ng - 1 - g);
+		const uint32_t coverEnd = __shfl_sync(0xffffffffu, d.w + d.z, lastLane);
+		const uint32_t lo = max(E0, __shfl_sync(0xffffffffu, d.w, 0)), hi = min(E1, coverEnd);
+		for(uint32_t base = lo; base < hi; base += 32 * K) {
+			unsigned long long idx[K];
 #pragma unroll
-			for(uint32_t j = 0; j < ILP; ++j) {
-				if(lane + 32 * j < len) s[j] = __ldcs(S.syn + start + lane + 32 * j);
-			}
+			for(int j = 0; j < K; ++j) {
+				const uint32_t e = base + lane + 32 * j;
+				uint32_t q = 0;
 #pragma unroll
-			for(uint32_t j = 0; j < ILP; ++j) {
-				if(lane + 32 * j < len) {
-					uint32_t sl = slot + (s[j].x >> 26) + 1;
-					sl = sl >= S.D ? sl - S.D : sl;
-					add_current(S, sl, s[j].x & (MAX_NEURONS - 1), (int32_t) s[j].y);
+				for(uint32_t step = 16; step > 0; step >>= 1) {
+					if(__shfl_sync(0xffffffffu, d.w, q + step) <= e) q += step;
 				}
+				const unsigned long long st = (unsigned long long) __shfl_sync(0xffffffffu, d.x, q)
+						| ((unsigned long long) __shfl_sync(0xffffffffu, d.y, q) << 32);
+				idx[j] = st + (e - __shfl_sync(0xffffffffu, d.w, q));
 			}
-		} else {
-			uint32_t sd[ILP];
-			int32_t acc[ILP];
-			uint64_t h[ILP];
+			if(KIND == 0) {
+				uint2 sy[K];
 #pragma unroll
-			for(uint32_t j = 0; j < ILP; ++j) {
-				if(lane + 32 * j < len) {
-					sd[j] = __ldcs(S.rcmSrc + start + lane + 32 * j);
-					acc[j] = __ldcs(S.rcmAcc + start + lane + 32 * j);
+				for(int j = 0; j < K; ++j) if(base + lane + 32 * j < hi) sy[j] = __ldcs(S.syn + idx[j]);
+#pragma unroll
+				for(int j = 0; j < K; ++j) {
+					if(base + lane + 32 * j < hi) {
+						const int32_t w = (int32_t) sy[j].y;
+						unsigned long long* a = reinterpret_cast<unsigned long long*>(S.slot + (sy[j].x & (MAX_NEURONS - 1)));
+						red_add_u64(a + (w >= 0 ? 0 : 1), (unsigned long long) (long long) w);
+					}
 				}
-			}
+			} else {
+				uint32_t sd[K];
+				int32_t acc[K];
+				uint64_t h[K];
 #pragma unroll
-			for(uint32_t j = 0; j < ILP; ++j) {
-				if(lane + 32 * j < len) h[j] = hist[sd[j] & (MAX_NEURONS - 1)];
-			}
+				for(int j = 0; j < K; ++j) {
+					if(base + lane + 32 * j < hi) {
+						sd[j] = __ldcs(S.rcmSrc + idx[j]);
+						acc[j] = __ldcs(S.rcmAcc + idx[j]);
+					}
+				}
 #pragma unroll
-			for(uint32_t j = 0; j < ILP; ++j) {
-				if(lane + 32 * j < len) {
-					const uint32_t delay = (sd[j] >> 26) + 1;
-					const int32_t dw = stdp_weight_change(S.sp, h[j] >> (delay & 63));
-					if(dw != 0) __stcs(S.rcmAcc + start + lane + 32 * j, (int32_t) ((uint32_t) acc[j] + (uint32_t) dw));
+				for(int j = 0; j < K; ++j) if(base + lane + 32 * j < hi) h[j] = hist[sd[j] & (MAX_NEURONS - 1)];
+#pragma unroll
+				for(int j = 0; j < K; ++j) {
+					if(base + lane + 32 * j < hi) {
+						const uint32_t delay = (sd[j] >> 26) + 1;
+						const int32_t dw = stdp_weight_change(S.sp, h[j] >> (delay & 63));
+						if(dw != 0) __stcs(S.rcmAcc + idx[j], (int32_t) ((uint32_t) acc[j] + (uint32_t) dw));
+					}
 				}
 			}
 		}
+		if(hi >= E1) break;
+		g += 32;
+	}
+}
+
+// what a pre-phase does
+constexpr uint32_t PHASE_DELIVER = 1;  // the published delay groups
+constexpr uint32_t PHASE_STDP = 2;     // the published STDP groups
+constexpr uint32_t PHASE_RESET = 4;    // empty the lists the next update publishes into
+
+// Pre-phase of a step over the lists published by the update of the step
+// with parity `pub`, each list's entries spread evenly over the `nwarps`
+// warps.
+__device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uint32_t what, uint32_t warp,
+		uint32_t nwarps)
+{
+	const unsigned long long cd = (what & PHASE_DELIVER) ? S.dlvWork.count[pub] : 0ull;
+	const unsigned long long cs = (what & PHASE_STDP) ? S.stdpWork.count[pub] : 0ull;
+	if((what & PHASE_RESET) && warp == 0 && (threadIdx.x & 31) == 0) {
+		S.dlvWork.count[pub ^ 1u] = 0;
+		S.stdpWork.count[pub ^ 1u] = 0;
+	}
+	const uint64_t* hist = S.hist + (size_t) pub * S.N;
+	process_list<0, 8>(S, S.dlvWork, (uint32_t) (cd >> 32), (uint32_t) cd, hist, warp, nwarps);
+	process_list<1, 4>(S, S.stdpWork, (uint32_t) (cs >> 32), (uint32_t) cs, hist, warp, nwarps);
+}
+
+// Pre-phase of step t (pub = (t - 1) & 1), or with what = PHASE_STDP the
+// STDP accumulation of the last step before applyStdp.
+__global__ void __launch_bounds__(STEP_THREADS)
+deliver_kernel(const DevSim S, uint32_t pub, uint32_t what, uint32_t offset, int fromDev)
+{
+	if(fromDev) {
+		uint32_t cur, ring;
+		step_indices(S, offset, cur, ring);
+		pub = cur ^ 1u;
+	}
+	deliver_range(S, pub, what, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, (gridDim.x * blockDim.x) >> 5);
+}
+
+// Grid-wide barrier of the persistent kernel (all CTAs co-resident: it is
+// launched cooperatively).  Thread 0 of each CTA makes the CTA's writes
+// visible (the fence after the CTA barrier), arrives on a launch-wide
+// counter with a release reduction and polls the counter until every CTA
+// has arrived at this barrier: barrier b is complete when the counter
+// reaches (b + 1) x gridDim.x.  A wait gives up after BARRIER_SPIN_LIMIT
+// polls (seconds; a phase takes microseconds): it sets the error word, which
+// makes every CTA leave the step loop at its next barrier, and the host
+// reports the error.
+constexpr uint32_t BARRIER_SPIN_LIMIT = 1u << 24;
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p)
+{
+	uint32_t v;
+	asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+	return v;
+}
+
+__device__ __forceinline__ void red_release_add(uint32_t* p, uint32_t v)
+{
+	asm volatile("red.release.gpu.global.add.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+
+// target: this CTA's count of completed barriers x gridDim.x (shared)
+__device__ __forceinline__ bool grid_barrier(GridBarrier* gb, uint32_t& target, uint32_t& ok)
+{
+	__syncthreads();
+	if(threadIdx.x == 0) {
+		target += gridDim.x;
+		__threadfence();
+		red_release_add(&gb->count, 1u);
+		uint32_t polls = 0;
+		while(ld_acquire(&gb->count) < target) {
+			if(++polls > BARRIER_SPIN_LIMIT || ld_acquire(&gb->error)) {
+				atomicExch(&gb->error, 1u);
+				ok = 0;
+				break;
+			}
+			__nanosleep(20);
+		}
+		__threadfence();
+	}
+	__syncthreads();
+	return ok != 0;
+}
+
+// Persistent step loop: `steps` consecutive steps from cycle `cycle0` in one
+// cooperative launch, each step's pre-phase and update separated by grid
+// barriers, then the STDP accumulation of the last step (so applyStdp may
+// follow directly; its deliveries stay pending for the next step).  CTA c
+// owns the partitions c, c + gridDim.x, ... of P neurons; the pre-phases
+// spread the chunks over all warps of the grid.  Identical results to
+// deliver_kernel + update_kernel per step.
+__global__ void __launch_bounds__(RUN_THREADS, 2)
+run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0, GridBarrier* gb)
+{
+	__shared__ CtaCounters sC;
+	__shared__ uint32_t sTarget, sOk;
+	if(threadIdx.x == 0) {
+		sC = CtaCounters{ 0, 0, 0 };
+		sTarget = 0;
+		sOk = 1;
+	}
+	__syncthreads();
+	const uint32_t nparts = (S.N + P - 1) / P;
+	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+	for(uint32_t k = 0; k < steps; ++k) {
+		const unsigned long long c = cycle0 + k;
+		const uint32_t cur = (uint32_t) (c & 1);
+		const uint32_t ring = (uint32_t) (c % S.R);
+		deliver_range(S, cur ^ 1u, PHASE_DELIVER | PHASE_STDP | PHASE_RESET, warp, nwarps);
+		if(!grid_barrier(gb, sTarget, sOk)) return;
+		for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
+			update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC);
+		}
+		__syncthreads();
+		flush_counters(S, ring, sC);
+		if(!grid_barrier(gb, sTarget, sOk)) return;
+	}
+	if(steps) {
+		const uint32_t last = (uint32_t) ((cycle0 + steps - 1) & 1);
+		deliver_range(S, last, PHASE_STDP, warp, nwarps);
+		if(!grid_barrier(gb, sTarget, sOk)) return;
+		if(blockIdx.x == 0 && threadIdx.x == 0) S.stdpWork.count[last] = 0;
 	}
 }
 
@@ -289,20 +516,20 @@ collect_touched_kernel(const DevSim S)
 	}
 }
 
-// applyStdp over the targets touched since the last call (their incoming
-// plastic synapses are the only ones with a nonzero accumulator).  One warp
-// per chunk; d.w of an apply chunk is its target.
+// applyStdp (src/nemo/ConnectivityMatrix.cpp:241-294) over the targets
+// touched since the last call (their incoming plastic synapses are the only
+// ones with a nonzero accumulator).  One warp per chunk; d.w of an apply
+// chunk is its target.
 __global__ void __launch_bounds__(STEP_THREADS)
-apply_touched_kernel(const DevSim S, int32_t reward, uint32_t par, uint32_t slot)
+apply_touched_kernel(const DevSim S, int32_t reward)
 {
 	const uint32_t nch = *S.applyChunkCount;
 	const uint32_t lane = threadIdx.x & 31;
 	const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-	const uint64_t* hist = S.hist + (size_t) par * S.N;
 	for(uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nch; c += nw) {
 		const uint4 d = S.applyChunks[c];
 		const unsigned long long start = (unsigned long long) d.x | ((unsigned long long) d.y << 32);
-		const uint32_t len = d.z, tgt = d.w;
+		const uint32_t len = d.z;
 		int32_t acc[ILP];
 		uint32_t fwd[ILP];
 		int32_t w[ILP];
@@ -315,27 +542,21 @@ apply_touched_kernel(const DevSim S, int32_t reward, uint32_t par, uint32_t slot
 #pragma unroll
 		for(uint32_t j = 0; j < ILP; ++j) {
 			if(!acc[j]) continue;
-			const unsigned long long p = start + lane + 32 * j;
 			const int32_t nw2 = stdp_updated_weight(S.sp, w[j], fx_mul_dev(reward, acc[j]));
-			if(nw2 != w[j]) {
-				S.syn[fwd[j]].y = (uint32_t) nw2;
-				if(S.D) compensate_inflight(S, hist, S.rcmSrc[p], tgt, slot, w[j], nw2);
-			}
-			S.rcmAcc[p] = 0;
+			if(nw2 != w[j]) S.syn[fwd[j]].y = (uint32_t) nw2;
+			S.rcmAcc[start + lane + 32 * j] = 0;
 		}
 	}
 }
 
-// applyStdp (src/nemo/ConnectivityMatrix.cpp:241-294), first call: one warp
-// per target over every incoming plastic synapse, so that weights that
-// start outside their clamp range are clamped as in the reference.  Later
-// calls use apply_touched_kernel.
+// applyStdp, first call: one warp per target over every incoming plastic
+// synapse, so that weights that start outside their clamp range are clamped
+// as in the reference.  Later calls use apply_touched_kernel.
 __global__ void __launch_bounds__(STEP_THREADS)
-apply_full_kernel(const DevSim S, int32_t reward, uint32_t par, uint32_t slot)
+apply_full_kernel(const DevSim S, int32_t reward)
 {
 	const uint32_t lane = threadIdx.x & 31;
 	const uint32_t warpsTotal = gridDim.x * (STEP_THREADS / 32);
-	const uint64_t* hist = S.hist + (size_t) par * S.N;
 	for(uint32_t tgt = blockIdx.x * (STEP_THREADS / 32) + (threadIdx.x >> 5); tgt < S.N; tgt += warpsTotal) {
 		unsigned long long b = S.rcmPtr[tgt], e = S.rcmPtr[tgt + 1];
 		for(unsigned long long p = b + lane; p < e; p += 32) {
@@ -343,10 +564,7 @@ apply_full_kernel(const DevSim S, int32_t reward, uint32_t par, uint32_t slot)
 			const uint32_t fwd = S.rcmFwd[p];
 			const int32_t w = (int32_t) S.syn[fwd].y;
 			const int32_t nw = stdp_updated_weight(S.sp, w, fx_mul_dev(reward, acc));
-			if(nw != w) {
-				S.syn[fwd].y = (uint32_t) nw;
-				if(S.D) compensate_inflight(S, hist, S.rcmSrc[p], tgt, slot, w, nw);
-			}
+			if(nw != w) S.syn[fwd].y = (uint32_t) nw;
 			if(acc) S.rcmAcc[p] = 0;
 		}
 	}
@@ -625,17 +843,57 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	const unsigned D = std::max(1u, m_maxDelay);
 	std::vector<unsigned long long> outPtr(N + 1);
 	hvector<uint64_t> pos(Sn);
+	// deliverSpikes' validSpikes = ~(~0 << maxDelay) with x86 shift
+	// semantics (src/nemo/cpu/Simulation.cpp:263): nothing is delivered when
+	// the maximum delay is 0 or 64
+	const bool deliver = m_maxDelay >= 1 && m_maxDelay <= 63;
+	std::vector<uint64_t> delayMask(N, 0);
+	uint64_t dlvGroups = 0;  // delay groups of all sources (all pending at once, at most)
 	{
 		hvector<uint64_t> rowStart((size_t) N * D + 1, 0);
 		for(size_t k = 0; k < Sn; ++k) rowStart[(size_t) lsrc[k] * D + sdelay[k]]++;
 		for(size_t r = 0; r < (size_t) N * D; ++r) rowStart[r + 1] += rowStart[r];
 		for(unsigned s = 0; s <= N; ++s) outPtr[s] = rowStart[(size_t) s * D];
+		m_outDegree.resize(N);
+		for(unsigned s = 0; s < N; ++s) {
+			m_outDegree[s] = (uint32_t) (outPtr[s + 1] - outPtr[s]);
+			m_maxOutDeg = std::max(m_maxOutDeg, m_outDegree[s]);
+		}
+		// delay groups: the end of each source's delay-d group within its row
+		const bool narrow = m_maxOutDeg < 65536;
+		hvector<uint16_t> end16(narrow ? (size_t) N * D : 0);
+		hvector<uint32_t> end32(narrow ? 0 : (size_t) N * D);
+		for(unsigned s = 0; s < N; ++s) {
+			const uint64_t base = rowStart[(size_t) s * D];
+			uint64_t prev = 0;
+			for(unsigned d = 1; d <= D; ++d) {
+				const uint64_t e = rowStart[(size_t) s * D + d] - base;
+				if(narrow) end16[(size_t) s * D + d - 1] = (uint16_t) e;
+				else end32[(size_t) s * D + d - 1] = (uint32_t) e;
+				if(deliver && e > prev) {
+					delayMask[s] |= 1ull << (d - 1);
+					++dlvGroups;
+				}
+				prev = e;
+			}
+		}
+		S.dStride = D;
+		if(narrow) {
+			auto* p = dalloc<uint16_t>(end16.size());
+			NB_CUDA(cudaMemcpyAsync(p, end16.data(), end16.size() * 2, cudaMemcpyHostToDevice, m_stream));
+			S.dEnd16 = p;
+			S.dEnd32 = nullptr;
+		} else {
+			auto* p = dalloc<uint32_t>(end32.size());
+			NB_CUDA(cudaMemcpyAsync(p, end32.data(), end32.size() * 4, cudaMemcpyHostToDevice, m_stream));
+			S.dEnd16 = nullptr;
+			S.dEnd32 = p;
+		}
+		auto* dm = dalloc<uint64_t>(N);
+		NB_CUDA(cudaMemcpyAsync(dm, delayMask.data(), (size_t) N * 8, cudaMemcpyHostToDevice, m_stream));
+		S.delayMask = dm;
+		NB_CUDA(cudaStreamSynchronize(m_stream)); // the host tables go out of scope
 		for(size_t k = 0; k < Sn; ++k) pos[k] = rowStart[(size_t) lsrc[k] * D + sdelay[k] - 1]++;
-	}
-	m_outDegree.resize(N);
-	for(unsigned s = 0; s < N; ++s) {
-		m_outDegree[s] = (uint32_t) (outPtr[s + 1] - outPtr[s]);
-		m_maxOutDeg = std::max(m_maxOutDeg, m_outDegree[s]);
 	}
 	{
 		hvector<uint2> syn(Sn);
@@ -725,19 +983,24 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	auto* dRcmPtr = dalloc<unsigned long long>(N + 1);
 	NB_CUDA(cudaMemcpyAsync(dRcmPtr, rcmPtr.data(), (N + 1) * 8, cudaMemcpyHostToDevice, m_stream));
 	S.rcmPtr = dRcmPtr;
-	// chunk lists: enough for every neuron firing and being an STDP target
-	// in the same step
+	// work lists: room for every delay group of every source pending and
+	// every neuron being an STDP target in the same step (entries are
+	// counted in 32 bits)
 	{
-		const uint64_t CH = 128;
-		uint64_t capF = 0, capS = 0;
-		for(unsigned n = 0; n < N; ++n) {
-			capF += (outPtr[n + 1] - outPtr[n] + CH - 1) / CH;
-			capS += (rcmPtr[n + 1] - rcmPtr[n] + CH - 1) / CH;
+		const uint64_t plastic = rcmPtr[N];
+		if(Sn >= (1ull << 32) || plastic >= (1ull << 32) || dlvGroups >= (1ull << 32)) {
+			NB_THROW(NEMO_API_UNSUPPORTED, "network too large for the work lists");
 		}
-		if(capF + capS >= (1ull << 32)) NB_THROW(NEMO_API_UNSUPPORTED, "network too large for the chunk lists");
-		S.chunks = dalloc<uint4>(capF + capS);
-		S.chunkCount = dalloc<uint32_t>(2);
-		S.applyChunks = dalloc<uint4>(capS);
+		auto makeList = [&](WorkList& L, uint64_t groups, uint64_t entries) {
+			L.group = dalloc<uint4>(groups);
+			L.count = dalloc<unsigned long long>(2);
+			L.bucket = dalloc<uint32_t>(entries / BUCKET + 1);
+		};
+		makeList(S.dlvWork, dlvGroups, Sn);
+		makeList(S.stdpWork, N, plastic);
+		uint64_t capA = 0;
+		for(unsigned n = 0; n < N; ++n) capA += (rcmPtr[n + 1] - rcmPtr[n] + CHUNK - 1) / CHUNK;
+		S.applyChunks = dalloc<uint4>(capA);
 		S.applyChunkCount = dalloc<uint32_t>(1);
 	}
 
@@ -761,13 +1024,7 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	S.fstim = dalloc<uint32_t>(S.W);
 	S.touchedBits = dalloc<uint32_t>(S.W);
 	S.curExt = dalloc<float>(N);
-	// validSpikes = ~(~0 << maxDelay) with x86 shift semantics
-	// (src/nemo/cpu/Simulation.cpp:263): nothing is delivered when the
-	// maximum delay is 0 or 64
-	S.D = (m_maxDelay >= 1 && m_maxDelay <= 63) ? m_maxDelay + 1 : 0;
-	S.slots = S.D ? dalloc<uint2>((size_t) S.D * N) : nullptr;
-	S.slotHigh = S.D ? dalloc<int2>((size_t) S.D * N) : nullptr;
-	S.slotFlag = dalloc<uint32_t>(std::max(1u, S.D));
+	S.slot = dalloc<ulonglong2>(N);
 	S.cycleDev = dalloc<unsigned long long>(1);
 	NB_CUDA(cudaMallocHost(&m_hCycle, 8));
 	S.R = (uint32_t) std::max<size_t>(16, std::min<size_t>(1024, (64u << 20) / ((size_t) S.W * 4)));
@@ -780,10 +1037,25 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	if(needCalib) S.calib = device_calibration(m_device);
 	NB_CUDA(cudaDeviceGetAttribute(&m_sms, cudaDevAttrMultiProcessorCount, m_device));
 	m_deliverGrid = (unsigned) m_sms * 8;
-	// default launch shape: two partitions per SM
+	// default shape of the two-launch step (set while the persistent loop is
+	// not yet configured): two partitions per SM
 	{
 		uint32_t P = (uint32_t) ((N + 2 * m_sms - 1) / (2 * m_sms));
 		setLaunch(P, std::min<uint32_t>(1024, std::max<uint32_t>(128, (P + 31) & ~31u)));
+	}
+	// the persistent step loop needs every CTA resident at once: a
+	// cooperative launch of at most the occupancy limit
+	{
+		int coop = 0;
+		NB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, m_device));
+		m_runGrid = coop ? runGridFor(RUN_THREADS) : 0;
+		if(m_runGrid) {
+			const size_t per = (N + m_runGrid - 1) / m_runGrid;
+			m_runP = (uint32_t) std::max<size_t>(32, (per + 31) & ~(size_t) 31);
+			m_barrier = dalloc<GridBarrier>(1);
+			NB_CUDA(cudaMallocHost(&m_hBarrierError, 4));
+			*m_hBarrierError = 0;
+		}
 	}
 	NB_CUDA(cudaStreamSynchronize(m_stream));
 	resetTimer();
@@ -796,6 +1068,7 @@ Simulation::~Simulation()
 	for(void* p : m_allocs) cudaFree(p);
 	if(m_graph) cudaGraphExecDestroy(m_graph);
 	if(m_hCycle) cudaFreeHost(m_hCycle);
+	if(m_hBarrierError) cudaFreeHost(m_hBarrierError);
 	if(m_hFired) cudaFreeHost(m_hFired);
 	if(m_hStim) cudaFreeHost(m_hStim);
 	if(m_dStim) cudaFree(m_dStim);
@@ -844,8 +1117,26 @@ void Simulation::timedEnd()
 	NB_CUDA(cudaEventRecord(m_evPool[m_evUse.back().second + 1], m_stream));
 }
 
+unsigned Simulation::runGridFor(uint32_t T) const
+{
+	int perSm = 0;
+	NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, run_kernel, (int) T, 0));
+	return perSm > 0 ? (unsigned) perSm * (unsigned) m_sms : 0u;
+}
+
 void Simulation::setLaunch(uint32_t P, uint32_t T)
 {
+	if(persistentActive()) {
+		// any multiple of 32 neurons per partition; 64 to RUN_THREADS threads
+		m_runP = std::max<uint32_t>(32, (std::min<uint32_t>(P, 1u << 30) + 31) & ~31u);
+		T = std::max<uint32_t>(64, std::min<uint32_t>(RUN_THREADS, (T + 31) & ~31u));
+		const unsigned g = runGridFor(T);
+		if(g) {
+			m_runT = T;
+			m_runGrid = g;
+		}
+		return;
+	}
 	P = std::max<uint32_t>(32, std::min<uint32_t>(MAX_PARTITION, (P + 31) & ~31u));
 	T = std::max<uint32_t>(32, std::min<uint32_t>(1024, (T + 31) & ~31u));
 	// the per-CTA work offsets are 32-bit
@@ -857,24 +1148,75 @@ void Simulation::setLaunch(uint32_t P, uint32_t T)
 void Simulation::launchStep(bool /*fullRecord*/)
 {
 	const uint32_t cur = (uint32_t) (m_cycle & 1);
-	const uint32_t slot = m_dev.D ? (uint32_t) (m_cycle % m_dev.D) : 0;
 	const uint32_t ring = (uint32_t) (m_cycle % m_dev.R);
 	const unsigned grid = (m_N + m_P - 1) / m_P;
-	timedBegin(K_STEP);
-	update_kernel<<<grid, m_T, 0, m_stream>>>(m_dev, m_P, cur, slot, ring, 0, 0);
-	timedEnd();
 	timedBegin(K_STDP);
-	deliver_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, cur, slot, 0, 0);
+	deliver_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, cur ^ 1u,
+			PHASE_DELIVER | PHASE_STDP | PHASE_RESET, 0, 0);
+	timedEnd();
+	timedBegin(K_STEP);
+	update_kernel<<<grid, m_T, 0, m_stream>>>(m_dev, m_P, cur, ring, 0, 0);
 	timedEnd();
 	m_cycle++;
 	m_timerSteps++;
+	m_stdpPending = true;
 }
 
-// n consecutive steps: whole CUDA graphs of GRAPH_STEPS steps (captured once
-// per launch shape and replayed from a device cycle counter), then single
-// launches for the rest
+// the STDP accumulation of the last step, which the next step's pre-phase
+// would otherwise run (before applyStdp, that must be now)
+void Simulation::flushStdp()
+{
+	if(!m_stdpPending) return;
+	m_stdpPending = false;
+	if(!m_dev.stdp || m_cycle == 0) return;
+	const uint32_t last = (uint32_t) ((m_cycle - 1) & 1);
+	timedBegin(K_STDP);
+	deliver_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, last, PHASE_STDP, 0, 0);
+	timedEnd();
+	NB_CUDA(cudaMemsetAsync(m_dev.stdpWork.count + last, 0, 8, m_stream));
+}
+
+// n consecutive steps in one cooperative launch of the persistent step loop
+void Simulation::launchRun(unsigned n)
+{
+	NB_CUDA(cudaMemsetAsync(m_barrier, 0, sizeof(GridBarrier), m_stream));
+	DevSim dev = m_dev;
+	uint32_t P = m_runP, steps = n;
+	unsigned long long c0 = m_cycle;
+	GridBarrier* gb = m_barrier;
+	void* args[] = { &dev, &P, &steps, &c0, &gb };
+	// no more CTAs than partitions (a CTA without one only takes part in the
+	// delivery phase, which the other CTAs' warps cover as well)
+	const unsigned grid = (unsigned) std::min<uint64_t>(m_runGrid, std::max<uint64_t>(1, (m_N + P - 1) / P));
+	timedBegin(K_RUN);
+	NB_CUDA(cudaLaunchCooperativeKernel((const void*) run_kernel, dim3(grid), dim3(m_runT), args, 0, m_stream));
+	timedEnd();
+	m_cycle += n;
+	m_timerSteps += n;
+	m_stdpPending = false;  // the loop ends with the last step's STDP accumulation
+	// read back with the run's statistics; checked by checkBarrier()
+	NB_CUDA(cudaMemcpyAsync(m_hBarrierError, &m_barrier->error, 4, cudaMemcpyDeviceToHost, m_stream));
+}
+
+// after a stream synchronisation: a grid-barrier wait of the persistent step
+// loop that gave up leaves the simulation state undefined
+void Simulation::checkBarrier()
+{
+	if(m_hBarrierError && *m_hBarrierError) {
+		*m_hBarrierError = 0;
+		NB_THROW(NEMO_CUDA_ERROR, "persistent step loop: a grid barrier wait timed out");
+	}
+}
+
+// n consecutive steps: the persistent step loop, or whole CUDA graphs of
+// GRAPH_STEPS two-launch steps (captured once per launch shape and replayed
+// from a device cycle counter) and single launches for the rest
 void Simulation::launchSteps(unsigned n)
 {
+	if(usePersistent && m_runGrid && n > 1) {
+		launchRun(n);
+		return;
+	}
 	if(!useGraphs || profiling || n < GRAPH_STEPS) {
 		for(unsigned i = 0; i < n; ++i) launchStep(false);
 		return;
@@ -886,6 +1228,7 @@ void Simulation::launchSteps(unsigned n)
 		NB_CUDA(cudaGraphLaunch(m_graph, m_stream));
 		m_cycle += GRAPH_STEPS;
 		m_timerSteps += GRAPH_STEPS;
+		m_stdpPending = true;
 		n -= GRAPH_STEPS;
 	}
 	// the pinned cycle value must not change before the copy above ran
@@ -904,8 +1247,9 @@ void Simulation::buildGraph()
 	cudaGraph_t g;
 	NB_CUDA(cudaStreamBeginCapture(m_stream, cudaStreamCaptureModeThreadLocal));
 	for(unsigned k = 0; k < GRAPH_STEPS; ++k) {
-		update_kernel<<<grid, m_T, 0, m_stream>>>(m_dev, m_P, 0, 0, 0, k, 1);
-		deliver_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, 0, 0, k, 1);
+		deliver_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, 0,
+				PHASE_DELIVER | PHASE_STDP | PHASE_RESET, k, 1);
+		update_kernel<<<grid, m_T, 0, m_stream>>>(m_dev, m_P, 0, 0, k, 1);
 	}
 	advance_cycle_kernel<<<1, 1, 0, m_stream>>>(m_dev.cycleDev, GRAPH_STEPS);
 	NB_CUDA(cudaStreamEndCapture(m_stream, &g));
@@ -982,20 +1326,16 @@ const std::vector<unsigned>& Simulation::step(const unsigned* fstim, size_t nf,
 
 void Simulation::applyStdpDevice(int32_t R)
 {
-	// the last completed step's history and slot; before the first step
-	// the history is all zero, so nothing is in flight
-	const uint64_t last = m_cycle ? m_cycle - 1 : 0;
-	const uint32_t par = (uint32_t) (last & 1);
-	const uint32_t slot = m_dev.D ? (uint32_t) (last % m_dev.D) : 0;
+	flushStdp();
 	const bool fullPassDone = m_weightsClamped;
 	timedBegin(K_APPLY);
 	if(!m_weightsClamped) {
 		unsigned grid = std::min<unsigned>((m_N + 7) / 8, (unsigned) m_sms * 8);
-		apply_full_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, R, par, slot);
+		apply_full_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, R);
 	} else {
 		unsigned cgrid = std::max(1u, std::min<unsigned>((m_dev.W + STEP_THREADS - 1) / STEP_THREADS, (unsigned) m_sms * 4));
 		collect_touched_kernel<<<cgrid, STEP_THREADS, 0, m_stream>>>(m_dev);
-		apply_touched_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, R, par, slot);
+		apply_touched_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, R);
 	}
 	timedEnd();
 	// updatedWeight's result always lies within the clamp range of its sign
@@ -1070,6 +1410,7 @@ void Simulation::run(unsigned steps, unsigned stdpPeriod, float reward, unsigned
 		}
 		sync();
 		NB_CUDA(cudaGetLastError());
+		checkBarrier();
 		float ms = 0;
 		NB_CUDA(cudaEventElapsedTime(&ms, m_ev0, m_ev1));
 		runMs += ms;
@@ -1160,13 +1501,18 @@ float Simulation::autotune(unsigned trialSteps)
 	regions.emplace_back(m_dev.hist, (size_t) 2 * m_N * 8);
 	regions.emplace_back(m_dev.fstim, (size_t) m_dev.W * 4);
 	regions.emplace_back(m_dev.curExt, (size_t) m_N * 4);
-	if(m_dev.D) {
-		regions.emplace_back(m_dev.slots, (size_t) m_dev.D * m_N * 8);
-		regions.emplace_back(m_dev.slotHigh, (size_t) m_dev.D * m_N * 8);
-		regions.emplace_back(m_dev.slotFlag, (size_t) m_dev.D * 4);
+	regions.emplace_back(m_dev.slot, (size_t) m_N * 16);
+	// the work lists published by the last step (pending for the next)
+	for(const WorkList* L : { &m_dev.dlvWork, &m_dev.stdpWork }) {
+		unsigned long long c[2];
+		NB_CUDA(cudaMemcpy(c, L->count, 16, cudaMemcpyDeviceToHost));
+		const uint64_t groups = std::max(c[0] >> 32, c[1] >> 32);
+		const uint64_t entries = std::max(c[0] & 0xffffffffull, c[1] & 0xffffffffull);
+		regions.emplace_back(L->group, (size_t) groups * 16);
+		regions.emplace_back(L->bucket, (size_t) (entries / BUCKET + 1) * 4);
+		regions.emplace_back(L->count, 16);
 	}
 	if(m_dev.stdp) regions.emplace_back(m_dev.rcmAcc, (size_t) lastPlastic * 4);
-	regions.emplace_back(m_dev.chunkCount, 8);
 	regions.emplace_back(m_dev.applyChunkCount, 4);
 	regions.emplace_back(m_dev.touchedBits, (size_t) m_dev.W * 4);
 	std::vector<void*> backup;
@@ -1183,6 +1529,7 @@ float Simulation::autotune(unsigned trialSteps)
 	}
 	const uint64_t cycle = m_cycle;
 	const unsigned long timerSteps = m_timerSteps;
+	const bool stdpPending = m_stdpPending;
 	const bool prof = profiling;
 	profiling = false;
 	auto restore = [&]() {
@@ -1193,36 +1540,58 @@ float Simulation::autotune(unsigned trialSteps)
 		}
 		m_cycle = cycle;
 		m_timerSteps = timerSteps;
+		m_stdpPending = stdpPending;
 	};
 
-	// candidates: 1 to 16 partitions per SM, 128 to 1024 threads per CTA
 	std::vector<std::pair<uint32_t, uint32_t>> cands;
-	for(unsigned k : {1u, 2u, 3u, 4u, 6u, 8u, 12u, 16u}) {
-		uint32_t P = (uint32_t) ((m_N + (size_t) k * m_sms - 1) / ((size_t) k * m_sms));
-		P = std::max<uint32_t>(32, std::min<uint32_t>(MAX_PARTITION, (P + 31) & ~31u));
-		for(uint32_t T : {128u, 256u, 512u, 1024u}) {
-			if(T > std::max<uint32_t>(128, P)) continue;
-			if(std::find(cands.begin(), cands.end(), std::make_pair(P, T)) == cands.end()) cands.emplace_back(P, T);
+	const bool pers = persistentActive();
+	if(pers) {
+		// persistent loop: 192 to RUN_THREADS threads per CTA, 1 to 4 partitions per CTA
+		for(uint32_t T : {192u, 256u, RUN_THREADS}) {
+			const unsigned g = runGridFor(T);
+			if(!g) continue;
+			for(unsigned k : {1u, 2u, 4u}) {
+				uint32_t P = (uint32_t) ((m_N + (size_t) k * g - 1) / ((size_t) k * g));
+				P = std::max<uint32_t>(32, (P + 31) & ~31u);
+				if(std::find(cands.begin(), cands.end(), std::make_pair(P, T)) == cands.end()) cands.emplace_back(P, T);
+			}
+		}
+	} else {
+		// two-launch step: 1 to 16 partitions per SM, 128 to 1024 threads per CTA
+		for(unsigned k : {1u, 2u, 3u, 4u, 6u, 8u, 12u, 16u}) {
+			uint32_t P = (uint32_t) ((m_N + (size_t) k * m_sms - 1) / ((size_t) k * m_sms));
+			P = std::max<uint32_t>(32, std::min<uint32_t>(MAX_PARTITION, (P + 31) & ~31u));
+			for(uint32_t T : {128u, 256u, 512u, 1024u}) {
+				if(T > std::max<uint32_t>(128, P)) continue;
+				if(std::find(cands.begin(), cands.end(), std::make_pair(P, T)) == cands.end()) cands.emplace_back(P, T);
+			}
 		}
 	}
-	const uint32_t P0 = m_P, T0 = m_T;
+	const uint32_t P0 = partition(), T0 = threads();
 	float best = -1;
 	uint32_t bestP = P0, bestT = T0;
 	try {
 		for(auto& c : cands) {
 			setLaunch(c.first, c.second);
-			launchStep(false); // untimed warm-up of this shape
+			// untimed warm-up of this shape
+			if(pers) launchRun(1);
+			else launchStep(false);
 			NB_CUDA(cudaEventRecord(m_ev0, m_stream));
-			for(unsigned i = 0; i < trialSteps; ++i) launchStep(false);
+			if(pers) {
+				launchRun(trialSteps);
+			} else {
+				for(unsigned i = 0; i < trialSteps; ++i) launchStep(false);
+			}
 			NB_CUDA(cudaEventRecord(m_ev1, m_stream));
 			sync();
 			NB_CUDA(cudaGetLastError());
+			checkBarrier();
 			float ms = 0;
 			NB_CUDA(cudaEventElapsedTime(&ms, m_ev0, m_ev1));
 			if(best < 0 || ms < best) {
 				best = ms;
-				bestP = m_P;
-				bestT = m_T;
+				bestP = partition();
+				bestT = threads();
 			}
 			restore();
 		}

@@ -18,6 +18,15 @@ namespace nemo_b200 {
 constexpr unsigned MAX_TYPES = 8;
 constexpr unsigned STEP_THREADS = 256;   // block size of the apply/stimulus kernels
 constexpr unsigned MAX_PARTITION = 2048; // neurons per CTA of the step kernel
+constexpr unsigned RUN_THREADS = 384;    // block size of the persistent step loop
+
+// Grid barrier of the persistent step loop (device memory, zeroed before
+// each launch).
+struct GridBarrier {
+	uint32_t count;  // arrivals so far: barrier b of the launch is complete at (b + 1) x CTAs
+	uint32_t error;  // set when a wait gave up
+	uint32_t pad[2];
+};
 
 struct TypeRange {
 	int kind;
@@ -35,6 +44,17 @@ struct StdpParams {
 	int32_t minE, maxE, minI, maxI;
 };
 
+// A list of ranges ("groups") published by one phase for the next, which
+// spreads their entries evenly over all warps of the GPU: group i is
+// {start lo, start hi, length, first entry}, its entries numbered
+// consecutively after those of groups 0..i-1, and bucket[b] is the group
+// that holds entry 32 b.
+struct WorkList {
+	uint4* group;
+	unsigned long long* count;  // [2] by the parity of the publishing step: groups << 32 | entries
+	uint32_t* bucket;
+};
+
 // Everything a kernel needs, passed by value.  Neuron arrays use the
 // backend-local index: type order, then insertion order
 // (src/nemo/cpu/Simulation.cpp:58-73).
@@ -42,18 +62,23 @@ struct DevSim {
 	uint32_t N;       // neurons
 	uint32_t W;       // 32-bit words per neuron bit-vector
 	uint32_t ntypes;
-	uint32_t D;       // accumulator slots (max delay + 1); 0 = nothing is ever delivered
+	uint32_t dStride; // entries per source in the delay-group tables (the maximum delay)
 	uint32_t R;       // firing ring length (steps)
 	TypeRange types[MAX_TYPES];
 	uint32_t* rng;            // [4][N] xorshift words
 	uint64_t* hist;           // [2][N] firing history, double-buffered by step parity
 	uint32_t* fstim;          // [W] pending firing stimulus
 	float* curExt;            // [N] pending current stimulus
-	uint2* slots;             // [D][N] low words of the E and -I fixed-point sums per delivery step
-	int2* slotHigh;           // [D][N] their high words (touched only on carry/borrow)
-	uint32_t* slotFlag;       // [D] set when a slot holds a nonzero high word
-	const unsigned long long* outPtr; // [N+1] outgoing synapses per source
+	ulonglong2* slot;         // [N] int64 E and I fixed-point sums (two's complement) of this step's arrivals
+	const unsigned long long* outPtr; // [N+1] outgoing synapses per source, sorted by delay
 	uint2* syn;               // [S] {target | (delay - 1) << 26, weight}
+	// delay groups: bit d - 1 of delayMask[n] is set when source n has
+	// synapses of delay d that deliverSpikes delivers; dEnd[n][d - 1] is the
+	// end of its delay-d group within its row (uint16 when every row is
+	// shorter than 65536, else uint32; the other pointer is null)
+	const uint64_t* delayMask;
+	const uint16_t* dEnd16;
+	const uint32_t* dEnd32;
 	uint32_t* firedRing;      // [R][W] fired bit-vector per step
 	uint32_t* firedCount;     // [R]
 	unsigned long long* eventCount; // [R] synaptic events (out-degree of fired neurons)
@@ -63,10 +88,10 @@ struct DevSim {
 	const uint32_t* rcmSrc;   // source | (delay - 1) << 26
 	const uint32_t* rcmFwd;   // index into syn
 	int32_t* rcmAcc;          // STDP accumulator per incoming plastic synapse
-	// work of the current step, published by update_kernel for deliver_kernel:
-	// {start lo, start hi, length <= 128, 0 = outgoing synapses | 1 = STDP}
-	uint4* chunks;
-	uint32_t* chunkCount;     // [2] by step parity
+	// work published by a step's update for the next pre-phase: the delay
+	// groups arriving next step (ranges of syn) and the incoming plastic
+	// synapses of its STDP targets (ranges of the reverse matrix)
+	WorkList dlvWork, stdpWork;
 	// incoming plastic synapses of the targets touched since the last
 	// applyStdp: {start lo, start hi, length, target}
 	uint4* applyChunks;
@@ -115,20 +140,26 @@ public:
 	void resetTimer();
 
 	// timing of the last run(): whole run and, when profiling is on, each
-	// kernel kind (CUDA events around every launch)
-	enum { K_STEP = 0, K_STDP = 1, K_APPLY = 2, K_KINDS = 3 };  // update, deliver, applyStdp
+	// kernel kind (CUDA events around every launch): update and deliver
+	// kernels of the two-launch step, applyStdp, persistent step loop
+	enum { K_STEP = 0, K_STDP = 1, K_APPLY = 2, K_RUN = 3, K_KINDS = 4 };
 	float lastRunMs = 0;
-	float kernelMs[K_KINDS] = {0, 0, 0};
-	unsigned kernelLaunches[K_KINDS] = {0, 0, 0};
+	float kernelMs[K_KINDS] = {0, 0, 0, 0};
+	unsigned kernelLaunches[K_KINDS] = {0, 0, 0, 0};
 	uint64_t lastFired = 0, lastEvents = 0, lastStdpEntries = 0, lastPlastic = 0;
 	bool profiling = false;
-	bool useGraphs = true;  // replay the step loop from CUDA graphs in run()
+	bool useGraphs = true;  // replay the two-launch step loop from CUDA graphs in run()
+	// run() advances its step loop with one persistent cooperative launch per
+	// segment between applyStdp calls (else with the two-launch step)
+	bool usePersistent = true;
 
-	// partition size (neurons per CTA) and threads per CTA of the step
-	// kernel; results do not depend on them
-	uint32_t partition() const { return m_P; }
-	uint32_t threads() const { return m_T; }
+	// launch shape of the active step loop (persistent or two-launch):
+	// partition size (neurons per partition; a CTA owns one or more) and
+	// threads per CTA; results do not depend on them
+	uint32_t partition() const { return persistentActive() ? m_runP : m_P; }
+	uint32_t threads() const { return persistentActive() ? m_runT : m_T; }
 	void setLaunch(uint32_t P, uint32_t T);
+	bool persistentActive() const { return usePersistent && m_runGrid != 0; }
 	// time candidate launch shapes on trial steps from a saved copy of the
 	// simulation state, restore it, and keep the fastest; returns its time
 	// per step in microseconds
@@ -149,6 +180,16 @@ private:
 	size_t synapseKey(uint64_t id) const;
 	void launchStep(bool fullRecord);
 	void launchSteps(unsigned n);
+	void launchRun(unsigned n);
+	void flushStdp();
+	bool m_stdpPending = false;  // the last step's STDP accumulation has not run yet
+	void checkBarrier();
+	GridBarrier* m_barrier = nullptr;
+	uint32_t* m_hBarrierError = nullptr;  // pinned copy of m_barrier->error
+	unsigned m_runGrid = 0;  // co-resident CTAs of run_kernel at m_runT threads (0: no cooperative launch)
+	uint32_t m_runP = 0;     // neurons per partition of run_kernel
+	uint32_t m_runT = RUN_THREADS;
+	unsigned runGridFor(uint32_t T) const;
 	void buildGraph();
 	static constexpr unsigned GRAPH_STEPS = 100;
 	cudaGraphExec_t m_graph = nullptr;

@@ -56,9 +56,11 @@ def test_batch_member_matches_oracle():
     assert np.array_equal(c, co) and np.array_equal(i, io)
 
 
-def test_batch_with_stdp_and_launch_shapes():
+@pytest.mark.parametrize("persistent", [True, False])
+def test_batch_with_stdp_and_launch_shapes(persistent):
     specs = sweep(seed=5, count=4, stdp=True)
     batch = nb.Batch([build(nb, s) for s in specs], nets.standard_stdp(nb))
+    batch.set_persistent(persistent)
     batch.set_launch(64, 64)
     counts, _, ids = batch.run(300, 100, 1.0)
     streams = batch.streams(counts, ids)

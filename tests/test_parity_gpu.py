@@ -116,11 +116,14 @@ def test_step_matches_run():
     assert counts.sum() == len(stream)
 
 
-def test_stdp_bitexact():
+@pytest.mark.parametrize("persistent", [True, False])
+def test_stdp_bitexact(persistent):
     """A 2000 x 200 random network with STDP (delays 1-20, window 20+20,
-    applyStdp(1.0) every 100 ms): fire stream, state and every weight."""
+    applyStdp(1.0) every 100 ms): fire stream, state and every weight, with
+    the persistent step loop and with the two-launch step."""
     sims = (nb.Simulation(nb.example_random(2000, 200, 20, True), nets.standard_stdp(nb)),
             O.Simulation(O.example_random(2000, 200, 20, True), nets.standard_stdp(O)))
+    sims[0].set_persistent(persistent)
     p, o = run_both(sims, 1000, stdp_period=100)
     assert_streams_equal(p, o)
     nsyn = 2000 * 200
@@ -130,11 +133,13 @@ def test_stdp_bitexact():
     assert same_bits(sims[0].type_state(0, 2, 2000), sims[1].type_state(0, 2, 2000))
 
 
-def test_stdp_inflight_compensation():
+@pytest.mark.parametrize("persistent", [True, False])
+def test_stdp_inflight_compensation(persistent):
     """applyStdp between a spike's emission and its arrival: the arriving
     weight is the updated one (long delays, frequent applyStdp)."""
     sims = (nb.Simulation(nb.example_random(1500, 150, 40, True), nets.standard_stdp(nb, n=20)),
             O.Simulation(O.example_random(1500, 150, 40, True), nets.standard_stdp(O, n=20)))
+    sims[0].set_persistent(persistent)
     p, o = run_both(sims, 600, stdp_period=7, reward=0.8)
     assert_streams_equal(p, o)
     assert np.array_equal(sims[0].weights_fx(1500 * 150), sims[1].weights_fx(1500 * 150))
@@ -153,11 +158,14 @@ def test_mixed_plugins_bitexact():
         assert same_bits(sims[0].type_state(t, ns, n), sims[1].type_state(t, ns, n))
 
 
+@pytest.mark.parametrize("persistent", [True, False])
 @pytest.mark.parametrize("shape", [(32, 32), (64, 64), (96, 128), (256, 128), (1024, 256), (2048, 1024)])
-def test_launch_shape_does_not_change_results(shape):
-    """Any partition size / block size gives the same bit-exact results."""
+def test_launch_shape_does_not_change_results(shape, persistent):
+    """Any partition size / block size gives the same bit-exact results, in
+    either step-loop mode (the reference simulation uses the default)."""
     ref = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
     sim = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
+    sim.set_persistent(persistent)
     sim.set_launch(*shape)
     assert sim.launch()[0] == shape[0]
     a = ref.run(300, 100, 1.0)
@@ -167,10 +175,13 @@ def test_launch_shape_does_not_change_results(shape):
 
 
 def test_graph_replay_matches_single_launches():
-    """run() replays 100-step CUDA graphs from a device cycle counter; the
-    results equal single launches, across applyStdp calls and remainders."""
+    """The two-launch step loop replays 100-step CUDA graphs from a device
+    cycle counter; the results equal single launches, across applyStdp calls
+    and remainders."""
     a = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
     b = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
+    a.set_persistent(False)
+    b.set_persistent(False)
     b.set_graphs(False)
     for steps, period in [(537, 100), (250, 0), (333, 70)]:
         ra = a.run(steps, period, 1.0)
@@ -184,10 +195,28 @@ def test_graph_replay_matches_single_launches():
     assert np.array_equal(a.weights_fx(450000), b.weights_fx(450000))
 
 
-def test_autotune_restores_state():
+def test_persistent_loop_matches_two_launch_step():
+    """The persistent step loop (one cooperative launch per segment between
+    applyStdp calls) equals the two-launch step, across applyStdp calls,
+    remainders, single-step segments and interleaved nemo_step calls."""
+    a = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
+    b = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
+    b.set_persistent(False)
+    for steps, period in [(537, 100), (250, 0), (333, 70), (5, 1), (101, 2)]:
+        ra = a.run(steps, period, 1.0)
+        rb = b.run(steps, period, 1.0)
+        assert np.array_equal(ra[0], rb[0]) and np.array_equal(ra[2], rb[2])
+        assert list(a.step()) == list(b.step())
+    assert np.array_equal(a.weights_fx(450000), b.weights_fx(450000))
+    assert same_bits(a.type_state(0, 2, 3000), b.type_state(0, 2, 3000))
+
+
+@pytest.mark.parametrize("persistent", [True, False])
+def test_autotune_restores_state(persistent):
     """The autotuner's trial steps leave the simulation exactly as it was."""
     ref = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
     sim = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
+    sim.set_persistent(persistent)
     a0 = ref.run(150, 100, 1.0)
     b0 = sim.run(150, 100, 1.0)
     us = sim.autotune(20)
