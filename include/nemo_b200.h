@@ -353,6 +353,31 @@ NEMO_B200_API nemo_status_t nemo_b200_bptt_readout(nemo_b200_bptt_t, float* out,
 NEMO_B200_API nemo_status_t nemo_b200_bptt_backward(nemo_b200_bptt_t, const float* w, const float* a, const float* b,
 		const float* c, const float* d, const float* noise, const float* target, float* dw, float* da, float* db,
 		void* stream);
+/* Extension with no counterpart in the reference: nemo_step (same stimulus
+ * arguments and results) that allocates no memory of any kind -- no device
+ * or pinned allocation, no host heap, no allocating library call -- for
+ * callers that must not allocate: a closed-loop controller stepping the
+ * simulation every millisecond from a real-time thread, where a device
+ * allocation or free would synchronise the device and stall the loop, or a
+ * host application whose memory is budgeted up front.  The stimulus is
+ * staged in a fixed static buffer of NEMO_B200_NO_ALLOC_STIMULUS_MAX 32-bit
+ * words on each device; fstim_count + 2 x istim_count above that returns
+ * NEMO_BUFFER_OVERFLOW without stepping.  The fired neurons' ids (in
+ * nemo_step's order) are written to fired[0 .. fired_capacity); *fired_count
+ * receives their number, and NEMO_BUFFER_OVERFLOW is returned (after the
+ * step) when it exceeds fired_capacity.  An invalid neuron index returns
+ * NEMO_INVALID_INPUT without stepping; a batch of networks returns
+ * NEMO_API_UNSUPPORTED.  Errors are reported by the status code only
+ * (formatting a message would allocate): nemo_strerror is not updated.  The
+ * first call on a device looks up the static buffer's device address and
+ * should come before any stream capture.  The static buffers are shared:
+ * calls that overlap in time, from several threads or on several
+ * simulations, race and must be serialised by the caller. */
+#define NEMO_B200_NO_ALLOC_STIMULUS_MAX 65536
+NEMO_B200_API nemo_status_t nemo_b200_step_no_alloc(nemo_simulation_t,
+		const unsigned fstim_nidx[], size_t fstim_count,
+		const unsigned istim_nidx[], const float istim_current[], size_t istim_count,
+		unsigned fired[], size_t fired_capacity, size_t* fired_count);
 /* Host build of the device's glibc-exact nrand (for tests): advances the
  * xorshift state in place and returns the normal deviate. */
 NEMO_B200_API float nemo_b200_host_nrand(unsigned state[4]);

@@ -238,6 +238,22 @@ class Simulation:
             return []
         return np.ctypeslib.as_array(fired, shape=(n.value,)).tolist()
 
+    def step_no_alloc(self, fstim=None, istim=None, capacity: int = 1 << 16):
+        """step() through nemo_b200_step_no_alloc, which allocates nothing (an
+        extension): returns (status code, fired ids).  Errors are status codes
+        only (NEMO_INVALID_INPUT, NEMO_BUFFER_OVERFLOW, ...), not exceptions."""
+        f = _u32(fstim) if fstim is not None and len(fstim) else _EMPTY_U32
+        if istim:
+            inid = _u32([p[0] for p in istim])
+            icur = _f32([p[1] for p in istim])
+        else:
+            inid, icur = _EMPTY_U32, _EMPTY_F32
+        out = np.zeros(max(capacity, 1), np.uint32)
+        n = C.c_size_t()
+        status = lib().nemo_b200_step_no_alloc(self._h, f, 0 if f is _EMPTY_U32 else len(f), inid, icur,
+                                               0 if inid is _EMPTY_U32 else len(inid), out, capacity, C.byref(n))
+        return status, out[:min(n.value, capacity)].tolist()
+
     def run(self, steps: int, stdp_period: int = 0, reward: float = 1.0, ids: bool = True,
             max_ids: int | None = None):
         """Device-resident run of `steps` unstimulated steps (an extension):

@@ -52,6 +52,7 @@ SIGNATURES = {
     "nemo_new_simulation": (vp, [vp, vp]),
     "nemo_delete_simulation": (None, [vp]),
     "nemo_step": (st, [vp, u32p, sz, u32p, f32p, sz, C.POINTER(PU), C.POINTER(sz)]),
+    "nemo_b200_step_no_alloc": (st, [vp, u32p, sz, u32p, f32p, sz, u32p, sz, C.POINTER(sz)]),
     "nemo_apply_stdp": (st, [vp, C.c_float]),
     "nemo_get_membrane_potential": (st, [vp, C.c_uint, PF]),
     "nemo_get_neuron_state_n": (st, [vp, C.c_uint, C.c_uint, PF]),

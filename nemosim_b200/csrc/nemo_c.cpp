@@ -441,6 +441,19 @@ nemo_status_t nemo_step(nemo_simulation_t s, unsigned fstim[], size_t nf, unsign
 	});
 }
 
+// Allocation-free: no CALL wrapper (its error path formats a message) and
+// no exception may escape (stepNoAlloc throws nothing).
+nemo_status_t nemo_b200_step_no_alloc(nemo_simulation_t s, const unsigned fstim[], size_t nf, const unsigned inidx[],
+		const float icur[], size_t ni, unsigned fired[], size_t cap, size_t* nfired)
+{
+	if(!s || !nfired || (nf && !fstim) || (ni && (!inidx || !icur)) || (cap && !fired)) {
+		g_lastStatus = NEMO_INVALID_INPUT;
+		return NEMO_INVALID_INPUT;
+	}
+	g_lastStatus = S(s).stepNoAlloc(fstim, nf, inidx, icur, ni, fired, cap, nfired);
+	return g_lastStatus;
+}
+
 nemo_status_t nemo_apply_stdp(nemo_simulation_t s, float reward)
 {
 	NULLCHECK(s);

@@ -583,6 +583,118 @@ __global__ void stimulus_kernel(const DevSim S, const uint32_t* fidx, uint32_t n
 }
 
 // ---------------------------------------------------------------------------
+// nemo_step without allocation (nemo_b200_step_no_alloc)
+//
+// For callers that must not allocate (a real-time loop that steps every
+// millisecond, where a device allocation or free would synchronise the
+// device; an application with a fixed memory budget), the stimulus is
+// staged through fixed static buffers instead of the simulation's growable
+// staging buffers: g_stimStage on the host and g_noAllocStim on each device,
+// NEMO_B200_NO_ALLOC_STIMULUS_MAX words (256 KiB) each.  Nothing in them is
+// read before this call writes it, so nothing needs clearing.  The buffers
+// are shared by every simulation of the process: overlapping calls race.
+
+static __device__ __align__(256) uint32_t g_noAllocStim[NEMO_B200_NO_ALLOC_STIMULUS_MAX];
+
+namespace {
+constexpr int NO_ALLOC_MAX_DEVICES = 64;
+uint32_t* g_noAllocStimAddr[NO_ALLOC_MAX_DEVICES];  // device address of g_noAllocStim per device
+uint32_t g_stimStage[NEMO_B200_NO_ALLOC_STIMULUS_MAX];
+// current stimulus before deduplication: local index, value, order
+uint32_t g_curIdx[NEMO_B200_NO_ALLOC_STIMULUS_MAX / 2];
+float g_curVal[NEMO_B200_NO_ALLOC_STIMULUS_MAX / 2];
+uint32_t g_curOrder[NEMO_B200_NO_ALLOC_STIMULUS_MAX / 2];
+} // namespace
+
+bool Simulation::findLocal(unsigned g, unsigned* l) const
+{
+	auto it = m_g2l[0].find(g);
+	if(it == m_g2l[0].end()) return false;
+	*l = it->second;
+	return true;
+}
+
+nemo_status_t Simulation::stepNoAlloc(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur,
+		size_t ni, unsigned* fired, size_t cap, size_t* nfired) noexcept
+{
+	if(m_nets > 1) return NEMO_API_UNSUPPORTED;
+	if(nf > NEMO_B200_NO_ALLOC_STIMULUS_MAX || ni > NEMO_B200_NO_ALLOC_STIMULUS_MAX / 2
+			|| nf + 2 * ni > NEMO_B200_NO_ALLOC_STIMULUS_MAX) {
+		return NEMO_BUFFER_OVERFLOW;
+	}
+	if(cudaSetDevice(m_device) != cudaSuccess) return NEMO_CUDA_ERROR;
+	if(m_device < 0 || m_device >= NO_ALLOC_MAX_DEVICES) return NEMO_API_UNSUPPORTED;
+	uint32_t*& stim = g_noAllocStimAddr[m_device];
+	if(!stim) {
+		// once per device, with the device current
+		void* p = nullptr;
+		if(cudaGetSymbolAddress(&p, g_noAllocStim) != cudaSuccess || !p) return NEMO_CUDA_ERROR;
+		stim = static_cast<uint32_t*>(p);
+	}
+	// validate and map the stimulus before touching any state
+	// (src/nemo/cpu/Simulation.cpp:141-163)
+	for(size_t i = 0; i < nf; ++i) {
+		unsigned l;
+		if(!findLocal(fstim[i], &l)) return NEMO_INVALID_INPUT;
+		g_stimStage[i] = l;
+	}
+	for(size_t i = 0; i < ni; ++i) {
+		unsigned l;
+		if(!findLocal(inidx[i], &l)) return NEMO_INVALID_INPUT;
+		g_curIdx[i] = l;
+		g_curVal[i] = icur[i];
+		g_curOrder[i] = (uint32_t) i;
+	}
+	// the last current given for a neuron wins: order by (neuron, position)
+	// in place and keep the last of each neuron's run
+	std::sort(g_curOrder, g_curOrder + ni, [](uint32_t a, uint32_t b) {
+		return g_curIdx[a] != g_curIdx[b] ? g_curIdx[a] < g_curIdx[b] : a < b;
+	});
+	size_t nu = 0;
+	for(size_t k = 0; k < ni; ++k) {
+		if(k + 1 < ni && g_curIdx[g_curOrder[k + 1]] == g_curIdx[g_curOrder[k]]) continue;
+		g_curOrder[nu++] = g_curOrder[k];
+	}
+	for(size_t k = 0; k < nu; ++k) {
+		g_stimStage[nf + k] = g_curIdx[g_curOrder[k]];
+		memcpy(&g_stimStage[nf + nu + k], &g_curVal[g_curOrder[k]], 4);
+	}
+	const size_t words = nf + 2 * nu;
+	if(words) {
+		// the previous call's kernels read the device buffer: it finished
+		// before that call returned (it synchronised the stream)
+		if(cudaMemcpyAsync(stim, g_stimStage, words * 4, cudaMemcpyHostToDevice, m_stream) != cudaSuccess) {
+			return NEMO_CUDA_ERROR;
+		}
+		const uint32_t nmax = (uint32_t) std::max(nf, nu);
+		stimulus_kernel<<<(nmax + 255) / 256, 256, 0, m_stream>>>(m_dev, stim, (uint32_t) nf, stim + nf,
+				reinterpret_cast<const float*>(stim + nf + nu), (uint32_t) nu);
+	}
+	const uint32_t ring = (uint32_t) (m_cycle % m_dev.R);
+	launchStep(true);
+	if(cudaMemcpyAsync(m_hFired, m_dev.firedRing + (size_t) ring * m_dev.W, (size_t) m_dev.W * 4,
+			cudaMemcpyDeviceToHost, m_stream) != cudaSuccess) {
+		return NEMO_CUDA_ERROR;
+	}
+	if(cudaStreamSynchronize(m_stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) return NEMO_CUDA_ERROR;
+	// fired neurons in ascending local index, as global ids
+	// (setFiring, src/nemo/cpu/Simulation.cpp:200-208)
+	size_t count = 0;
+	for(uint32_t w = 0; w < m_dev.W; ++w) {
+		uint32_t bits = m_hFired[w];
+		while(bits) {
+			const uint32_t l = w * 32 + (uint32_t) __builtin_ctz(bits);
+			bits &= bits - 1;
+			if(count < cap) fired[count] = m_l2g[l];
+			++count;
+			stepEvents += m_outDegree[l];
+		}
+	}
+	*nfired = count;
+	return count > cap ? NEMO_BUFFER_OVERFLOW : NEMO_OK;
+}
+
+// ---------------------------------------------------------------------------
 // libm calibration tables on the device
 
 LibmCalib device_calibration(int device)

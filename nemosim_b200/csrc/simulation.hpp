@@ -114,6 +114,9 @@ public:
 	const std::vector<unsigned>& step(const unsigned* fstim, size_t nf,
 			const unsigned* inidx, const float* icur, size_t ni);
 	void applyStdp(float reward);
+	// step() that allocates nothing and throws nothing (nemo_b200_step_no_alloc)
+	nemo_status_t stepNoAlloc(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
+			unsigned* fired, size_t cap, size_t* nfired) noexcept;
 	void run(unsigned steps, unsigned stdpPeriod, float reward, unsigned* counts,
 			uint64_t* events, unsigned* ids, size_t cap, size_t* len);
 
@@ -176,6 +179,7 @@ private:
 	};
 
 	unsigned localIdx(unsigned g) const;
+	bool findLocal(unsigned g, unsigned* l) const;  // localIdx without throwing (one network)
 	void locate(unsigned g, const HostType** t, unsigned* i) const;
 	size_t synapseKey(uint64_t id) const;
 	void launchStep(bool fullRecord);
