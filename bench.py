@@ -53,6 +53,7 @@ DMAX = 44
 WINDOW_MS = 100
 METRIC = "synaptic events/s (100k x 1k Izhikevich, STDP)"
 UNIT = "events/s"
+BATCH_DMAX = 20  # delays 1-20 ms in the batched configuration
 
 # algorithmic bytes (per neuron-step, per fired neuron, per event, per STDP
 # entry) of the step kernel
@@ -389,6 +390,141 @@ def run_b200(args, rank, world, local):
         dist.destroy_process_group()
 
 
+def run_batch(args, local):
+    """The batched configuration: networks of uneven size, each with its own
+    generator seed and input-noise sigma, advanced together by one Batch,
+    against the same networks run one after another as plain Simulations
+    on the same GPU (device time of the runs; construction untimed).  Every
+    network's fire stream in the batch is compared with its own run."""
+    import nemosim_b200 as nb
+
+    rng = np.random.default_rng(args.batch_seed)
+    specs = [dict(n=int(rng.integers(args.batch_min_neurons, args.batch_max_neurons + 1)),
+                  f=int(rng.integers(args.batch_min_fanout, args.batch_max_fanout + 1)),
+                  seed=1000 + 17 * k, sigma=float(rng.uniform(2.0, 8.0)))
+             for k in range(args.batch_networks)]
+    conf = nb.Configuration()
+    conf.set_cuda_backend(local)
+    ms = args.batch_ms
+
+    def make(sp):
+        return nb.example_random(sp["n"], sp["f"], BATCH_DMAX, False, seed=sp["seed"],
+                                 sigma_exc=sp["sigma"], sigma_inh=sp["sigma"])
+
+    # one throwaway network first, so that no timed run pays one-time setup
+    warm = nb.Simulation(make(specs[0]), conf)
+    warm.run(ms, ids=False)
+    del warm
+
+    t0 = time.perf_counter()
+    nets, seq_ms, seq = [], 0.0, []
+    for sp in specs:
+        net = make(sp)
+        sim = nb.Simulation(net, conf)
+        c, _, ids = sim.run(ms, max_ids=sp["n"] * ms // 10)  # room for 100 Hz
+        seq_ms += sim.run_stats()["run_ms"]
+        seq.append((c, ids))
+        del sim
+        nets.append(net)
+    seq_wall = time.perf_counter() - t0
+
+    t0 = time.perf_counter()
+    batch = nb.Batch(nets, conf)
+    del nets
+    build_s = time.perf_counter() - t0
+    tuned_us = batch.autotune(20)
+    launch = batch.launch()
+    neurons = sum(sp["n"] for sp in specs)
+    with ClockSampler(local) as clk:
+        counts, events, ids = batch.run(ms, max_ids=neurons * ms // 10)
+    st = batch.run_stats()
+    batch_ms = st["run_ms"]
+    streams = batch.streams(counts, ids)
+    mismatched = sum(1 for (c1, i1), (c2, i2) in zip(streams, seq)
+                     if not (np.array_equal(c1, c2) and np.array_equal(i1, i2)))
+    # the same batch continued with two launches per step from CUDA graphs
+    batch.set_persistent(False)
+    batch.run(ms, ids=False)
+    graph_ms = batch.run_stats()["run_ms"]
+    synapses = sum(sp["n"] * sp["f"] for sp in specs)
+    line = {
+        "metric": "batched speedup vs sequential plain runs", "value": seq_ms / batch_ms, "unit": "x",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "fp32+f64+int64", "data": "synthetic",
+        "config": {"workload": f"batch-{args.batch_networks}-izhikevich", "networks": args.batch_networks,
+                   "neurons": [args.batch_min_neurons, args.batch_max_neurons],
+                   "fanout": [args.batch_min_fanout, args.batch_max_fanout], "max_delay_ms": BATCH_DMAX,
+                   "sigma": [2.0, 8.0], "ms": ms, "total_neurons": neurons, "total_synapses": synapses,
+                   "generator": "random::construct (src/examples/random.cpp) per network, own seed and sigma"},
+        "batch_ms": batch_ms, "sequential_ms": seq_ms, "sequential_wall_s": seq_wall,
+        "batch_two_launch_graphs_ms": graph_ms, "speedup_two_launch_graphs": seq_ms / graph_ms,
+        "batch_events_per_s": st["events"] / (batch_ms / 1e3),
+        "bitexact_vs_individual_runs": mismatched == 0, "mismatched_networks": mismatched,
+        "launch": {"partition": launch[0], "threads": launch[1], "autotuned_us_per_step": tuned_us},
+        "batch_build_s": build_s, "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_bptt(args, local):
+    """The differentiable configuration at full size: one gradient step
+    (forward + hand-written adjoint) against PyTorch float32 autograd of
+    the same unrolled dynamics on the same GPU (the baseline leg)."""
+    import torch
+    from nemosim_b200.bptt import DifferentiableNetwork
+    from oracle import bptt_torch as baseline
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    N, F, T, B, R, CK = 4096, 200, 500, 16, 256, 50
+    net = DifferentiableNetwork.random(N, F, max_delay=10, seed=1)
+    teacher = DifferentiableNetwork.random(N, F, max_delay=10, seed=101)
+    g = torch.Generator(device="cpu").manual_seed(1)
+    noise = (5.0 * torch.randn((T, B, N), generator=g)).to(dev)
+    Wt, at, bt = teacher.tensors(dev, requires_grad=False)
+    target = teacher.model(B, T, R, CK).readout_trains(Wt, at, bt, noise)
+
+    def ours(dtype, reps):
+        m = net.model(B, T, R, CK, False, state_dtype=dtype)
+        W, a, b = net.tensors(dev)
+        for _ in range(args.warmup):
+            W.grad = a.grad = b.grad = None
+            m.loss(W, a, b, noise, target).backward()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record()
+        for _ in range(reps):
+            W.grad = a.grad = b.grad = None
+            m.loss(W, a, b, noise, target).backward()
+        end.record()
+        torch.cuda.synchronize()
+        return start.elapsed_time(end) / reps
+
+    with ClockSampler(local) as clk:
+        ms32 = ours(torch.float32, args.steps)
+        ms64 = ours(torch.float64, args.steps)
+    W, a, b = net.tensors(dev)
+    c, d = net.constants(dev)
+    st = baseline.Structure(net.source, net.target, net.delay, N, dev)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    baseline.loss(W, a, b, c, d, noise, target, st, R, False).backward()
+    end.record()
+    torch.cuda.synchronize()
+    torch_ms = start.elapsed_time(end)
+    line = {
+        "metric": "BPTT gradient step speedup vs PyTorch autograd (same GPU)", "value": torch_ms / ms32,
+        "unit": "x", "n_gpus": 1, "higher_is_better": True, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": "bptt-izhikevich-4096x200", "neurons": N, "synapses_per_neuron": F,
+                   "ms": T, "substeps": 4 * T, "trials": B, "readout": R, "checkpoint_ms": CK,
+                   "delays_ms": [1, 10], "noise_sigma": 5.0},
+        "adjoint_ms": ms32, "adjoint_fp64_state_ms": ms64, "torch_autograd_ms": torch_ms,
+        "speedup_fp64_state": torch_ms / ms64, "steps": args.steps, "warmup": args.warmup,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -404,6 +540,16 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--no-persistent", action="store_true")
+    ap.add_argument("--workload", choices=["headline", "batch256", "bptt"], default="headline",
+                    help="headline: the 100k x 1k STDP network (default); batch256: batched networks "
+                         "against sequential runs; bptt: differentiable mode against PyTorch autograd")
+    ap.add_argument("--batch-networks", type=int, default=256)
+    ap.add_argument("--batch-min-neurons", type=int, default=1000)
+    ap.add_argument("--batch-max-neurons", type=int, default=32000)
+    ap.add_argument("--batch-min-fanout", type=int, default=100)
+    ap.add_argument("--batch-max-fanout", type=int, default=1000)
+    ap.add_argument("--batch-ms", type=int, default=1000)
+    ap.add_argument("--batch-seed", type=int, default=0)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
@@ -412,6 +558,12 @@ def main():
         rank = int(os.environ.get("RANK", 0))
         args.gpus = int(os.environ.get("WORLD_SIZE", args.gpus))
         run_reference(args, rank, 1)
+        return
+    if args.workload != "headline":
+        local = int(os.environ.get("LOCAL_RANK", 0))
+        if int(os.environ.get("RANK", 0)) != 0:
+            return  # these comparisons run on one GPU
+        (run_batch if args.workload == "batch256" else run_bptt)(args, local)
         return
     rank, world, local = dist_setup(args)
     args.gpus = world if world > 1 else args.gpus

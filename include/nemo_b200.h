@@ -278,8 +278,11 @@ NEMO_B200_API nemo_status_t nemo_b200_set_profiling(nemo_simulation_t, int on);
 NEMO_B200_API nemo_status_t nemo_b200_set_graphs(nemo_simulation_t, int on);
 /* Choose how nemo_b200_run advances the steps between applyStdp calls: one
  * persistent cooperative launch per segment, its update and delivery phases
- * separated by grid barriers (on, the default), or two launches per step
- * (off).  nemo_step always uses two launches.  Results are identical. */
+ * separated by grid barriers (on), or two launches per step (off).  The
+ * default is on, except for networks with more than two neurons per thread
+ * of the persistent loop's co-resident CTAs (large batches), where one
+ * launch per phase over the whole network is faster.  nemo_step always uses
+ * two launches.  Results are identical. */
 NEMO_B200_API nemo_status_t nemo_b200_set_persistent(nemo_simulation_t, int on);
 /* Statistics of the last nemo_b200_run: its device time in ms (CUDA events
  * on the simulation's stream), and per kernel kind (0 = update kernel and

@@ -115,6 +115,27 @@ __device__ __forceinline__ void reserve_groups(unsigned long long* counter, uint
 	e = (uint32_t) base + ie - ne;
 }
 
+// reserve_groups on two lists, both atomics in flight together
+__device__ __forceinline__ void reserve_groups2(unsigned long long* c1, uint32_t ng1, uint32_t ne1, uint32_t& g1,
+		uint32_t& e1, unsigned long long* c2, uint32_t ng2, uint32_t ne2, uint32_t& g2, uint32_t& e2)
+{
+	const uint32_t ig1 = warp_inclusive_scan(ng1), ie1 = warp_inclusive_scan(ne1);
+	const uint32_t ig2 = warp_inclusive_scan(ng2), ie2 = warp_inclusive_scan(ne2);
+	const uint32_t tg1 = __shfl_sync(0xffffffffu, ig1, 31), te1 = __shfl_sync(0xffffffffu, ie1, 31);
+	const uint32_t tg2 = __shfl_sync(0xffffffffu, ig2, 31), te2 = __shfl_sync(0xffffffffu, ie2, 31);
+	unsigned long long b1 = 0, b2 = 0;
+	if((threadIdx.x & 31) == 31) {
+		if(tg1 | te1) b1 = atomicAdd(c1, ((unsigned long long) tg1 << 32) | te1);
+		if(tg2 | te2) b2 = atomicAdd(c2, ((unsigned long long) tg2 << 32) | te2);
+	}
+	b1 = __shfl_sync(0xffffffffu, b1, 31);
+	b2 = __shfl_sync(0xffffffffu, b2, 31);
+	g1 = (uint32_t) (b1 >> 32) + ig1 - ng1;
+	e1 = (uint32_t) b1 + ie1 - ne1;
+	g2 = (uint32_t) (b2 >> 32) + ig2 - ng2;
+	e2 = (uint32_t) b2 + ie2 - ne2;
+}
+
 // group g = entries [e, e + len) = [start, start + len) of the list's array
 __device__ __forceinline__ void write_group(const WorkList& L, uint32_t g, uint32_t e, unsigned long long start,
 		uint32_t len)
@@ -157,6 +178,8 @@ __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, ui
 		uint32_t fw = 0, outdeg = 0, indeg = 0;
 		unsigned long long ob = 0, rb = 0;
 		uint64_t pend = 0;
+		bool hist_nonzero = false;
+		uint32_t g1End = 0, gpD = 0, gpBeg = 0, gpEnd = 0;
 		if(n < last) {
 			uint32_t k = 0;
 			while(k + 1 < S.ntypes && n >= S.types[k + 1].base) ++k;
@@ -178,6 +201,16 @@ __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, ui
 			}
 			NeuronRegs R;
 			load_neuron(S, T, nl, n, R);
+			// the delay-group ends this neuron will most likely publish, loaded
+			// before the arithmetic: its delay-1 group (if it fires now) and
+			// the first group pending from its earlier spikes
+			const uint64_t pendPrev = (hp << 1) & dm;
+			if(dm & 1ull) g1End = delay_end(S, n, 1);
+			if(pendPrev) {
+				gpD = (uint32_t) __ffsll((long long) pendPrev);
+				gpBeg = delay_end(S, n, gpD - 1);
+				gpEnd = delay_end(S, n, gpD);
+			}
 
 			if(acc.x | acc.y) S.slot[n] = make_ulonglong2(0, 0);
 			if(__float_as_uint(ext) != 0u) S.curExt[n] = 0.0f;
@@ -189,6 +222,7 @@ __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, ui
 			store_neuron(S, T, nl, n, R);
 			const uint64_t h = (hp << 1) | (uint64_t) fired;
 			histCur[n] = h;
+			hist_nonzero = h != 0;
 			ob = o0;
 			if(fired) outdeg = (uint32_t) (o1 - o0);
 			// groups arriving next step: delay d of a source that fired d - 1
@@ -203,32 +237,38 @@ __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, ui
 			}
 		}
 		const uint32_t fb = __ballot_sync(0xffffffffu, fired);
+		const uint32_t rbits = __ballot_sync(0xffffffffu, hist_nonzero);
 		if(lane == 0 && n < last) {
 			S.firedRing[(size_t) ring * S.W + (n >> 5)] = fb;
+			S.recent[(size_t) cur * S.recentWords + (n >> 5)] = rbits;
 			if(fw) S.fstim[n >> 5] = 0u;
 		}
-		// the delay groups that arrive next step
-		if(__any_sync(0xffffffffu, pend != 0)) {
-			uint32_t ng = 0, ne = 0;
-			for(uint64_t b = pend; b; b &= b - 1) {
-				const uint32_t d = (uint32_t) __ffsll((long long) b);
-				ne += delay_end(S, n, d) - delay_end(S, n, d - 1);
-				++ng;
-			}
-			uint32_t g, e;
-			reserve_groups(&S.dlvWork.count[cur], ng, ne, g, e);
-			for(uint64_t b = pend; b; b &= b - 1) {
-				const uint32_t d = (uint32_t) __ffsll((long long) b);
-				const uint32_t e0 = delay_end(S, n, d - 1), len = delay_end(S, n, d) - e0;
-				write_group(S.dlvWork, g++, e, ob + e0, len);
-				e += len;
-			}
+		// the delay groups that arrive next step and the incoming plastic
+		// synapses of this step's STDP targets, both reserved at once
+		// range [e0, e1) of this neuron's delay-d group in its row
+		auto group = [&](uint32_t d, uint32_t& e0, uint32_t& e1) {
+			if(d == 1) { e0 = 0; e1 = g1End; }
+			else if(d == gpD) { e0 = gpBeg; e1 = gpEnd; }
+			else { e0 = delay_end(S, n, d - 1); e1 = delay_end(S, n, d); }
+		};
+		uint32_t ngD = 0, neD = 0;
+		for(uint64_t b = pend; b; b &= b - 1) {
+			uint32_t e0, e1;
+			group((uint32_t) __ffsll((long long) b), e0, e1);
+			neD += e1 - e0;
+			++ngD;
 		}
-		// the incoming plastic synapses of this step's STDP targets
-		if(__any_sync(0xffffffffu, target)) {
-			uint32_t g, e;
-			reserve_groups(&S.stdpWork.count[cur], target ? 1u : 0u, target ? indeg : 0u, g, e);
-			if(target) write_group(S.stdpWork, g, e, rb, indeg);
+		const uint32_t ngS = target ? 1u : 0u, neS = target ? indeg : 0u;
+		if(__any_sync(0xffffffffu, (ngD | ngS) != 0)) {
+			uint32_t gD, eD, gS, eS;
+			reserve_groups2(&S.dlvWork.count[cur], ngD, neD, gD, eD, &S.stdpWork.count[cur], ngS, neS, gS, eS);
+			for(uint64_t b = pend; b; b &= b - 1) {
+				uint32_t e0, e1;
+				group((uint32_t) __ffsll((long long) b), e0, e1);
+				write_group(S.dlvWork, gD++, eD, ob + e0, e1 - e0);
+				eD += e1 - e0;
+			}
+			if(target) write_group(S.stdpWork, gS, eS, rb, indeg);
 		}
 		// targets touched in this STDP period, for applyStdp
 		const uint32_t tb = __ballot_sync(0xffffffffu, target);
@@ -296,7 +336,7 @@ __device__ __forceinline__ void red_add_u64(unsigned long long* p, unsigned long
 //          step that published the list
 template<int KIND, int K>
 __device__ __forceinline__ void process_list(const DevSim& S, const WorkList& L, uint32_t ng, uint32_t ne,
-		const uint64_t* hist, uint32_t warp, uint32_t nwarps)
+		const uint64_t* hist, const uint32_t* recent, uint32_t warp, uint32_t nwarps)
 {
 	if(ne == 0) return;
 	const uint32_t lane = threadIdx.x & 31;
@@ -351,7 +391,12 @@ __device__ __forceinline__ void process_list(const DevSim& S, const WorkList& L,
 					}
 				}
 #pragma unroll
-				for(int j = 0; j < K; ++j) if(base + lane + 32 * j < hi) h[j] = hist[sd[j] & (MAX_NEURONS - 1)];
+				for(int j = 0; j < K; ++j) {
+					// a source that fired in none of the last 64 steps has history 0
+					const uint32_t src = sd[j] & (MAX_NEURONS - 1);
+					h[j] = 0;
+					if(base + lane + 32 * j < hi && (!recent || ((recent[src >> 5] >> (src & 31)) & 1u))) h[j] = hist[src];
+				}
 #pragma unroll
 				for(int j = 0; j < K; ++j) {
 					if(base + lane + 32 * j < hi) {
@@ -385,8 +430,25 @@ __device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uin
 		S.stdpWork.count[pub ^ 1u] = 0;
 	}
 	const uint64_t* hist = S.hist + (size_t) pub * S.N;
-	process_list<0, 8>(S, S.dlvWork, (uint32_t) (cd >> 32), (uint32_t) cd, hist, warp, nwarps);
-	process_list<1, 4>(S, S.stdpWork, (uint32_t) (cs >> 32), (uint32_t) cs, hist, warp, nwarps);
+	// the sources' "fired in the last 64 steps" bits, copied to shared
+	// memory with asynchronous 16-byte copies that overlap the deliveries
+	// (every thread of the CTA calls this function)
+	extern __shared__ __align__(16) uint32_t sRecent[];
+	const bool filter = S.recentBytes && (uint32_t) cs;
+	if(filter) {
+		const uint32_t* g = S.recent + (size_t) pub * S.recentWords;
+		for(uint32_t q = threadIdx.x; q < S.recentWords / 4; q += blockDim.x) {
+			const uint32_t dst = (uint32_t) __cvta_generic_to_shared(sRecent + 4 * q);
+			asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(g + 4 * q) : "memory");
+		}
+		asm volatile("cp.async.commit_group;" ::: "memory");
+	}
+	process_list<0, 8>(S, S.dlvWork, (uint32_t) (cd >> 32), (uint32_t) cd, hist, nullptr, warp, nwarps);
+	if(filter) asm volatile("cp.async.wait_all;" ::: "memory");
+	__syncthreads();
+	process_list<1, 4>(S, S.stdpWork, (uint32_t) (cs >> 32), (uint32_t) cs, hist, filter ? sRecent : nullptr, warp,
+			nwarps);
+	__syncthreads();  // the shared copy is rewritten by the next call
 }
 
 // Pre-phase of step t (pub = (t - 1) & 1), or with what = PHASE_STDP the
@@ -1133,6 +1195,9 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	}
 
 	S.hist = dalloc<uint64_t>(2 * (size_t) N);
+	S.recentWords = (S.W + 3) & ~3u;  // 16-byte rows for the asynchronous copy
+	S.recent = dalloc<uint32_t>(2 * (size_t) S.recentWords);
+	S.recentBytes = (S.stdp && (size_t) S.recentWords * 4 <= RECENT_FILTER_MAX_BYTES) ? S.recentWords * 4 : 0u;
 	S.fstim = dalloc<uint32_t>(S.W);
 	S.touchedBits = dalloc<uint32_t>(S.W);
 	S.curExt = dalloc<float>(N);
@@ -1168,6 +1233,10 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 			NB_CUDA(cudaMallocHost(&m_hBarrierError, 4));
 			*m_hBarrierError = 0;
 		}
+		// the persistent loop's CTAs are those that fit at once; when each
+		// thread would update more than two neurons in turn, the update is
+		// faster as one launch over the whole network (a large batch)
+		if((uint64_t) N > 2ull * m_runGrid * m_runT) usePersistent = false;
 	}
 	NB_CUDA(cudaStreamSynchronize(m_stream));
 	resetTimer();
@@ -1232,7 +1301,7 @@ void Simulation::timedEnd()
 unsigned Simulation::runGridFor(uint32_t T) const
 {
 	int perSm = 0;
-	NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, run_kernel, (int) T, 0));
+	NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, run_kernel, (int) T, m_dev.recentBytes));
 	return perSm > 0 ? (unsigned) perSm * (unsigned) m_sms : 0u;
 }
 
@@ -1263,7 +1332,7 @@ void Simulation::launchStep(bool /*fullRecord*/)
 	const uint32_t ring = (uint32_t) (m_cycle % m_dev.R);
 	const unsigned grid = (m_N + m_P - 1) / m_P;
 	timedBegin(K_STDP);
-	deliver_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, cur ^ 1u,
+	deliver_kernel<<<m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream>>>(m_dev, cur ^ 1u,
 			PHASE_DELIVER | PHASE_STDP | PHASE_RESET, 0, 0);
 	timedEnd();
 	timedBegin(K_STEP);
@@ -1283,7 +1352,7 @@ void Simulation::flushStdp()
 	if(!m_dev.stdp || m_cycle == 0) return;
 	const uint32_t last = (uint32_t) ((m_cycle - 1) & 1);
 	timedBegin(K_STDP);
-	deliver_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, last, PHASE_STDP, 0, 0);
+	deliver_kernel<<<m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream>>>(m_dev, last, PHASE_STDP, 0, 0);
 	timedEnd();
 	NB_CUDA(cudaMemsetAsync(m_dev.stdpWork.count + last, 0, 8, m_stream));
 }
@@ -1301,7 +1370,8 @@ void Simulation::launchRun(unsigned n)
 	// delivery phase, which the other CTAs' warps cover as well)
 	const unsigned grid = (unsigned) std::min<uint64_t>(m_runGrid, std::max<uint64_t>(1, (m_N + P - 1) / P));
 	timedBegin(K_RUN);
-	NB_CUDA(cudaLaunchCooperativeKernel((const void*) run_kernel, dim3(grid), dim3(m_runT), args, 0, m_stream));
+	NB_CUDA(cudaLaunchCooperativeKernel((const void*) run_kernel, dim3(grid), dim3(m_runT), args, m_dev.recentBytes,
+			m_stream));
 	timedEnd();
 	m_cycle += n;
 	m_timerSteps += n;
@@ -1359,7 +1429,7 @@ void Simulation::buildGraph()
 	cudaGraph_t g;
 	NB_CUDA(cudaStreamBeginCapture(m_stream, cudaStreamCaptureModeThreadLocal));
 	for(unsigned k = 0; k < GRAPH_STEPS; ++k) {
-		deliver_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, 0,
+		deliver_kernel<<<m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream>>>(m_dev, 0,
 				PHASE_DELIVER | PHASE_STDP | PHASE_RESET, k, 1);
 		update_kernel<<<grid, m_T, 0, m_stream>>>(m_dev, m_P, 0, 0, k, 1);
 	}
@@ -1611,6 +1681,7 @@ float Simulation::autotune(unsigned trialSteps)
 	for(const HostType& t : m_types) regions.emplace_back(t.dState, (size_t) t.n * t.desc->nstate * 4);
 	regions.emplace_back(m_dev.rng, (size_t) 4 * m_N * 4);
 	regions.emplace_back(m_dev.hist, (size_t) 2 * m_N * 8);
+	regions.emplace_back(m_dev.recent, (size_t) 2 * m_dev.recentWords * 4);
 	regions.emplace_back(m_dev.fstim, (size_t) m_dev.W * 4);
 	regions.emplace_back(m_dev.curExt, (size_t) m_N * 4);
 	regions.emplace_back(m_dev.slot, (size_t) m_N * 16);

@@ -28,6 +28,11 @@ struct GridBarrier {
 	uint32_t pad[2];
 };
 
+// STDP accumulation first tests a source against a shared-memory copy of the
+// "fired in the last 64 steps" bit-vector (W words), when it fits in this
+// many bytes; else it reads every source's history.
+constexpr unsigned RECENT_FILTER_MAX_BYTES = 48 * 1024;
+
 struct TypeRange {
 	int kind;
 	uint32_t base, n;
@@ -67,6 +72,9 @@ struct DevSim {
 	TypeRange types[MAX_TYPES];
 	uint32_t* rng;            // [4][N] xorshift words
 	uint64_t* hist;           // [2][N] firing history, double-buffered by step parity
+	uint32_t* recent;         // [2][recentWords] bit-vectors: history nonzero (fired in the last 64 steps), by parity
+	uint32_t recentWords;     // W rounded up to a multiple of 4
+	uint32_t recentBytes;     // bytes of shared memory for the copy of one recent bit-vector (0 = none)
 	uint32_t* fstim;          // [W] pending firing stimulus
 	float* curExt;            // [N] pending current stimulus
 	ulonglong2* slot;         // [N] int64 E and I fixed-point sums (two's complement) of this step's arrivals
@@ -153,7 +161,9 @@ public:
 	bool profiling = false;
 	bool useGraphs = true;  // replay the two-launch step loop from CUDA graphs in run()
 	// run() advances its step loop with one persistent cooperative launch per
-	// segment between applyStdp calls (else with the two-launch step)
+	// segment between applyStdp calls (else with the two-launch step); on by
+	// default unless the network has more than two neurons per thread of the
+	// persistent loop's co-resident CTAs
 	bool usePersistent = true;
 
 	// launch shape of the active step loop (persistent or two-launch):

@@ -280,6 +280,15 @@ def test_dynamic_window_length(stdp):
         nb.Simulation(net, conf).step()
 
 
+def test_literal_c2_delays_are_rejected():
+    """The benchmark network with its literal 1-64 ms delays and the 20 ms
+    post-fire window: max delay + |post| > 64 is rejected at creation
+    (src/nemo/StdpFunction.cpp:51-60); 44 is the largest accepted."""
+    with pytest.raises(nb.NemoError):
+        nb.Simulation(nb.example_random(1000, 50, 64, True), nets.standard_stdp(nb))
+    nb.Simulation(nb.example_random(1000, 50, 44, True), nets.standard_stdp(nb)).step()
+
+
 def test_invalid_target_fails():
     net = nb.Network()
     iz = net.add_neuron_type("Izhikevich")
