@@ -172,24 +172,31 @@ def dist_setup(args):
     return rank, world, local
 
 
-def dist_max(x: float, world: int) -> float:
+def _reduce(x: float, world: int, op: str) -> float:
+    """All-reduce one number over the ranks (NCCL on the GPUs; gloo on CPU)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=getattr(dist.ReduceOp, op))
     return float(t.item())
+
+
+def dist_max(x: float, world: int) -> float:
+    return _reduce(x, world, "MAX")
 
 
 def dist_sum(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(x, world, "SUM")
+
+
+def replica_throughput(events: float, run_ms: float, world: int) -> tuple:
+    """Whole-job events/s of N independent replicas: all ranks' events over
+    the slowest rank's device time.  Returns (events/s, max ms)."""
+    ms = dist_max(run_ms, world)
+    return dist_sum(events, world) / (ms / 1e3), ms
 
 
 def barrier(world: int):
@@ -283,9 +290,7 @@ def run_b200(args, rank, world, local):
         sim.run(W * args.steps, W, 1.0, ids=False)
     st = sim.run_stats()
     barrier(world)
-    run_ms = dist_max(st["run_ms"], world)
-    events = dist_sum(float(st["events"]), world)
-    value = events / (run_ms / 1e3)
+    value, run_ms = replica_throughput(float(st["events"]), st["run_ms"], world)
     sim_ms_per_s = args.steps * W / (run_ms / 1e3)
 
     # profiled pass: per-kernel CUDA events for the roofline

@@ -66,6 +66,8 @@ struct NeuronRegs {
 	float p[9];     // parameters
 	float x[4];     // state
 	uint32_t r[4];  // xorshift words
+	float noise;    // this step's nrand, when precomputed (pre)
+	bool pre;
 };
 
 __device__ __forceinline__ void load_rng(const DevSim& S, uint32_t n, NeuronRegs& R)
@@ -86,18 +88,23 @@ __device__ __forceinline__ void store_rng(const DevSim& S, uint32_t n, const Neu
 
 // parameters and state of neuron nl of type T (the plugin layouts of
 // src/nemo/plugins/Izhikevich.h, IF_curr_exp.h, PoissonSource.h)
-__device__ __forceinline__ void load_neuron(const DevSim& S, const TypeRange& T, uint32_t nl, uint32_t n, NeuronRegs& R)
+// With pre, an Izhikevich neuron's nrand for this step was computed (and its
+// RNG words advanced) by precompute_noise at the end of the previous step.
+__device__ __forceinline__ void load_neuron(const DevSim& S, const TypeRange& T, uint32_t nl, uint32_t n, NeuronRegs& R,
+		bool pre)
 {
 	const float* P = T.param;
 	const float* X = T.state;
 	const uint32_t nn = T.n;
+	R.pre = pre;
 	switch(T.kind) {
 		case KIND_IZHIKEVICH:
 #pragma unroll
 			for(int k = 0; k < 5; ++k) R.p[k] = P[k * nn + nl];  // a, b, c, d, sigma
 			R.x[0] = X[nl];       // u
 			R.x[1] = X[nn + nl];  // v
-			load_rng(S, n, R);
+			if(pre) R.noise = S.noise[n];
+			else load_rng(S, n, R);
 			break;
 		case KIND_IF_CURR_EXP:
 #pragma unroll
@@ -122,7 +129,10 @@ __device__ __forceinline__ bool update_izhikevich(const LibmCalib& calib, Neuron
 {
 	const float a = R.p[0], b = R.p[1], sigma = R.p[4];
 	float I = __fadd_rn(__fadd_rn(cE, cI), ext);
-	if(sigma != 0.0f) I = __fadd_rn(I, __fmul_rn(sigma, nb_nrand(calib, R.r[0], R.r[1], R.r[2], R.r[3])));
+	if(sigma != 0.0f) {
+		const float z = R.pre ? R.noise : nb_nrand(calib, R.r[0], R.r[1], R.r[2], R.r[3]);
+		I = __fadd_rn(I, __fmul_rn(sigma, z));
+	}
 	float u = R.x[0], v = R.x[1];
 	const double dI = (double) I;
 	bool fired = false;
@@ -208,7 +218,7 @@ __device__ __forceinline__ void store_neuron(const DevSim& S, const TypeRange& T
 		case KIND_IZHIKEVICH:
 			X[nl] = R.x[0];
 			X[nn + nl] = R.x[1];
-			if(R.p[4] != 0.0f) store_rng(S, n, R);
+			if(R.p[4] != 0.0f && !R.pre) store_rng(S, n, R);
 			break;
 		case KIND_IF_CURR_EXP:
 #pragma unroll
@@ -219,6 +229,25 @@ __device__ __forceinline__ void store_neuron(const DevSim& S, const TypeRange& T
 			break;
 		default:
 			break;
+	}
+}
+
+// nrand of the next step for the Izhikevich neurons [first, last) of a CTA
+// with sigma != 0 (the same draws the update would make, in the same order),
+// for the update's pre flag.
+__device__ __forceinline__ void precompute_noise(const DevSim& S, uint32_t first, uint32_t last)
+{
+	for(uint32_t n = first + threadIdx.x; n < last; n += blockDim.x) {
+		uint32_t k = 0;
+		while(k + 1 < S.ntypes && n >= S.types[k + 1].base) ++k;
+		const TypeRange& T = S.types[k];
+		if(T.kind != KIND_IZHIKEVICH) continue;
+		const uint32_t nl = n - T.base;
+		if(T.param[4 * T.n + nl] == 0.0f) continue;
+		NeuronRegs R;
+		load_rng(S, n, R);
+		S.noise[n] = nb_nrand(S.calib, R.r[0], R.r[1], R.r[2], R.r[3]);
+		store_rng(S, n, R);
 	}
 }
 

@@ -101,41 +101,6 @@ __device__ __forceinline__ void write_chunks(uint4* list, uint32_t pos, unsigned
 
 constexpr uint32_t BUCKET = 32;  // entries per bucket of a work list
 
-// Reserve ng groups and ne entries per lane in a work list (one atomic per
-// warp); returns this lane's first group and first entry.
-__device__ __forceinline__ void reserve_groups(unsigned long long* counter, uint32_t ng, uint32_t ne, uint32_t& g,
-		uint32_t& e)
-{
-	const uint32_t ig = warp_inclusive_scan(ng), ie = warp_inclusive_scan(ne);
-	const uint32_t tg = __shfl_sync(0xffffffffu, ig, 31), te = __shfl_sync(0xffffffffu, ie, 31);
-	unsigned long long base = 0;
-	if((tg | te) && (threadIdx.x & 31) == 31) base = atomicAdd(counter, ((unsigned long long) tg << 32) | te);
-	base = __shfl_sync(0xffffffffu, base, 31);
-	g = (uint32_t) (base >> 32) + ig - ng;
-	e = (uint32_t) base + ie - ne;
-}
-
-// reserve_groups on two lists, both atomics in flight together
-__device__ __forceinline__ void reserve_groups2(unsigned long long* c1, uint32_t ng1, uint32_t ne1, uint32_t& g1,
-		uint32_t& e1, unsigned long long* c2, uint32_t ng2, uint32_t ne2, uint32_t& g2, uint32_t& e2)
-{
-	const uint32_t ig1 = warp_inclusive_scan(ng1), ie1 = warp_inclusive_scan(ne1);
-	const uint32_t ig2 = warp_inclusive_scan(ng2), ie2 = warp_inclusive_scan(ne2);
-	const uint32_t tg1 = __shfl_sync(0xffffffffu, ig1, 31), te1 = __shfl_sync(0xffffffffu, ie1, 31);
-	const uint32_t tg2 = __shfl_sync(0xffffffffu, ig2, 31), te2 = __shfl_sync(0xffffffffu, ie2, 31);
-	unsigned long long b1 = 0, b2 = 0;
-	if((threadIdx.x & 31) == 31) {
-		if(tg1 | te1) b1 = atomicAdd(c1, ((unsigned long long) tg1 << 32) | te1);
-		if(tg2 | te2) b2 = atomicAdd(c2, ((unsigned long long) tg2 << 32) | te2);
-	}
-	b1 = __shfl_sync(0xffffffffu, b1, 31);
-	b2 = __shfl_sync(0xffffffffu, b2, 31);
-	g1 = (uint32_t) (b1 >> 32) + ig1 - ng1;
-	e1 = (uint32_t) b1 + ie1 - ne1;
-	g2 = (uint32_t) (b2 >> 32) + ig2 - ng2;
-	e2 = (uint32_t) b2 + ie2 - ne2;
-}
-
 // group g = entries [e, e + len) = [start, start + len) of the list's array
 __device__ __forceinline__ void write_group(const WorkList& L, uint32_t g, uint32_t e, unsigned long long start,
 		uint32_t len)
@@ -154,10 +119,12 @@ __device__ __forceinline__ uint32_t delay_end(const DevSim& S, uint32_t n, uint3
 }
 
 // CTA-level counters of one step, added to the per-step ring counters once
-// per CTA
+// per CTA, and the CTA's work-list reservations (groups << 32 | entries)
 struct CtaCounters {
 	uint32_t fired;
 	unsigned long long events, stdp;
+	unsigned long long resD, resS;    // the warps' reservations, summed
+	unsigned long long baseD, baseS;  // the CTA's place in the delivery / STDP lists
 };
 
 // Neuron update of step t (src/nemo/cpu/Simulation.cpp:94-111 minus the
@@ -166,7 +133,7 @@ struct CtaCounters {
 // blockDim.x threads loop over them.  Every thread of the CTA calls it.
 // cur = t & 1.
 __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, uint32_t last, uint32_t cur,
-		uint32_t ring, CtaCounters& C)
+		uint32_t ring, CtaCounters& C, bool preNoise = false)
 {
 	const uint32_t tid = threadIdx.x, lane = tid & 31;
 	const uint64_t* histPrev = S.hist + (size_t) (cur ^ 1u) * S.N;
@@ -200,7 +167,7 @@ __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, ui
 				r1 = S.rcmPtr[n + 1];
 			}
 			NeuronRegs R;
-			load_neuron(S, T, nl, n, R);
+			load_neuron(S, T, nl, n, R, preNoise);
 			// the delay-group ends this neuron will most likely publish, loaded
 			// before the arithmetic: its delay-1 group (if it fires now) and
 			// the first group pending from its earlier spikes
@@ -259,16 +226,39 @@ __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, ui
 			++ngD;
 		}
 		const uint32_t ngS = target ? 1u : 0u, neS = target ? indeg : 0u;
-		if(__any_sync(0xffffffffu, (ngD | ngS) != 0)) {
-			uint32_t gD, eD, gS, eS;
-			reserve_groups2(&S.dlvWork.count[cur], ngD, neD, gD, eD, &S.stdpWork.count[cur], ngS, neS, gS, eS);
+		// reserve both lists for the whole CTA: warps add their totals to
+		// shared counters, one thread reserves the CTA's share of each
+		// global list (so that warps do not queue on two global addresses)
+		const uint32_t igD = warp_inclusive_scan(ngD), ieD = warp_inclusive_scan(neD);
+		const uint32_t igS = warp_inclusive_scan(ngS), ieS = warp_inclusive_scan(neS);
+		unsigned long long wD = 0, wS = 0;
+		if(lane == 31) {
+			if(igD | ieD) wD = atomicAdd(&C.resD, ((unsigned long long) igD << 32) | ieD);
+			if(igS | ieS) wS = atomicAdd(&C.resS, ((unsigned long long) igS << 32) | ieS);
+		}
+		__syncthreads();
+		if(tid == 0) {
+			C.baseD = C.resD ? atomicAdd(&S.dlvWork.count[cur], C.resD) : 0ull;
+			C.baseS = C.resS ? atomicAdd(&S.stdpWork.count[cur], C.resS) : 0ull;
+			C.resD = 0;
+			C.resS = 0;
+		}
+		__syncthreads();
+		wD = __shfl_sync(0xffffffffu, wD, 31);
+		wS = __shfl_sync(0xffffffffu, wS, 31);
+		if(ngD) {
+			uint32_t gD = (uint32_t) (C.baseD >> 32) + (uint32_t) (wD >> 32) + igD - ngD;
+			uint32_t eD = (uint32_t) C.baseD + (uint32_t) wD + ieD - neD;
 			for(uint64_t b = pend; b; b &= b - 1) {
 				uint32_t e0, e1;
 				group((uint32_t) __ffsll((long long) b), e0, e1);
 				write_group(S.dlvWork, gD++, eD, ob + e0, e1 - e0);
 				eD += e1 - e0;
 			}
-			if(target) write_group(S.stdpWork, gS, eS, rb, indeg);
+		}
+		if(ngS) {
+			write_group(S.stdpWork, (uint32_t) (C.baseS >> 32) + (uint32_t) (wS >> 32) + igS - ngS,
+					(uint32_t) C.baseS + (uint32_t) wS + ieS - neS, rb, indeg);
 		}
 		// targets touched in this STDP period, for applyStdp
 		const uint32_t tb = __ballot_sync(0xffffffffu, target);
@@ -308,7 +298,7 @@ update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t ring, uint32_t 
 {
 	if(fromDev) step_indices(S, offset, cur, ring);
 	__shared__ CtaCounters sC;
-	if(threadIdx.x == 0) sC = CtaCounters{ 0, 0, 0 };
+	if(threadIdx.x == 0) sC = CtaCounters{ 0, 0, 0, 0, 0, 0, 0 };
 	__syncthreads();
 	const uint32_t first = blockIdx.x * P;
 	update_range(S, first, min(S.N, first + P), cur, ring, sC);
@@ -354,7 +344,9 @@ __device__ __forceinline__ void process_list(const DevSim& S, const WorkList& L,
 		const uint32_t coverEnd = __shfl_sync(0xffffffffu, d.w + d.z, lastLane);
 		const uint32_t lo = max(E0, __shfl_sync(0xffffffffu, d.w, 0)), hi = min(E1, coverEnd);
 		for(uint32_t base = lo; base < hi; base += 32 * K) {
-			unsigned long long idx[K];
+			// entry indices into syn / the reverse matrix, both shorter than
+			// 2^32 entries (checked when the simulation is built)
+			uint32_t idx[K];
 #pragma unroll
 			for(int j = 0; j < K; ++j) {
 				const uint32_t e = base + lane + 32 * j;
@@ -363,9 +355,7 @@ __device__ __forceinline__ void process_list(const DevSim& S, const WorkList& L,
 				for(uint32_t step = 16; step > 0; step >>= 1) {
 					if(__shfl_sync(0xffffffffu, d.w, q + step) <= e) q += step;
 				}
-				const unsigned long long st = (unsigned long long) __shfl_sync(0xffffffffu, d.x, q)
-						| ((unsigned long long) __shfl_sync(0xffffffffu, d.y, q) << 32);
-				idx[j] = st + (e - __shfl_sync(0xffffffffu, d.w, q));
+				idx[j] = __shfl_sync(0xffffffffu, d.x, q) + (e - __shfl_sync(0xffffffffu, d.w, q));
 			}
 			if(KIND == 0) {
 				uint2 sy[K];
@@ -487,7 +477,37 @@ __device__ __forceinline__ void red_release_add(uint32_t* p, uint32_t v)
 	asm volatile("red.release.gpu.global.add.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
 
-// target: this CTA's count of completed barriers x gridDim.x (shared)
+// The barrier in two halves: grid_arrive, then work that needs nothing from
+// the other CTAs, then grid_wait.  target: this CTA's count of completed
+// barriers x gridDim.x (shared).
+__device__ __forceinline__ void grid_arrive(GridBarrier* gb, uint32_t& target)
+{
+	__syncthreads();
+	if(threadIdx.x == 0) {
+		target += gridDim.x;
+		__threadfence();
+		red_release_add(&gb->count, 1u);
+	}
+}
+
+__device__ __forceinline__ bool grid_wait(GridBarrier* gb, uint32_t& target, uint32_t& ok)
+{
+	if(threadIdx.x == 0) {
+		uint32_t polls = 0;
+		while(ld_acquire(&gb->count) < target) {
+			if(++polls > BARRIER_SPIN_LIMIT || ld_acquire(&gb->error)) {
+				atomicExch(&gb->error, 1u);
+				ok = 0;
+				break;
+			}
+			__nanosleep(20);
+		}
+		__threadfence();
+	}
+	__syncthreads();
+	return ok != 0;
+}
+
 __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, uint32_t& target, uint32_t& ok)
 {
 	__syncthreads();
@@ -523,7 +543,7 @@ run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0
 	__shared__ CtaCounters sC;
 	__shared__ uint32_t sTarget, sOk;
 	if(threadIdx.x == 0) {
-		sC = CtaCounters{ 0, 0, 0 };
+		sC = CtaCounters{ 0, 0, 0, 0, 0, 0, 0 };
 		sTarget = 0;
 		sOk = 1;
 	}
@@ -537,11 +557,17 @@ run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0
 		deliver_range(S, cur ^ 1u, PHASE_DELIVER | PHASE_STDP | PHASE_RESET, warp, nwarps);
 		if(!grid_barrier(gb, sTarget, sOk)) return;
 		for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
-			update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC);
+			update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC, k > 0);
 		}
 		__syncthreads();
 		flush_counters(S, ring, sC);
-		if(!grid_barrier(gb, sTarget, sOk)) return;
+		// while the other CTAs finish: the next step's noise of this CTA's
+		// neurons (it depends on their RNG words only)
+		grid_arrive(gb, sTarget);
+		if(k + 1 < steps) {
+			for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) precompute_noise(S, p * P, min(S.N, p * P + P));
+		}
+		if(!grid_wait(gb, sTarget, sOk)) return;
 	}
 	if(steps) {
 		const uint32_t last = (uint32_t) ((cycle0 + steps - 1) & 1);
@@ -1195,6 +1221,7 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	}
 
 	S.hist = dalloc<uint64_t>(2 * (size_t) N);
+	S.noise = dalloc<float>(N);
 	S.recentWords = (S.W + 3) & ~3u;  // 16-byte rows for the asynchronous copy
 	S.recent = dalloc<uint32_t>(2 * (size_t) S.recentWords);
 	S.recentBytes = (S.stdp && (size_t) S.recentWords * 4 <= RECENT_FILTER_MAX_BYTES) ? S.recentWords * 4 : 0u;

@@ -71,6 +71,7 @@ struct DevSim {
 	uint32_t R;       // firing ring length (steps)
 	TypeRange types[MAX_TYPES];
 	uint32_t* rng;            // [4][N] xorshift words
+	float* noise;             // [N] next step's nrand, precomputed inside the persistent loop
 	uint64_t* hist;           // [2][N] firing history, double-buffered by step parity
 	uint32_t* recent;         // [2][recentWords] bit-vectors: history nonzero (fired in the last 64 steps), by parity
 	uint32_t recentWords;     // W rounded up to a multiple of 4
