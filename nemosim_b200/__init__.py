@@ -62,12 +62,15 @@ class Configuration:
 
     def __init__(self):
         self._h = lib().nemo_new_configuration()
+        self._delete = lib().nemo_delete_configuration
         if not self._h:
             raise NemoError(10, lib().nemo_strerror().decode())
 
     def __del__(self):
+        # the deleter was bound at construction (at interpreter exit this
+        # module's globals may already be gone)
         if getattr(self, "_h", None):
-            lib().nemo_delete_configuration(self._h)
+            self._delete(self._h)
             self._h = None
 
     def set_stdp_function(self, prefire, postfire, *limits):
@@ -103,12 +106,15 @@ class Network:
 
     def __init__(self, _handle=None):
         self._h = _handle if _handle is not None else lib().nemo_new_network()
+        self._delete = lib().nemo_delete_network
         if not self._h:
             raise NemoError(10, lib().nemo_strerror().decode())
 
     def __del__(self):
+        # the deleter was bound at construction (at interpreter exit this
+        # module's globals may already be gone)
         if getattr(self, "_h", None):
-            lib().nemo_delete_network(self._h)
+            self._delete(self._h)
             self._h = None
 
     def add_neuron_type(self, name: str) -> int:
@@ -214,10 +220,13 @@ class Simulation:
         if not h:
             raise NemoError(lib().nemo_b200_last_status(), lib().nemo_strerror().decode())
         self._h = h
+        self._delete = lib().nemo_delete_simulation
 
     def __del__(self):
+        # the deleter was bound at construction (at interpreter exit this
+        # module's globals may already be gone)
         if getattr(self, "_h", None):
-            lib().nemo_delete_simulation(self._h)
+            self._delete(self._h)
             self._h = None
 
     def step(self, fstim=None, istim=None):
@@ -425,6 +434,7 @@ class Batch(Simulation):
         if not h:
             raise NemoError(lib().nemo_b200_last_status(), lib().nemo_strerror().decode())
         self._h = h
+        self._delete = lib().nemo_delete_simulation
         self.count = len(networks)
 
     def run(self, steps: int, stdp_period: int = 0, reward: float = 1.0, ids: bool = True,

@@ -110,11 +110,13 @@ class BpttModel:
         if not h:
             raise NemoError(lib().nemo_b200_last_status(), lib().nemo_strerror().decode())
         self._h = h
+        # kept for __del__, which may run after this module's globals are gone
+        self._delete = lib().nemo_b200_bptt_delete
         self.c, self.d = net.constants(self.device)
 
     def __del__(self):
         if getattr(self, "_h", None):
-            lib().nemo_b200_bptt_delete(self._h)
+            self._delete(self._h)
             self._h = None
 
     def loss(self, W, a, b, noise, target):
