@@ -408,23 +408,40 @@ constexpr uint32_t PHASE_STDP = 2;     // the published STDP groups
 constexpr uint32_t PHASE_RESET = 4;    // empty the lists the next update publishes into
 
 // Pre-phase of a step over the lists published by the update of the step
-// with parity `pub`, each list's entries spread evenly over the `nwarps`
-// warps.
-__device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uint32_t what, uint32_t warp,
-		uint32_t nwarps)
+// with parity `pub`.  When there are both deliveries and STDP entries, the
+// CTAs split into two groups in proportion to the work (an STDP entry, two
+// dependent loads, counted as two deliveries) so that the two lists' chains
+// of dependent loads run at the same time; each list's entries are spread
+// evenly over its group's warps.  Every thread of the grid calls this.
+__device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uint32_t what)
 {
 	const unsigned long long cd = (what & PHASE_DELIVER) ? S.dlvWork.count[pub] : 0ull;
 	const unsigned long long cs = (what & PHASE_STDP) ? S.stdpWork.count[pub] : 0ull;
-	if((what & PHASE_RESET) && warp == 0 && (threadIdx.x & 31) == 0) {
+	const uint32_t nd = (uint32_t) cd, ns = (uint32_t) cs;
+	const uint32_t wpc = blockDim.x >> 5, lw = threadIdx.x >> 5;
+	if((what & PHASE_RESET) && blockIdx.x == 0 && threadIdx.x == 0) {
 		S.dlvWork.count[pub ^ 1u] = 0;
 		S.stdpWork.count[pub ^ 1u] = 0;
 	}
 	const uint64_t* hist = S.hist + (size_t) pub * S.N;
+	// CTAs [0, gs) take the STDP list, [gs, gridDim.x) the deliveries
+	uint32_t gs = ns ? gridDim.x : 0u;
+	if(nd && ns) {
+		gs = (uint32_t) ((unsigned long long) gridDim.x * 2ull * ns / ((unsigned long long) nd + 2ull * ns));
+		gs = max(1u, min(gridDim.x - 1u, gs));
+		if(gridDim.x == 1) gs = 0;  // one CTA: it does both, deliveries first
+	}
+	const bool doStdp = ns && (blockIdx.x < gs || gridDim.x == 1);
+	const bool doDlv = nd && (blockIdx.x >= gs || gridDim.x == 1);
+	if(doDlv) {
+		const uint32_t first = gridDim.x == 1 ? 0u : gs;
+		process_list<0, 8>(S, S.dlvWork, (uint32_t) (cd >> 32), nd, hist, nullptr, (blockIdx.x - first) * wpc + lw,
+				(gridDim.x - first) * wpc);
+	}
 	// the sources' "fired in the last 64 steps" bits, copied to shared
-	// memory with asynchronous 16-byte copies that overlap the deliveries
-	// (every thread of the CTA calls this function)
+	// memory with asynchronous 16-byte copies
 	extern __shared__ __align__(16) uint32_t sRecent[];
-	const bool filter = S.recentBytes && (uint32_t) cs;
+	const bool filter = doStdp && S.recentBytes;
 	if(filter) {
 		const uint32_t* g = S.recent + (size_t) pub * S.recentWords;
 		for(uint32_t q = threadIdx.x; q < S.recentWords / 4; q += blockDim.x) {
@@ -432,12 +449,14 @@ __device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uin
 			asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(g + 4 * q) : "memory");
 		}
 		asm volatile("cp.async.commit_group;" ::: "memory");
+		asm volatile("cp.async.wait_all;" ::: "memory");
 	}
-	process_list<0, 8>(S, S.dlvWork, (uint32_t) (cd >> 32), (uint32_t) cd, hist, nullptr, warp, nwarps);
-	if(filter) asm volatile("cp.async.wait_all;" ::: "memory");
 	__syncthreads();
-	process_list<1, 4>(S, S.stdpWork, (uint32_t) (cs >> 32), (uint32_t) cs, hist, filter ? sRecent : nullptr, warp,
-			nwarps);
+	if(doStdp) {
+		const uint32_t cstdp = gridDim.x == 1 ? 1u : gs;
+		process_list<1, 4>(S, S.stdpWork, (uint32_t) (cs >> 32), ns, hist, filter ? sRecent : nullptr,
+				blockIdx.x * wpc + lw, cstdp * wpc);
+	}
 	__syncthreads();  // the shared copy is rewritten by the next call
 }
 
@@ -451,7 +470,7 @@ deliver_kernel(const DevSim S, uint32_t pub, uint32_t what, uint32_t offset, int
 		step_indices(S, offset, cur, ring);
 		pub = cur ^ 1u;
 	}
-	deliver_range(S, pub, what, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, (gridDim.x * blockDim.x) >> 5);
+	deliver_range(S, pub, what);
 }
 
 // Grid-wide barrier of the persistent kernel (all CTAs co-resident: it is
@@ -549,12 +568,11 @@ run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0
 	}
 	__syncthreads();
 	const uint32_t nparts = (S.N + P - 1) / P;
-	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
 	for(uint32_t k = 0; k < steps; ++k) {
 		const unsigned long long c = cycle0 + k;
 		const uint32_t cur = (uint32_t) (c & 1);
 		const uint32_t ring = (uint32_t) (c % S.R);
-		deliver_range(S, cur ^ 1u, PHASE_DELIVER | PHASE_STDP | PHASE_RESET, warp, nwarps);
+		deliver_range(S, cur ^ 1u, PHASE_DELIVER | PHASE_STDP | PHASE_RESET);
 		if(!grid_barrier(gb, sTarget, sOk)) return;
 		for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
 			update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC, k > 0);
@@ -571,36 +589,36 @@ run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0
 	}
 	if(steps) {
 		const uint32_t last = (uint32_t) ((cycle0 + steps - 1) & 1);
-		deliver_range(S, last, PHASE_STDP, warp, nwarps);
+		deliver_range(S, last, PHASE_STDP);
 		if(!grid_barrier(gb, sTarget, sOk)) return;
 		if(blockIdx.x == 0 && threadIdx.x == 0) S.stdpWork.count[last] = 0;
 	}
 }
 
 // Turns the targets touched since the last applyStdp (a bit-vector) into
-// chunks of their incoming plastic synapses, and clears the bit-vector.
+// chunks of their incoming plastic synapses, and clears the bit-vector: one
+// thread per neuron, one reservation per warp.
 __global__ void __launch_bounds__(STEP_THREADS)
 collect_touched_kernel(const DevSim S)
 {
 	const uint32_t stride = gridDim.x * blockDim.x;
-	const uint32_t words = (S.W + 31) & ~31u;  // whole warps take part in the reservation
-	for(uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += stride) {
-		const uint32_t bits = w < S.W ? S.touchedBits[w] : 0u;
-		uint32_t nch = 0;
-		for(uint32_t b = bits; b; b &= b - 1) {
-			const uint32_t n = w * 32 + __ffs(b) - 1;
-			nch += (uint32_t) ((S.rcmPtr[n + 1] - S.rcmPtr[n] + CHUNK - 1) / CHUNK);
+	const uint32_t lane = threadIdx.x & 31;
+	const uint32_t end = S.W * 32;  // whole warps, so that all lanes take part in the reservation
+	for(uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < end; n += stride) {
+		const uint32_t word = S.touchedBits[n >> 5];
+		const bool touched = n < S.N && ((word >> lane) & 1u);
+		unsigned long long rb = 0;
+		uint32_t len = 0;
+		if(touched) {
+			rb = S.rcmPtr[n];
+			len = (uint32_t) (S.rcmPtr[n + 1] - rb);
 		}
-		uint32_t pos = reserve_chunks(S.applyChunkCount, nch);
-		for(uint32_t b = bits; b; b &= b - 1) {
-			const uint32_t n = w * 32 + __ffs(b) - 1;
-			const unsigned long long rb = S.rcmPtr[n];
-			const uint32_t len = (uint32_t) (S.rcmPtr[n + 1] - rb);
-			const uint32_t c = (len + CHUNK - 1) / CHUNK;
-			write_chunks(S.applyChunks, pos, rb, len, c, n);
-			pos += c;
+		const uint32_t nch = (len + CHUNK - 1) / CHUNK;
+		if(__any_sync(0xffffffffu, nch != 0)) {
+			const uint32_t pos = reserve_chunks(S.applyChunkCount, nch);
+			write_chunks(S.applyChunks, pos, rb, len, nch, n);
 		}
-		if(bits) S.touchedBits[w] = 0u;
+		if(lane == 0 && word) S.touchedBits[n >> 5] = 0u;
 	}
 }
 
@@ -1387,7 +1405,9 @@ void Simulation::flushStdp()
 // n consecutive steps in one cooperative launch of the persistent step loop
 void Simulation::launchRun(unsigned n)
 {
-	NB_CUDA(cudaMemsetAsync(m_barrier, 0, sizeof(GridBarrier), m_stream));
+	// the arrival counter restarts for every launch; the error word is
+	// sticky until checkBarrier reads it
+	NB_CUDA(cudaMemsetAsync(&m_barrier->count, 0, 4, m_stream));
 	DevSim dev = m_dev;
 	uint32_t P = m_runP, steps = n;
 	unsigned long long c0 = m_cycle;
@@ -1403,16 +1423,20 @@ void Simulation::launchRun(unsigned n)
 	m_cycle += n;
 	m_timerSteps += n;
 	m_stdpPending = false;  // the loop ends with the last step's STDP accumulation
-	// read back with the run's statistics; checked by checkBarrier()
-	NB_CUDA(cudaMemcpyAsync(m_hBarrierError, &m_barrier->error, 4, cudaMemcpyDeviceToHost, m_stream));
+	m_barrierUsed = true;
 }
 
 // after a stream synchronisation: a grid-barrier wait of the persistent step
-// loop that gave up leaves the simulation state undefined
+// loop that gave up (in any launch since the last check) leaves the
+// simulation state undefined
 void Simulation::checkBarrier()
 {
-	if(m_hBarrierError && *m_hBarrierError) {
+	if(!m_barrierUsed) return;
+	m_barrierUsed = false;
+	NB_CUDA(cudaMemcpy(m_hBarrierError, &m_barrier->error, 4, cudaMemcpyDeviceToHost));
+	if(*m_hBarrierError) {
 		*m_hBarrierError = 0;
+		NB_CUDA(cudaMemset(&m_barrier->error, 0, 4));
 		NB_THROW(NEMO_CUDA_ERROR, "persistent step loop: a grid barrier wait timed out");
 	}
 }
@@ -1542,7 +1566,8 @@ void Simulation::applyStdpDevice(int32_t R)
 		unsigned grid = std::min<unsigned>((m_N + 7) / 8, (unsigned) m_sms * 8);
 		apply_full_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, R);
 	} else {
-		unsigned cgrid = std::max(1u, std::min<unsigned>((m_dev.W + STEP_THREADS - 1) / STEP_THREADS, (unsigned) m_sms * 4));
+		const unsigned cgrid = std::max(1u, std::min<unsigned>((m_dev.W * 32 + STEP_THREADS - 1) / STEP_THREADS,
+				(unsigned) m_sms * 8));
 		collect_touched_kernel<<<cgrid, STEP_THREADS, 0, m_stream>>>(m_dev);
 		apply_touched_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, R);
 	}

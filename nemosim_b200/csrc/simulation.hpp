@@ -201,6 +201,7 @@ private:
 	void checkBarrier();
 	GridBarrier* m_barrier = nullptr;
 	uint32_t* m_hBarrierError = nullptr;  // pinned copy of m_barrier->error
+	bool m_barrierUsed = false;           // a persistent launch ran since the last checkBarrier
 	unsigned m_runGrid = 0;  // co-resident CTAs of run_kernel at m_runT threads (0: no cooperative launch)
 	uint32_t m_runP = 0;     // neurons per partition of run_kernel
 	uint32_t m_runT = RUN_THREADS;
