@@ -296,7 +296,7 @@ NEMO_B200_API nemo_status_t nemo_b200_run_stats(nemo_simulation_t, float* run_ms
 /* Launch shape of the active step loop: neurons per partition (rounded up
  * to a multiple of 32; at most 2048 for the two-launch step, where a CTA
  * owns one partition; a CTA of the persistent loop owns one or more) and
- * threads per CTA (a multiple of 32, at most 1024; 64 to 384 for the
+ * threads per CTA (a multiple of 32, at most 1024; 64 to 768 for the
  * persistent loop).  Results are identical for every shape. */
 NEMO_B200_API nemo_status_t nemo_b200_set_launch(nemo_simulation_t, unsigned partition, unsigned threads);
 NEMO_B200_API nemo_status_t nemo_b200_get_launch(nemo_simulation_t, unsigned* partition, unsigned* threads);

@@ -556,7 +556,7 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, uint32_t& target, 
 // owns the partitions c, c + gridDim.x, ... of P neurons; the pre-phases
 // spread the chunks over all warps of the grid.  Identical results to
 // deliver_kernel + update_kernel per step.
-__global__ void __launch_bounds__(RUN_THREADS, 2)
+__global__ void __launch_bounds__(RUN_THREADS, 1)
 run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0, GridBarrier* gb)
 {
 	__shared__ CtaCounters sC;
@@ -1258,7 +1258,13 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 
 	if(needCalib) S.calib = device_calibration(m_device);
 	NB_CUDA(cudaDeviceGetAttribute(&m_sms, cudaDevAttrMultiProcessorCount, m_device));
-	m_deliverGrid = (unsigned) m_sms * 8;
+	// the two-launch pre-phase: as many CTAs as fit on the GPU at once
+	{
+		int perSm = 0;
+		NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, deliver_kernel, STEP_THREADS, S.recentBytes));
+		m_deliverGrid = (unsigned) std::max(1, perSm) * (unsigned) m_sms;
+	}
+	m_applyGrid = (unsigned) m_sms * 8;
 	// default shape of the two-launch step (set while the persistent loop is
 	// not yet configured): two partitions per SM
 	{
@@ -1270,7 +1276,8 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	{
 		int coop = 0;
 		NB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, m_device));
-		m_runGrid = coop ? runGridFor(RUN_THREADS) : 0;
+		m_runT = 384;  // the default shape: two CTAs of 384 threads per SM
+		m_runGrid = coop ? runGridFor(m_runT) : 0;
 		if(m_runGrid) {
 			const size_t per = (N + m_runGrid - 1) / m_runGrid;
 			m_runP = (uint32_t) std::max<size_t>(32, (per + 31) & ~(size_t) 31);
@@ -1569,7 +1576,7 @@ void Simulation::applyStdpDevice(int32_t R)
 		const unsigned cgrid = std::max(1u, std::min<unsigned>((m_dev.W * 32 + STEP_THREADS - 1) / STEP_THREADS,
 				(unsigned) m_sms * 8));
 		collect_touched_kernel<<<cgrid, STEP_THREADS, 0, m_stream>>>(m_dev);
-		apply_touched_kernel<<<m_deliverGrid, STEP_THREADS, 0, m_stream>>>(m_dev, R);
+		apply_touched_kernel<<<m_applyGrid, STEP_THREADS, 0, m_stream>>>(m_dev, R);
 	}
 	timedEnd();
 	// updatedWeight's result always lies within the clamp range of its sign
@@ -1781,8 +1788,8 @@ float Simulation::autotune(unsigned trialSteps)
 	std::vector<std::pair<uint32_t, uint32_t>> cands;
 	const bool pers = persistentActive();
 	if(pers) {
-		// persistent loop: 192 to RUN_THREADS threads per CTA, 1 to 4 partitions per CTA
-		for(uint32_t T : {192u, 256u, RUN_THREADS}) {
+		// persistent loop: 256 to RUN_THREADS threads per CTA, 1 to 4 partitions per CTA
+		for(uint32_t T : {256u, 384u, RUN_THREADS}) {
 			const unsigned g = runGridFor(T);
 			if(!g) continue;
 			for(unsigned k : {1u, 2u, 4u}) {

@@ -18,7 +18,7 @@ namespace nemo_b200 {
 constexpr unsigned MAX_TYPES = 8;
 constexpr unsigned STEP_THREADS = 256;   // block size of the apply/stimulus kernels
 constexpr unsigned MAX_PARTITION = 2048; // neurons per CTA of the step kernel
-constexpr unsigned RUN_THREADS = 384;    // block size of the persistent step loop
+constexpr unsigned RUN_THREADS = 768;    // largest block of the persistent step loop (registers for 768 x 1 or 384 x 2 per SM)
 
 // Grid barrier of the persistent step loop (device memory, zeroed before
 // each launch).
@@ -204,7 +204,7 @@ private:
 	bool m_barrierUsed = false;           // a persistent launch ran since the last checkBarrier
 	unsigned m_runGrid = 0;  // co-resident CTAs of run_kernel at m_runT threads (0: no cooperative launch)
 	uint32_t m_runP = 0;     // neurons per partition of run_kernel
-	uint32_t m_runT = RUN_THREADS;
+	uint32_t m_runT = 384;
 	unsigned runGridFor(uint32_t T) const;
 	void buildGraph();
 	static constexpr unsigned GRAPH_STEPS = 100;
@@ -213,7 +213,8 @@ private:
 	unsigned long long* m_hCycle = nullptr;
 	size_t decodeBatchStep(uint32_t r, unsigned step, unsigned* counts, unsigned* ids, size_t pos, size_t cap);
 	std::vector<std::vector<uint32_t>> m_batchScratch;
-	unsigned m_deliverGrid = 1184;
+	unsigned m_deliverGrid = 1184;  // CTAs of deliver_kernel
+	unsigned m_applyGrid = 1184;    // CTAs of apply_touched_kernel
 	uint32_t m_P = 256, m_T = 256;
 	uint32_t m_maxOutDeg = 0, m_maxPlasticInDeg = 0;
 	int m_sms = 148;
