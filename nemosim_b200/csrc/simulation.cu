@@ -132,8 +132,9 @@ struct CtaCounters {
 // multiple of 32, so warps cover whole bit-vector words); the CTA's
 // blockDim.x threads loop over them.  Every thread of the CTA calls it.
 // cur = t & 1.
+// hostFired: also write the fired bit-vector words there (host memory)
 __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, uint32_t last, uint32_t cur,
-		uint32_t ring, CtaCounters& C, bool preNoise = false)
+		uint32_t ring, CtaCounters& C, bool preNoise = false, uint32_t* hostFired = nullptr)
 {
 	const uint32_t tid = threadIdx.x, lane = tid & 31;
 	const uint64_t* histPrev = S.hist + (size_t) (cur ^ 1u) * S.N;
@@ -207,6 +208,7 @@ __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, ui
 		const uint32_t rbits = __ballot_sync(0xffffffffu, hist_nonzero);
 		if(lane == 0 && n < last) {
 			S.firedRing[(size_t) ring * S.W + (n >> 5)] = fb;
+			if(hostFired) hostFired[n >> 5] = fb;
 			S.recent[(size_t) cur * S.recentWords + (n >> 5)] = rbits;
 			if(fw) S.fstim[n >> 5] = 0u;
 		}
@@ -294,14 +296,15 @@ __device__ __forceinline__ void flush_counters(const DevSim& S, uint32_t ring, C
 // One step's neuron update: CTA c owns the partition of P consecutive
 // neurons starting at c * P (P a multiple of 32).
 __global__ void __launch_bounds__(1024)
-update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t ring, uint32_t offset, int fromDev)
+update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t ring, uint32_t offset, int fromDev,
+		uint32_t* hostFired = nullptr)
 {
 	if(fromDev) step_indices(S, offset, cur, ring);
 	__shared__ CtaCounters sC;
 	if(threadIdx.x == 0) sC = CtaCounters{ 0, 0, 0, 0, 0, 0, 0 };
 	__syncthreads();
 	const uint32_t first = blockIdx.x * P;
-	update_range(S, first, min(S.N, first + P), cur, ring, sC);
+	update_range(S, first, min(S.N, first + P), cur, ring, sC, false, hostFired);
 	__syncthreads();
 	flush_counters(S, ring, sC);
 }
@@ -461,14 +464,24 @@ __device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uin
 }
 
 // Pre-phase of step t (pub = (t - 1) & 1), or with what = PHASE_STDP the
-// STDP accumulation of the last step before applyStdp.
+// STDP accumulation of the last step before applyStdp.  With stim, it also
+// applies the step's stimulus (src/nemo/cpu/Simulation.cpp:141-171), read
+// from host memory: nf firing-stimulus indices, then ni current-stimulus
+// indices and ni values (distinct indices); the update reads them next.
 __global__ void __launch_bounds__(STEP_THREADS)
-deliver_kernel(const DevSim S, uint32_t pub, uint32_t what, uint32_t offset, int fromDev)
+deliver_kernel(const DevSim S, uint32_t pub, uint32_t what, uint32_t offset, int fromDev,
+		const uint32_t* stim = nullptr, uint32_t nf = 0, uint32_t ni = 0)
 {
 	if(fromDev) {
 		uint32_t cur, ring;
 		step_indices(S, offset, cur, ring);
 		pub = cur ^ 1u;
+	}
+	if(stim) {
+		for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < max(nf, ni); i += gridDim.x * blockDim.x) {
+			if(i < nf) atomicOr(&S.fstim[stim[i] >> 5], 1u << (stim[i] & 31));
+			if(i < ni) S.curExt[stim[nf + i]] = __uint_as_float(stim[nf + ni + i]);
+		}
 	}
 	deliver_range(S, pub, what);
 }
@@ -1255,6 +1268,8 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	S.eventCount = dalloc<unsigned long long>(S.R);
 	S.stdpCount = dalloc<unsigned long long>(S.R);
 	NB_CUDA(cudaMallocHost(&m_hFired, (size_t) S.R * S.W * 4));
+	NB_CUDA(cudaHostAlloc(&m_hFiredMapped, (size_t) S.W * 4, cudaHostAllocMapped));
+	NB_CUDA(cudaHostGetDevicePointer(&m_dFiredMapped, m_hFiredMapped, 0));
 
 	if(needCalib) S.calib = device_calibration(m_device);
 	NB_CUDA(cudaDeviceGetAttribute(&m_sms, cudaDevAttrMultiProcessorCount, m_device));
@@ -1303,8 +1318,8 @@ Simulation::~Simulation()
 	if(m_hCycle) cudaFreeHost(m_hCycle);
 	if(m_hBarrierError) cudaFreeHost(m_hBarrierError);
 	if(m_hFired) cudaFreeHost(m_hFired);
+	if(m_hFiredMapped) cudaFreeHost(m_hFiredMapped);
 	if(m_hStim) cudaFreeHost(m_hStim);
-	if(m_dStim) cudaFree(m_dStim);
 	if(m_ev0) cudaEventDestroy(m_ev0);
 	if(m_ev1) cudaEventDestroy(m_ev1);
 	for(cudaEvent_t e : m_evPool) cudaEventDestroy(e);
@@ -1503,56 +1518,65 @@ void Simulation::buildGraph()
 	m_graphT = m_T;
 }
 
+// One step with host buffers: the stimulus is staged in mapped host memory
+// that the pre-phase kernel reads, and the update writes the fired
+// bit-vector words to mapped host memory, so no copy is queued.
 const std::vector<unsigned>& Simulation::step(const unsigned* fstim, size_t nf,
 		const unsigned* inidx, const float* icur, size_t ni)
 {
 	NB_CUDA(cudaSetDevice(m_device));
 	// validate and map the stimulus before touching any state
 	// (src/nemo/cpu/Simulation.cpp:141-163; the last current for a neuron wins)
-	size_t nstim = nf + 2 * ni;
-	if(nstim) {
-		std::vector<uint32_t> fl(nf);
-		for(size_t i = 0; i < nf; ++i) fl[i] = localIdx(fstim[i]);
-		std::unordered_map<uint32_t, float> cur;
-		std::vector<uint32_t> corder;
+	std::vector<uint32_t>& fl = m_stepScratch;
+	fl.resize(nf);
+	for(size_t i = 0; i < nf; ++i) fl[i] = localIdx(fstim[i]);
+	std::vector<std::pair<uint32_t, float>>& cur = m_stepCurrents;
+	cur.clear();
+	if(ni) {
+		std::unordered_map<uint32_t, size_t> at;
 		for(size_t i = 0; i < ni; ++i) {
-			uint32_t l = localIdx(inidx[i]);
-			if(cur.find(l) == cur.end()) corder.push_back(l);
-			cur[l] = icur[i];
+			const uint32_t l = localIdx(inidx[i]);
+			auto it = at.find(l);
+			if(it == at.end()) {
+				at.emplace(l, cur.size());
+				cur.emplace_back(l, icur[i]);
+			} else {
+				cur[it->second].second = icur[i];
+			}
 		}
-		size_t need = nf + 2 * corder.size();
-		if(need > m_stimCap) {
-			if(m_hStim) cudaFreeHost(m_hStim);
-			if(m_dStim) cudaFree(m_dStim);
-			m_stimCap = std::max<size_t>(need, 1024);
-			NB_CUDA(cudaMallocHost(&m_hStim, m_stimCap * 4));
-			NB_CUDA(cudaMalloc(&m_dStim, m_stimCap * 4));
-		}
-		else {
-			sync(); // the staging buffer may still be in flight
-		}
-		memcpy(m_hStim, fl.data(), nf * 4);
-		for(size_t i = 0; i < corder.size(); ++i) {
-			m_hStim[nf + i] = corder[i];
-			float v = cur[corder[i]];
-			memcpy(&m_hStim[nf + corder.size() + i], &v, 4);
-		}
-		NB_CUDA(cudaMemcpyAsync(m_dStim, m_hStim, need * 4, cudaMemcpyHostToDevice, m_stream));
-		uint32_t nmax = (uint32_t) std::max(nf, corder.size());
-		stimulus_kernel<<<(nmax + 255) / 256, 256, 0, m_stream>>>(m_dev, m_dStim, (uint32_t) nf,
-				m_dStim + nf, reinterpret_cast<const float*>(m_dStim + nf + corder.size()), (uint32_t) corder.size());
 	}
+	const size_t need = nf + 2 * cur.size();
+	if(need > m_stimCap) {
+		// no kernel reads the old buffer: every step() ends synchronised
+		if(m_hStim) cudaFreeHost(m_hStim);
+		m_hStim = nullptr;
+		m_stimCap = std::max<size_t>(need, 1024);
+		NB_CUDA(cudaHostAlloc(&m_hStim, m_stimCap * 4, cudaHostAllocMapped));
+		NB_CUDA(cudaHostGetDevicePointer(&m_dStimMapped, m_hStim, 0));
+	}
+	if(need) {
+		memcpy(m_hStim, fl.data(), nf * 4);
+		for(size_t i = 0; i < cur.size(); ++i) {
+			m_hStim[nf + i] = cur[i].first;
+			memcpy(&m_hStim[nf + cur.size() + i], &cur[i].second, 4);
+		}
+	}
+	const uint32_t c = (uint32_t) (m_cycle & 1);
 	const uint32_t ring = (uint32_t) (m_cycle % m_dev.R);
-	launchStep(true);
-	NB_CUDA(cudaMemcpyAsync(m_hFired, m_dev.firedRing + (size_t) ring * m_dev.W, (size_t) m_dev.W * 4,
-			cudaMemcpyDeviceToHost, m_stream));
+	deliver_kernel<<<m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream>>>(m_dev, c ^ 1u,
+			PHASE_DELIVER | PHASE_STDP | PHASE_RESET, 0, 0, need ? m_dStimMapped : nullptr, (uint32_t) nf,
+			(uint32_t) cur.size());
+	update_kernel<<<(m_N + m_P - 1) / m_P, m_T, 0, m_stream>>>(m_dev, m_P, c, ring, 0, 0, m_dFiredMapped);
+	m_cycle++;
+	m_timerSteps++;
+	m_stdpPending = true;
 	sync();
 	NB_CUDA(cudaGetLastError());
 	// fired neurons in ascending local index, as global ids
 	// (setFiring, src/nemo/cpu/Simulation.cpp:200-208)
 	m_fired.clear();
 	for(uint32_t w = 0; w < m_dev.W; ++w) {
-		uint32_t bits = m_hFired[w];
+		uint32_t bits = m_hFiredMapped[w];
 		while(bits) {
 			uint32_t b = __builtin_ctz(bits);
 			bits &= bits - 1;

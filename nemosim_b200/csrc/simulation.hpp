@@ -257,9 +257,13 @@ private:
 
 	// host staging
 	uint32_t* m_hFired = nullptr;  // pinned, [R][W]
-	uint32_t* m_hStim = nullptr;   // pinned stimulus staging
-	uint32_t* m_dStim = nullptr;
+	uint32_t* m_hStim = nullptr;   // mapped pinned stimulus staging of step()
+	uint32_t* m_dStimMapped = nullptr;
 	size_t m_stimCap = 0;
+	uint32_t* m_hFiredMapped = nullptr;  // mapped pinned [W]: step()'s fired words
+	uint32_t* m_dFiredMapped = nullptr;
+	std::vector<uint32_t> m_stepScratch;
+	std::vector<std::pair<uint32_t, float>> m_stepCurrents;
 	std::vector<unsigned> m_fired;
 	std::vector<uint32_t> m_outDegree;
 
