@@ -447,11 +447,20 @@ def run_batch(args, local):
     streams = batch.streams(counts, ids)
     mismatched = sum(1 for (c1, i1), (c2, i2) in zip(streams, seq)
                      if not (np.array_equal(c1, c2) and np.array_equal(i1, i2)))
-    # the same batch continued with two launches per step from CUDA graphs
-    batch.set_persistent(False)
-    batch.run(ms, ids=False)
-    graph_ms = batch.run_stats()["run_ms"]
+    # the same batch continued with each step loop in turn (the default
+    # above is the persistent loop unless the batch has more than two neurons
+    # per resident thread)
+    loop_ms = {}
+    for persistent in (True, False):
+        batch.set_persistent(persistent)
+        batch.run(ms, ids=False)
+        loop_ms["persistent" if persistent else "two_launch_graphs"] = batch.run_stats()["run_ms"]
     synapses = sum(sp["n"] * sp["f"] for sp in specs)
+    # algorithmic bytes of the checked run (no STDP): neuron-steps, the
+    # fired neurons' c and d, synaptic events
+    alg = neurons * B_NEURON * ms + st["fired"] * B_FIRED + st["events"] * B_EVENT
+    peak, peak_kind = measured_peak_gbs()
+    achieved = alg / (batch_ms / 1e3) / 1e9
     line = {
         "metric": "batched speedup vs sequential plain runs", "value": seq_ms / batch_ms, "unit": "x",
         "n_gpus": 1, "higher_is_better": True, "dtype": "fp32+f64+int64", "data": "synthetic",
@@ -461,9 +470,11 @@ def run_batch(args, local):
                    "sigma": [2.0, 8.0], "ms": ms, "total_neurons": neurons, "total_synapses": synapses,
                    "generator": "random::construct (src/examples/random.cpp) per network, own seed and sigma"},
         "batch_ms": batch_ms, "sequential_ms": seq_ms, "sequential_wall_s": seq_wall,
-        "batch_two_launch_graphs_ms": graph_ms, "speedup_two_launch_graphs": seq_ms / graph_ms,
+        "continued_runs_ms": loop_ms,
         "batch_events_per_s": st["events"] / (batch_ms / 1e3),
         "bitexact_vs_individual_runs": mismatched == 0, "mismatched_networks": mismatched,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind, "alg_bytes": alg},
         "launch": {"partition": launch[0], "threads": launch[1], "autotuned_us_per_step": tuned_us},
         "batch_build_s": build_s, "clocks": clk.summary(),
     }

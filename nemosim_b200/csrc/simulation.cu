@@ -32,16 +32,18 @@ namespace nemo_b200 {
 //    update of step t - 1, adds its weights -- read now, at arrival, as the
 //    reference does -- into each target's accumulator; it also runs the
 //    STDP accumulation of step t - 1;
-//  - the update of step t advances every neuron and publishes, as chunks of
-//    at most CHUNK synapses in global lists, the delay groups that arrive
-//    at t + 1 and the incoming plastic synapses of this step's STDP targets.
+//  - the update of step t advances every neuron and publishes, as ranges in
+//    two work lists (WorkList), the delay groups that arrive at t + 1 and
+//    the incoming plastic synapses of this step's STDP targets.
 //
-// All warps of the GPU share the chunks of a phase, so its work is balanced
-// however the spikes fall.  The phases run as two kernels per step
-// (deliver_kernel, update_kernel) or inside the persistent step loop
-// (run_kernel), one cooperative launch for many steps.  STDP accumulation
-// of the last step runs before applyStdp (stdp_flush); deliveries stay
-// pending until the next step, so they read the weights applyStdp leaves.
+// A pre-phase spreads each list's entries evenly over its warps, so its
+// work is balanced however the spikes fall.  The phases run as two kernels
+// per step (deliver_kernel, update_kernel) or inside the persistent step
+// loop (run_kernel), one cooperative launch for many steps.  The STDP
+// accumulation of the last step runs before applyStdp (flushStdp);
+// deliveries stay pending until the next step, so they read the weights
+// applyStdp leaves.  applyStdp itself works on chunks of at most CHUNK
+// synapses of the targets touched since its last call.
 
 constexpr uint32_t CHUNK = 128;  // entries per chunk: 4 per lane of a warp
 constexpr uint32_t ILP = CHUNK / 32;
@@ -463,11 +465,20 @@ __device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uin
 	__syncthreads();  // the shared copy is rewritten by the next call
 }
 
+// A step's stimulus (src/nemo/cpu/Simulation.cpp:141-171) read from host
+// memory: nf firing-stimulus indices, then ni current-stimulus indices and
+// ni values (distinct indices), for the update that follows.
+__device__ __forceinline__ void apply_stimulus(const DevSim& S, const uint32_t* stim, uint32_t nf, uint32_t ni)
+{
+	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < max(nf, ni); i += gridDim.x * blockDim.x) {
+		if(i < nf) atomicOr(&S.fstim[stim[i] >> 5], 1u << (stim[i] & 31));
+		if(i < ni) S.curExt[stim[nf + i]] = __uint_as_float(stim[nf + ni + i]);
+	}
+}
+
 // Pre-phase of step t (pub = (t - 1) & 1), or with what = PHASE_STDP the
 // STDP accumulation of the last step before applyStdp.  With stim, it also
-// applies the step's stimulus (src/nemo/cpu/Simulation.cpp:141-171), read
-// from host memory: nf firing-stimulus indices, then ni current-stimulus
-// indices and ni values (distinct indices); the update reads them next.
+// applies the step's stimulus (apply_stimulus).
 __global__ void __launch_bounds__(STEP_THREADS)
 deliver_kernel(const DevSim S, uint32_t pub, uint32_t what, uint32_t offset, int fromDev,
 		const uint32_t* stim = nullptr, uint32_t nf = 0, uint32_t ni = 0)
@@ -477,12 +488,7 @@ deliver_kernel(const DevSim S, uint32_t pub, uint32_t what, uint32_t offset, int
 		step_indices(S, offset, cur, ring);
 		pub = cur ^ 1u;
 	}
-	if(stim) {
-		for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < max(nf, ni); i += gridDim.x * blockDim.x) {
-			if(i < nf) atomicOr(&S.fstim[stim[i] >> 5], 1u << (stim[i] & 31));
-			if(i < ni) S.curExt[stim[nf + i]] = __uint_as_float(stim[nf + ni + i]);
-		}
-	}
+	if(stim) apply_stimulus(S, stim, nf, ni);
 	deliver_range(S, pub, what);
 }
 
@@ -567,16 +573,23 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, uint32_t& target, 
 // barriers, then the STDP accumulation of the last step (so applyStdp may
 // follow directly; its deliveries stay pending for the next step).  CTA c
 // owns the partitions c, c + gridDim.x, ... of P neurons; the pre-phases
-// spread the chunks over all warps of the grid.  Identical results to
-// deliver_kernel + update_kernel per step.
+// spread the work lists over all CTAs of the grid.  After each update the
+// CTAs compute the next step's noise while the barrier completes.
+// Identical results to deliver_kernel + update_kernel per step.
+// base: the barrier counter's value when the launch starts.  Without
+// finalStdp the last step's STDP accumulation is left to the next
+// pre-phase, as after a two-launch step.  stim (the first step's stimulus,
+// apply_stimulus) and hostFired (the last step's fired words) serve
+// nemo_step.
 __global__ void __launch_bounds__(RUN_THREADS, 1)
-run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0, GridBarrier* gb)
+run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0, GridBarrier* gb, uint32_t base,
+		int finalStdp, const uint32_t* stim, uint32_t nf, uint32_t ni, uint32_t* hostFired)
 {
 	__shared__ CtaCounters sC;
 	__shared__ uint32_t sTarget, sOk;
 	if(threadIdx.x == 0) {
 		sC = CtaCounters{ 0, 0, 0, 0, 0, 0, 0 };
-		sTarget = 0;
+		sTarget = base;
 		sOk = 1;
 	}
 	__syncthreads();
@@ -585,10 +598,12 @@ run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0
 		const unsigned long long c = cycle0 + k;
 		const uint32_t cur = (uint32_t) (c & 1);
 		const uint32_t ring = (uint32_t) (c % S.R);
+		if(k == 0 && stim) apply_stimulus(S, stim, nf, ni);
 		deliver_range(S, cur ^ 1u, PHASE_DELIVER | PHASE_STDP | PHASE_RESET);
 		if(!grid_barrier(gb, sTarget, sOk)) return;
+		uint32_t* hf = k + 1 == steps ? hostFired : nullptr;
 		for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
-			update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC, k > 0);
+			update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC, k > 0, hf);
 		}
 		__syncthreads();
 		flush_counters(S, ring, sC);
@@ -600,7 +615,7 @@ run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0
 		}
 		if(!grid_wait(gb, sTarget, sOk)) return;
 	}
-	if(steps) {
+	if(steps && finalStdp) {
 		const uint32_t last = (uint32_t) ((cycle0 + steps - 1) & 1);
 		deliver_range(S, last, PHASE_STDP);
 		if(!grid_barrier(gb, sTarget, sOk)) return;
@@ -1425,26 +1440,35 @@ void Simulation::flushStdp()
 }
 
 // n consecutive steps in one cooperative launch of the persistent step loop
-void Simulation::launchRun(unsigned n)
+// (finalStdp, stim, nf, ni, hostFired: see run_kernel)
+void Simulation::launchRun(unsigned n, bool finalStdp, const uint32_t* stim, uint32_t nf, uint32_t ni,
+		uint32_t* hostFired)
 {
-	// the arrival counter restarts for every launch; the error word is
-	// sticky until checkBarrier reads it
-	NB_CUDA(cudaMemsetAsync(&m_barrier->count, 0, 4, m_stream));
 	DevSim dev = m_dev;
 	uint32_t P = m_runP, steps = n;
 	unsigned long long c0 = m_cycle;
 	GridBarrier* gb = m_barrier;
-	void* args[] = { &dev, &P, &steps, &c0, &gb };
 	// no more CTAs than partitions (a CTA without one only takes part in the
 	// delivery phase, which the other CTAs' warps cover as well)
 	const unsigned grid = (unsigned) std::min<uint64_t>(m_runGrid, std::max<uint64_t>(1, (m_N + P - 1) / P));
+	// the barrier counter runs on across launches; restart it well before
+	// it could wrap
+	const uint64_t arrivals = (uint64_t) grid * (2ull * n + (finalStdp ? 1 : 0));
+	if(m_barrierBase + arrivals >= (1ull << 31)) {
+		NB_CUDA(cudaMemsetAsync(&m_barrier->count, 0, 4, m_stream));
+		m_barrierBase = 0;
+	}
+	uint32_t base = (uint32_t) m_barrierBase;
+	int fin = finalStdp ? 1 : 0;
+	void* args[] = { &dev, &P, &steps, &c0, &gb, &base, &fin, &stim, &nf, &ni, &hostFired };
 	timedBegin(K_RUN);
 	NB_CUDA(cudaLaunchCooperativeKernel((const void*) run_kernel, dim3(grid), dim3(m_runT), args, m_dev.recentBytes,
 			m_stream));
 	timedEnd();
+	m_barrierBase += arrivals;
 	m_cycle += n;
 	m_timerSteps += n;
-	m_stdpPending = false;  // the loop ends with the last step's STDP accumulation
+	m_stdpPending = !finalStdp;
 	m_barrierUsed = true;
 }
 
@@ -1458,7 +1482,8 @@ void Simulation::checkBarrier()
 	NB_CUDA(cudaMemcpy(m_hBarrierError, &m_barrier->error, 4, cudaMemcpyDeviceToHost));
 	if(*m_hBarrierError) {
 		*m_hBarrierError = 0;
-		NB_CUDA(cudaMemset(&m_barrier->error, 0, 4));
+		NB_CUDA(cudaMemset(m_barrier, 0, sizeof(GridBarrier)));
+		m_barrierBase = 0;
 		NB_THROW(NEMO_CUDA_ERROR, "persistent step loop: a grid barrier wait timed out");
 	}
 }
@@ -1561,6 +1586,9 @@ const std::vector<unsigned>& Simulation::step(const unsigned* fstim, size_t nf,
 			memcpy(&m_hStim[nf + cur.size() + i], &cur[i].second, 4);
 		}
 	}
+	// two launches (a one-step cooperative launch of the persistent loop is
+	// slower here: its launch and grid barriers cost more than a second
+	// kernel)
 	const uint32_t c = (uint32_t) (m_cycle & 1);
 	const uint32_t ring = (uint32_t) (m_cycle % m_dev.R);
 	deliver_kernel<<<m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream>>>(m_dev, c ^ 1u,
@@ -1635,6 +1663,13 @@ void Simulation::run(unsigned steps, unsigned stdpPeriod, float reward, unsigned
 		if(!m_dev.stdp) NB_THROW(NEMO_LOGIC_ERROR, "applyStdp called, but no STDP model specified");
 		R = fx_toFix(reward);
 		if(R == 0 && reward != 0) NB_THROW(NEMO_INVALID_INPUT, "STDP reward rounded down to zero");
+	}
+	// the two-launch loop's CUDA graph is instantiated (once per launch
+	// shape) before the run's timing events, which time the simulation only
+	const unsigned longest = stdpPeriod ? std::min(stdpPeriod, steps) : steps;
+	if(!persistentActive() && useGraphs && !profiling && longest >= GRAPH_STEPS
+			&& (!m_graph || m_graphP != m_P || m_graphT != m_T)) {
+		buildGraph();
 	}
 	size_t total = 0;
 	float runMs = 0;

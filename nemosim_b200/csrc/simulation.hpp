@@ -20,8 +20,8 @@ constexpr unsigned STEP_THREADS = 256;   // block size of the apply/stimulus ker
 constexpr unsigned MAX_PARTITION = 2048; // neurons per CTA of the step kernel
 constexpr unsigned RUN_THREADS = 768;    // largest block of the persistent step loop (registers for 768 x 1 or 384 x 2 per SM)
 
-// Grid barrier of the persistent step loop (device memory, zeroed before
-// each launch).
+// Grid barrier of the persistent step loop (device memory; the counter is
+// zeroed before each launch, the error word when the host has read it).
 struct GridBarrier {
 	uint32_t count;  // arrivals so far: barrier b of the launch is complete at (b + 1) x CTAs
 	uint32_t error;  // set when a wait gave up
@@ -195,7 +195,9 @@ private:
 	size_t synapseKey(uint64_t id) const;
 	void launchStep(bool fullRecord);
 	void launchSteps(unsigned n);
-	void launchRun(unsigned n);
+	void launchRun(unsigned n, bool finalStdp = true, const uint32_t* stim = nullptr, uint32_t nf = 0, uint32_t ni = 0,
+			uint32_t* hostFired = nullptr);
+	uint64_t m_barrierBase = 0;  // the barrier counter's value after the launches so far
 	void flushStdp();
 	bool m_stdpPending = false;  // the last step's STDP accumulation has not run yet
 	void checkBarrier();
