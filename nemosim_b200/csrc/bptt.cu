@@ -67,16 +67,47 @@ __device__ __forceinline__ Real spike_grad(Real x)
 	return Real(0.5) * Real(10) / (q * q);
 }
 
+// Sum over the range [beg, end) of one neuron's synapses of w * x, with x
+// the value term(e) returns (0 when the term does not apply), in G
+// interleaved partial sums so that G terms' loads are in flight at once.
+// The forward pass and the replay call it with the same arguments, so they
+// agree bit for bit.
+constexpr int GATHER = 4;
+
+template<typename Real, typename Term>
+__device__ __forceinline__ Real gather(int beg, int end, Term term)
+{
+	Real sum[GATHER], w[GATHER], x[GATHER];
+#pragma unroll
+	for(int j = 0; j < GATHER; ++j) sum[j] = Real(0);
+	int e = beg;
+	for(; e + GATHER <= end; e += GATHER) {
+#pragma unroll
+		for(int j = 0; j < GATHER; ++j) term(e + j, w[j], x[j]);
+#pragma unroll
+		for(int j = 0; j < GATHER; ++j) sum[j] = fma(w[j], x[j], sum[j]);
+	}
+	for(; e < end; ++e) {
+		term(e, w[0], x[0]);
+		sum[0] = fma(w[0], x[0], sum[0]);
+	}
+#pragma unroll
+	for(int h = GATHER / 2; h > 0; h /= 2) {
+#pragma unroll
+		for(int j = 0; j < h; ++j) sum[j] += sum[j + h];
+	}
+	return sum[0];
+}
+
 // synaptic input of (n, b) at ms t from the stored spikes
 template<typename Real>
 __device__ __forceinline__ Real syn_input(const BpttDev& D, const BpttState<Real>& X, const float* W, int n, int b, int t)
 {
-	Real syn = Real(0);
-	for(int e = D.inStart[n]; e < D.inStart[n + 1]; ++e) {
+	return gather<Real>(D.inStart[n], D.inStart[n + 1], [&](int e, Real& w, Real& x) {
 		const int dl = D.inDelay[e];
-		if(t >= dl) syn = fma((Real) W[D.inSyn[e]], X.S[((size_t) D.inSrc[e] * D.T + (t - dl)) * D.B + b], syn);
-	}
-	return syn;
+		w = (Real) W[D.inSyn[e]];
+		x = t >= dl ? X.S[((size_t) D.inSrc[e] * D.T + (t - dl)) * D.B + b] : Real(0);
+	});
 }
 
 // one Euler sub-step and its reset; returns s
@@ -201,10 +232,11 @@ __global__ void bptt_backward_kernel(BpttDev D, BpttState<Real> X, BpttParams P,
 		X.lamR[n * D.B + b] = lr;
 		lamS = lr;
 	}
-	for(int e = D.outStart[n]; e < D.outStart[n + 1]; ++e) {
+	lamS += gather<Real>(D.outStart[n], D.outStart[n + 1], [&](int e, Real& w, Real& x) {
 		const int tt = t + D.outDelay[e];
-		if(tt < D.T) lamS = fma((Real) P.W[e], X.lamI[((size_t) D.outTgt[e] * D.T + tt) * D.B + b], lamS);
-	}
+		w = (Real) P.W[e];
+		x = tt < D.T ? X.lamI[((size_t) D.outTgt[e] * D.T + tt) * D.B + b] : Real(0);
+	});
 
 	// replay the sub-steps of ms t
 	const Real a = P.a[n], bb = P.b[n], c = P.c[n], d = P.d[n];
