@@ -89,7 +89,7 @@ __device__ __forceinline__ void store_rng(const DevSim& S, uint32_t n, const Neu
 // parameters and state of neuron nl of type T (the plugin layouts of
 // src/nemo/plugins/Izhikevich.h, IF_curr_exp.h, PoissonSource.h)
 // With pre, an Izhikevich neuron's nrand for this step was computed (and its
-// RNG words advanced) by precompute_noise at the end of the previous step.
+// RNG words advanced) by precompute_noise before the update.
 __device__ __forceinline__ void load_neuron(const DevSim& S, const TypeRange& T, uint32_t nl, uint32_t n, NeuronRegs& R,
 		bool pre)
 {
@@ -232,9 +232,9 @@ __device__ __forceinline__ void store_neuron(const DevSim& S, const TypeRange& T
 	}
 }
 
-// nrand of the next step for the Izhikevich neurons [first, last) of a CTA
-// with sigma != 0 (the same draws the update would make, in the same order),
-// for the update's pre flag.
+// nrand of the coming update for the Izhikevich neurons [first, last) of a
+// CTA with sigma != 0 (the same draws the update would make, in the same
+// order), for the update's pre flag.
 __device__ __forceinline__ void precompute_noise(const DevSim& S, uint32_t first, uint32_t last)
 {
 	for(uint32_t n = first + threadIdx.x; n < last; n += blockDim.x) {

@@ -573,8 +573,8 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, uint32_t& target, 
 // barriers, then the STDP accumulation of the last step (so applyStdp may
 // follow directly; its deliveries stay pending for the next step).  CTA c
 // owns the partitions c, c + gridDim.x, ... of P neurons; the pre-phases
-// spread the work lists over all CTAs of the grid.  After each update the
-// CTAs compute the next step's noise while the barrier completes.
+// spread the work lists over all CTAs of the grid.  After each pre-phase
+// the CTAs compute the step's noise while the barrier completes.
 // Identical results to deliver_kernel + update_kernel per step.
 // base: the barrier counter's value when the launch starts.  Without
 // finalStdp the last step's STDP accumulation is left to the next
@@ -600,20 +600,18 @@ run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0
 		const uint32_t ring = (uint32_t) (c % S.R);
 		if(k == 0 && stim) apply_stimulus(S, stim, nf, ni);
 		deliver_range(S, cur ^ 1u, PHASE_DELIVER | PHASE_STDP | PHASE_RESET);
-		if(!grid_barrier(gb, sTarget, sOk)) return;
+		// while the other CTAs finish the pre-phase: this step's noise of
+		// this CTA's neurons (it depends on their RNG words only)
+		grid_arrive(gb, sTarget);
+		for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) precompute_noise(S, p * P, min(S.N, p * P + P));
+		if(!grid_wait(gb, sTarget, sOk)) return;
 		uint32_t* hf = k + 1 == steps ? hostFired : nullptr;
 		for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
-			update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC, k > 0, hf);
+			update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC, true, hf);
 		}
 		__syncthreads();
 		flush_counters(S, ring, sC);
-		// while the other CTAs finish: the next step's noise of this CTA's
-		// neurons (it depends on their RNG words only)
-		grid_arrive(gb, sTarget);
-		if(k + 1 < steps) {
-			for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) precompute_noise(S, p * P, min(S.N, p * P + P));
-		}
-		if(!grid_wait(gb, sTarget, sOk)) return;
+		if(!grid_barrier(gb, sTarget, sOk)) return;
 	}
 	if(steps && finalStdp) {
 		const uint32_t last = (uint32_t) ((cycle0 + steps - 1) & 1);
