@@ -481,3 +481,11 @@ def libm_calibration():
     a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
     _check(lib().nemo_b200_libm_calibration(C.byref(a), C.byref(b), C.byref(c)))
     return a.value, b.value, c.value
+
+
+def libm_verify() -> int:
+    """Arguments (of all 100,663,298 reachable ones) at which the host build
+    of the device's logf/sinf differs from the host libm."""
+    n = C.c_uint64()
+    _check(lib().nemo_b200_libm_verify(C.byref(n)))
+    return n.value

@@ -108,6 +108,7 @@ SIGNATURES = {
     "nemo_b200_neuron_type_count": (C.c_uint, []),
     "nemo_b200_neuron_type_name": (C.c_char_p, [C.c_uint]),
     "nemo_b200_libm_calibration": (st, [C.POINTER(C.c_uint64)] * 3),
+    "nemo_b200_libm_verify": (st, [C.POINTER(C.c_uint64)]),
     "nemo_b200_last_status": (st, []),
     "nemo_b200_bptt_new": (vp, [C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_uint, sz, u32p, u32p, u32p,
                                 C.c_int, C.c_int]),

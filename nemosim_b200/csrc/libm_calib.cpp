@@ -22,7 +22,7 @@ namespace {
 struct Exc { uint32_t key, val; };
 
 void calibrate_range(bool isLog, uint32_t wbegin, uint32_t wend, uint32_t count,
-		std::vector<uint32_t>& bits, uint64_t& flips, std::vector<Exc>& exc)
+		std::vector<uint32_t>& bits, uint64_t& flips, double& near, std::vector<Exc>& exc)
 {
 	for(uint32_t w = wbegin; w < wend; ++w) {
 		uint32_t word = 0;
@@ -46,6 +46,7 @@ void calibrate_range(bool isLog, uint32_t wbegin, uint32_t wend, uint32_t count,
 			if(nb_fbits(libm) != nb_fbits(mine)) {
 				word |= 1u << b;
 				flips++;
+				near = std::max(near, nb_mid_gaps(mine, d));
 				float stepped = nb_step_toward(mine, d);
 				if(nb_fbits(stepped) != nb_fbits(libm)) {
 					exc.push_back(Exc{ (isLog ? 0u : (1u << 31)) | idx, nb_fbits(libm) });
@@ -57,23 +58,26 @@ void calibrate_range(bool isLog, uint32_t wbegin, uint32_t wend, uint32_t count,
 }
 
 void calibrate(bool isLog, uint32_t count, std::vector<uint32_t>& bits, uint64_t& flips,
-		std::vector<Exc>& exc)
+		double& near, std::vector<Exc>& exc)
 {
 	uint32_t nwords = (count + 31) / 32;
 	bits.assign(nwords, 0);
 	unsigned nt = std::max(1u, std::thread::hardware_concurrency());
 	std::vector<std::thread> threads;
 	std::vector<uint64_t> tflips(nt, 0);
+	std::vector<double> tnear(nt, 0.0);
 	std::vector<std::vector<Exc>> texc(nt);
 	uint32_t chunk = (nwords + nt - 1) / nt;
 	for(unsigned t = 0; t < nt; ++t) {
 		uint32_t b = std::min(nwords, t * chunk), e = std::min(nwords, (t + 1) * chunk);
-		threads.emplace_back([&, t, b, e] { calibrate_range(isLog, b, e, count, bits, tflips[t], texc[t]); });
+		threads.emplace_back([&, t, b, e] { calibrate_range(isLog, b, e, count, bits, tflips[t], tnear[t], texc[t]); });
 	}
 	for(auto& th : threads) th.join();
 	flips = 0;
+	near = 0.0;
 	for(unsigned t = 0; t < nt; ++t) {
 		flips += tflips[t];
+		near = std::max(near, tnear[t]);
 		exc.insert(exc.end(), texc[t].begin(), texc[t].end());
 	}
 }
@@ -86,8 +90,8 @@ const CalibTables& libm_calibration()
 	static std::once_flag once;
 	std::call_once(once, [] {
 		std::vector<Exc> exc;
-		calibrate(true, NB_LOG_COUNT, tables.logFlip, tables.logFlips, exc);
-		calibrate(false, NB_SIN_COUNT, tables.sinFlip, tables.sinFlips, exc);
+		calibrate(true, NB_LOG_COUNT, tables.logFlip, tables.logFlips, tables.logNear, exc);
+		calibrate(false, NB_SIN_COUNT, tables.sinFlip, tables.sinFlips, tables.sinNear, exc);
 		std::sort(exc.begin(), exc.end(), [](const Exc& a, const Exc& b) { return a.key < b.key; });
 		for(const Exc& e : exc) {
 			tables.excKey.push_back(e.key);
@@ -95,6 +99,37 @@ const CalibTables& libm_calibration()
 		}
 	});
 	return tables;
+}
+
+uint64_t libm_verify()
+{
+	const LibmCalib c = host_calib_view();
+	unsigned nt = std::max(1u, std::thread::hardware_concurrency());
+	std::vector<uint64_t> bad(nt, 0);
+	std::vector<std::thread> threads;
+	const uint64_t total = (uint64_t) NB_LOG_COUNT + NB_SIN_COUNT;
+	for(unsigned t = 0; t < nt; ++t) {
+		threads.emplace_back([&, t] {
+			for(uint64_t i = t; i < total; i += nt) {
+				float libm, mine;
+				if(i < NB_LOG_COUNT) {
+					float x = (float) i * 0x1p-24f;
+					libm = logf(x);
+					mine = nb_libm_logf(c, x);
+				} else {
+					float fu = nb_sin_value((uint32_t) (i - NB_LOG_COUNT));
+					float a = fu * NB_NRAND_A;
+					libm = sinf(a);
+					mine = nb_libm_sinf(c, fu, a);
+				}
+				bad[t] += nb_fbits(libm) != nb_fbits(mine);
+			}
+		});
+	}
+	for(auto& th : threads) th.join();
+	uint64_t n = 0;
+	for(uint64_t b : bad) n += b;
+	return n;
 }
 
 LibmCalib host_calib_view()
@@ -106,6 +141,8 @@ LibmCalib host_calib_view()
 	c.excKey = t.excKey.data();
 	c.excVal = t.excVal.data();
 	c.nexc = (uint32_t) t.excKey.size();
+	c.logNear = t.logNear;
+	c.sinNear = t.sinNear;
 	return c;
 }
 

@@ -686,6 +686,12 @@ nemo_status_t nemo_b200_libm_calibration(uint64_t* logFlips, uint64_t* sinFlips,
 	});
 }
 
+nemo_status_t nemo_b200_libm_verify(uint64_t* mismatches)
+{
+	NULLCHECK(mismatches);
+	CALL(*mismatches = libm_verify());
+}
+
 nemo_status_t nemo_b200_last_status(void) { return g_lastStatus; }
 
 nemo_b200_bptt_t nemo_b200_bptt_new(unsigned neurons, unsigned trials, unsigned ms, unsigned readout,

@@ -855,6 +855,8 @@ LibmCalib device_calibration(int device)
 	c.excKey = dKey;
 	c.excVal = dVal;
 	c.nexc = (uint32_t) nexc;
+	c.logNear = t.logNear;
+	c.sinNear = t.sinNear;
 	cache[device] = c;
 	return c;
 }

@@ -56,6 +56,14 @@ def test_libm_calibration_is_exact():
         assert np.array_equal(s, s2)
 
 
+def test_libm_emulation_is_exact_at_every_argument():
+    """logf over all 2^24 + 1 values of 1 - b and sinf over all 83,886,081
+    values of a that nrand can produce (src/nemo/RNG.cpp:27-32): the host
+    build of the device functions, with the flip table read only near float
+    rounding midpoints, returns the libm's bits everywhere."""
+    assert nb.libm_verify() == 0
+
+
 def _state_for(u1: int, u2: int) -> np.ndarray:
     """A xorshift128 state whose next two draws are u1 and u2
     (src/nemo/RNG.cpp:9-18): with s0 = 0 the first draw is s3 ^ (s3 >> 19),
