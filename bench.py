@@ -334,23 +334,39 @@ def run_b200(args, rank, world, local):
     per_kernel["apply_kernel"] = {"avg_launch_us": apply_ms * 1e3, "achieved_gbs": apply_gbs,
                                   "alg_bytes_per_launch": ps["plastic_synapses"] * B_APPLY}
 
-    # e2e through the C ABI with host buffers
+    # e2e through the C ABI with host buffers, the calls a C caller makes:
+    # nemo_step once per ms (a one-neuron firing stimulus from host memory,
+    # the fired ids returned in host memory) and nemo_apply_stdp once per
+    # period
+    import ctypes as C
+    L = nb.lib()
     rng = np.random.default_rng(rank)
     ke = max(1, min(args.steps, args.e2e_steps))
     ev0 = sim.step_events()
-    stim = rng.integers(0, args.neurons, size=ke * W).tolist()
+    stim = rng.integers(0, args.neurons, size=ke * W).astype(np.uint32)
+    no_u32, no_f32 = np.zeros(1, np.uint32), np.zeros(1, np.float32)
+    fired, nfired = C.POINTER(C.c_uint)(), C.c_size_t()
+    pf, pn = C.byref(fired), C.byref(nfired)
+    fired_total = 0
     barrier(world)
     t0 = time.perf_counter()
     k = 0
     for _ in range(ke):
         for _ in range(W):
-            sim.step([stim[k]])
+            nb._check(L.nemo_step(sim._h, stim[k:k + 1], 1, no_u32, no_f32, 0, pf, pn))
+            fired_total += nfired.value
             k += 1
-        sim.apply_stdp(1.0)
+        nb._check(L.nemo_apply_stdp(sim._h, 1.0))
     e2e_s = time.perf_counter() - t0
     barrier(world)
     e2e_s = dist_max(e2e_s, world)
     e2e_events = dist_sum(float(sim.step_events() - ev0), world)
+    # the same loop through the Python wrapper (fired ids as a list)
+    t0 = time.perf_counter()
+    for k in range(W):
+        sim.step([int(stim[k])])
+    sim.apply_stdp(1.0)
+    py_step_us = (time.perf_counter() - t0) / W * 1e6
     words = (args.neurons + 31) // 32
 
     cpu = None
@@ -376,7 +392,8 @@ def run_b200(args, rank, world, local):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_events / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 4 * W,
                     "d2h_bytes_per_step": 4 * words * W, "api": "nemo_step + nemo_apply_stdp (C ABI)",
-                    "sim_ms_per_s": ke * W / e2e_s},
+                    "sim_ms_per_s": ke * W / e2e_s, "fired_per_ms": fired_total / (ke * W),
+                    "python_step_us": py_step_us},
             # per period: the persistent loop (or 100 update + deliver launches,
             # plus the graph's cycle-counter kernel), then applyStdp's collect
             # and apply kernels

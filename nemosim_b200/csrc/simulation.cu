@@ -48,6 +48,37 @@ namespace nemo_b200 {
 constexpr uint32_t CHUNK = 128;  // entries per chunk: 4 per lane of a warp
 constexpr uint32_t ILP = CHUNK / 32;
 
+// Chained launches (programmatic dependent launch): deliver_kernel and
+// update_kernel alternate on one stream, each launched while its
+// predecessor still runs.  A chained kernel's CTAs first wait until the
+// previous grid has completed and its writes are visible (a no-op when the
+// kernel was launched without the chaining attribute), then allow the next
+// kernel's launch to begin, so only that launch's latency overlaps, never
+// the work of two steps.
+__device__ __forceinline__ void chain_wait_then_release()
+{
+	asm volatile("griddepcontrol.wait;" ::: "memory");
+	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Launches `kernel` on `st` chained to the stream's previous kernel.
+template<typename... KArgs, typename... Args>
+void launch_chained(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
+		Args... args)
+{
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3(grid);
+	cfg.blockDim = dim3(block);
+	cfg.dynamicSmemBytes = smem;
+	cfg.stream = st;
+	cudaLaunchAttribute attr;
+	attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	attr.val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = &attr;
+	cfg.numAttrs = 1;
+	NB_CUDA(cudaLaunchKernelEx(&cfg, kernel, ((KArgs) args)...));
+}
+
 // Inside a CUDA graph the step's cycle comes from a device counter (the
 // graph is replayed at different cycles): cycle = *cycleDev + offset.
 __device__ __forceinline__ void step_indices(const DevSim& S, uint32_t offset, uint32_t& cur, uint32_t& ring)
@@ -301,6 +332,7 @@ __global__ void __launch_bounds__(1024)
 update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t ring, uint32_t offset, int fromDev,
 		uint32_t* hostFired = nullptr)
 {
+	chain_wait_then_release();
 	if(fromDev) step_indices(S, offset, cur, ring);
 	__shared__ CtaCounters sC;
 	if(threadIdx.x == 0) sC = CtaCounters{ 0, 0, 0, 0, 0, 0, 0 };
@@ -483,6 +515,7 @@ __global__ void __launch_bounds__(STEP_THREADS)
 deliver_kernel(const DevSim S, uint32_t pub, uint32_t what, uint32_t offset, int fromDev,
 		const uint32_t* stim = nullptr, uint32_t nf = 0, uint32_t ni = 0)
 {
+	chain_wait_then_release();
 	if(fromDev) {
 		uint32_t cur, ring;
 		step_indices(S, offset, cur, ring);
@@ -1414,11 +1447,11 @@ void Simulation::launchStep(bool /*fullRecord*/)
 	const uint32_t ring = (uint32_t) (m_cycle % m_dev.R);
 	const unsigned grid = (m_N + m_P - 1) / m_P;
 	timedBegin(K_STDP);
-	deliver_kernel<<<m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream>>>(m_dev, cur ^ 1u,
-			PHASE_DELIVER | PHASE_STDP | PHASE_RESET, 0, 0);
+	launch_chained(deliver_kernel, m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream, m_dev, cur ^ 1u,
+			(uint32_t) (PHASE_DELIVER | PHASE_STDP | PHASE_RESET), 0u, 0, nullptr, 0u, 0u);
 	timedEnd();
 	timedBegin(K_STEP);
-	update_kernel<<<grid, m_T, 0, m_stream>>>(m_dev, m_P, cur, ring, 0, 0);
+	launch_chained(update_kernel, grid, m_T, 0, m_stream, m_dev, m_P, cur, ring, 0u, 0, nullptr);
 	timedEnd();
 	m_cycle++;
 	m_timerSteps++;
@@ -1527,9 +1560,9 @@ void Simulation::buildGraph()
 	cudaGraph_t g;
 	NB_CUDA(cudaStreamBeginCapture(m_stream, cudaStreamCaptureModeThreadLocal));
 	for(unsigned k = 0; k < GRAPH_STEPS; ++k) {
-		deliver_kernel<<<m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream>>>(m_dev, 0,
-				PHASE_DELIVER | PHASE_STDP | PHASE_RESET, k, 1);
-		update_kernel<<<grid, m_T, 0, m_stream>>>(m_dev, m_P, 0, 0, k, 1);
+		launch_chained(deliver_kernel, m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream, m_dev, 0u,
+				(uint32_t) (PHASE_DELIVER | PHASE_STDP | PHASE_RESET), k, 1, nullptr, 0u, 0u);
+		launch_chained(update_kernel, grid, m_T, 0, m_stream, m_dev, m_P, 0u, 0u, k, 1, nullptr);
 	}
 	advance_cycle_kernel<<<1, 1, 0, m_stream>>>(m_dev.cycleDev, GRAPH_STEPS);
 	NB_CUDA(cudaStreamEndCapture(m_stream, &g));
@@ -1591,10 +1624,11 @@ const std::vector<unsigned>& Simulation::step(const unsigned* fstim, size_t nf,
 	// kernel)
 	const uint32_t c = (uint32_t) (m_cycle & 1);
 	const uint32_t ring = (uint32_t) (m_cycle % m_dev.R);
-	deliver_kernel<<<m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream>>>(m_dev, c ^ 1u,
-			PHASE_DELIVER | PHASE_STDP | PHASE_RESET, 0, 0, need ? m_dStimMapped : nullptr, (uint32_t) nf,
-			(uint32_t) cur.size());
-	update_kernel<<<(m_N + m_P - 1) / m_P, m_T, 0, m_stream>>>(m_dev, m_P, c, ring, 0, 0, m_dFiredMapped);
+	launch_chained(deliver_kernel, m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream, m_dev, c ^ 1u,
+			(uint32_t) (PHASE_DELIVER | PHASE_STDP | PHASE_RESET), 0u, 0,
+			need ? (const uint32_t*) m_dStimMapped : nullptr, (uint32_t) nf, (uint32_t) cur.size());
+	launch_chained(update_kernel, (m_N + m_P - 1) / m_P, m_T, 0, m_stream, m_dev, m_P, c, ring, 0u, 0,
+			m_dFiredMapped);
 	m_cycle++;
 	m_timerSteps++;
 	m_stdpPending = true;
