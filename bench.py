@@ -19,8 +19,10 @@ wall second.
   value    device-resident run through the native run loop (CUDA events)
   e2e      the reference-facing C ABI, nemo_step once per ms with host
            buffers: a one-neuron firing stimulus goes host->device and the
-           fired bit-vector comes back every step (src/examples/common.cpp
-           --fstim), plus nemo_apply_stdp every 100 ms
+           fired neuron ids come back every step (src/examples/common.cpp
+           --fstim), plus nemo_apply_stdp every 100 ms; nemo_step runs
+           through the resident step loop (--no-resident: two kernel
+           launches per call)
   roofline the step loop's algorithmic bytes per launch / its measured
            average duration (CUDA events around each launch), against the
            measured HBM copy bandwidth; the persistent loop runs one period
@@ -338,22 +340,33 @@ def run_b200(args, rank, world, local):
     # nemo_step once per ms (a one-neuron firing stimulus from host memory,
     # the fired ids returned in host memory) and nemo_apply_stdp once per
     # period
+    # (bound here with plain pointer arguments, as C passes them)
     import ctypes as C
     L = nb.lib()
+    c_step = C.CDLL(nb.library_path()).nemo_step
+    c_step.restype = C.c_int
+    c_step.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                       C.c_void_p]
     rng = np.random.default_rng(rank)
     ke = max(1, min(args.steps, args.e2e_steps))
     ev0 = sim.step_events()
     stim = rng.integers(0, args.neurons, size=ke * W).astype(np.uint32)
     no_u32, no_f32 = np.zeros(1, np.uint32), np.zeros(1, np.float32)
     fired, nfired = C.POINTER(C.c_uint)(), C.c_size_t()
-    pf, pn = C.byref(fired), C.byref(nfired)
+    h, pf, pn = sim._h, C.addressof(fired), C.addressof(nfired)
+    p_stim, p_i, p_v = stim.ctypes.data, no_u32.ctypes.data, no_f32.ctypes.data
     fired_total = 0
+    resident = persistent and not args.no_resident
+    if not resident:
+        sim.set_resident_step(0)
     barrier(world)
     t0 = time.perf_counter()
     k = 0
     for _ in range(ke):
         for _ in range(W):
-            nb._check(L.nemo_step(sim._h, stim[k:k + 1], 1, no_u32, no_f32, 0, pf, pn))
+            rc = c_step(h, p_stim + 4 * k, 1, p_i, p_v, 0, pf, pn)
+            if rc:
+                nb._check(rc)
             fired_total += nfired.value
             k += 1
         nb._check(L.nemo_apply_stdp(sim._h, 1.0))
@@ -390,8 +403,13 @@ def run_b200(args, rank, world, local):
                          "kernel": dominant, "alg_bytes_per_launch": alg_bytes,
                          "avg_launch_us": step_ms * 1e3, "kernels": per_kernel},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_events / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 4 * W,
-                    "d2h_bytes_per_step": 4 * words * W, "api": "nemo_step + nemo_apply_stdp (C ABI)",
+            # nemo_step through the resident loop: per ms a 4-byte stimulus and
+            # a 16-byte request in, the fired ids and a 16-byte reply out (two
+            # launches: the fired bit-vector out instead)
+            "e2e": {"value": e2e_events / e2e_s, "unit": UNIT, "h2d_bytes_per_step": (4 + 16) * W,
+                    "d2h_bytes_per_step": (round(4 * fired_total / ke) + 16 * W) if resident else 4 * words * W,
+                    "api": "nemo_step + nemo_apply_stdp (C ABI)",
+                    "step_path": "resident step loop" if resident else "two launches per nemo_step",
                     "sim_ms_per_s": ke * W / e2e_s, "fired_per_ms": fired_total / (ke * W),
                     "python_step_us": py_step_us},
             # per period: the persistent loop (or 100 update + deliver launches,
@@ -567,6 +585,8 @@ def main():
     ap.add_argument("--neurons", type=int, default=NEURONS)
     ap.add_argument("--window", type=int, default=WINDOW_MS, help=argparse.SUPPRESS)
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-resident", action="store_true",
+                    help="nemo_step with two kernel launches per call instead of the resident step loop")
     ap.add_argument("--cpu-ms", type=int, default=200)
     ap.add_argument("--cpu-warm-ms", type=int, default=50)
     ap.add_argument("--no-cpu", action="store_true")

@@ -281,9 +281,21 @@ NEMO_B200_API nemo_status_t nemo_b200_set_graphs(nemo_simulation_t, int on);
  * separated by grid barriers (on), or two launches per step (off).  The
  * default is on, except for networks with more than two neurons per thread
  * of the persistent loop's co-resident CTAs (large batches), where one
- * launch per phase over the whole network is faster.  nemo_step always uses
- * two launches.  Results are identical. */
+ * launch per phase over the whole network is faster.  With it off, nemo_step
+ * uses two launches per call.  Results are identical. */
 NEMO_B200_API nemo_status_t nemo_b200_set_persistent(nemo_simulation_t, int on);
+/* nemo_step's resident step loop (no counterpart in the reference, whose
+ * step runs on the host, src/nemo/cpu/Simulation.cpp:94-111): when the
+ * persistent loop is in use (nemo_b200_set_persistent), nemo_step hands
+ * each step to a cooperative launch that stays on the GPU between calls,
+ * polling a flag in mapped host memory, instead of launching kernels and
+ * synchronising a stream per call.  The loop ends after idle_us
+ * microseconds without a nemo_step call (at most 100000; the next call
+ * launches it again), and before any other call on the simulation does
+ * GPU work.  While it is resident it occupies every SM, so other work on
+ * the GPU waits up to idle_us for it.  0 turns it off (two launches per
+ * nemo_step).  Default 200.  Results are identical either way. */
+NEMO_B200_API nemo_status_t nemo_b200_set_resident_step(nemo_simulation_t, unsigned idle_us);
 /* Statistics of the last nemo_b200_run: its device time in ms (CUDA events
  * on the simulation's stream), and per kernel kind (0 = update kernel and
  * 1 = deliver kernel of the two-launch step, 2 = applyStdp, 3 = persistent

@@ -369,6 +369,12 @@ class Simulation:
         launches per step."""
         _check(lib().nemo_b200_set_persistent(self._h, int(on)))
 
+    def set_resident_step(self, idle_us: int = 200):
+        """step() through a step loop that stays resident on the GPU between
+        calls and ends after `idle_us` microseconds without one (an
+        extension; 200 by default, 0 = two kernel launches per step)."""
+        _check(lib().nemo_b200_set_resident_step(self._h, int(idle_us)))
+
     def run_stats(self) -> dict:
         """Statistics of the last run() (an extension): device ms, per-kernel
         ms and launches (when profiling; "step" and "stdp" are the update and

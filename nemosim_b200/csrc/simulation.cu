@@ -4,6 +4,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include "kernels.cuh"
@@ -61,9 +62,10 @@ __device__ __forceinline__ void chain_wait_then_release()
 	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
-// Launches `kernel` on `st` chained to the stream's previous kernel.
+// Launches `kernel` on `st` chained to the stream's previous kernel.  A
+// launch error is reported as for <<<...>>> (cudaGetLastError), not thrown.
 template<typename... KArgs, typename... Args>
-void launch_chained(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
+cudaError_t launch_chained(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
 		Args... args)
 {
 	cudaLaunchConfig_t cfg = {};
@@ -76,7 +78,7 @@ void launch_chained(void (*kernel)(KArgs...), unsigned grid, unsigned block, siz
 	attr.val.programmaticStreamSerializationAllowed = 1;
 	cfg.attrs = &attr;
 	cfg.numAttrs = 1;
-	NB_CUDA(cudaLaunchKernelEx(&cfg, kernel, ((KArgs) args)...));
+	return cudaLaunchKernelEx(&cfg, kernel, ((KArgs) args)...);
 }
 
 // Inside a CUDA graph the step's cycle comes from a device counter (the
@@ -502,9 +504,14 @@ __device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uin
 // ni values (distinct indices), for the update that follows.
 __device__ __forceinline__ void apply_stimulus(const DevSim& S, const uint32_t* stim, uint32_t nf, uint32_t ni)
 {
+	// stim is host memory that the resident step loop re-reads each step:
+	// load it past the caches
 	for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < max(nf, ni); i += gridDim.x * blockDim.x) {
-		if(i < nf) atomicOr(&S.fstim[stim[i] >> 5], 1u << (stim[i] & 31));
-		if(i < ni) S.curExt[stim[nf + i]] = __uint_as_float(stim[nf + ni + i]);
+		if(i < nf) {
+			const uint32_t l = __ldcv(stim + i);
+			atomicOr(&S.fstim[l >> 5], 1u << (l & 31));
+		}
+		if(i < ni) S.curExt[__ldcv(stim + nf + i)] = __uint_as_float(__ldcv(stim + nf + ni + i));
 	}
 }
 
@@ -614,6 +621,31 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, uint32_t& target, 
 // pre-phase, as after a two-launch step.  stim (the first step's stimulus,
 // apply_stimulus) and hostFired (the last step's fired words) serve
 // nemo_step.
+// One step of the persistent loop at cycle c (the pre-phase, the noise in
+// the shadow of its barrier, the update), ending at a grid barrier; false
+// when a barrier wait gave up.
+__device__ __forceinline__ bool persistent_step(const DevSim& S, uint32_t P, unsigned long long c, GridBarrier* gb,
+		uint32_t& sTarget, uint32_t& sOk, CtaCounters& sC, const uint32_t* stim, uint32_t nf, uint32_t ni,
+		uint32_t* hostFired)
+{
+	const uint32_t nparts = (S.N + P - 1) / P;
+	const uint32_t cur = (uint32_t) (c & 1);
+	const uint32_t ring = (uint32_t) (c % S.R);
+	if(stim) apply_stimulus(S, stim, nf, ni);
+	deliver_range(S, cur ^ 1u, PHASE_DELIVER | PHASE_STDP | PHASE_RESET);
+	// while the other CTAs finish the pre-phase: this step's noise of this
+	// CTA's neurons (it depends on their RNG words only)
+	grid_arrive(gb, sTarget);
+	for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) precompute_noise(S, p * P, min(S.N, p * P + P));
+	if(!grid_wait(gb, sTarget, sOk)) return false;
+	for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
+		update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC, true, hostFired);
+	}
+	__syncthreads();
+	flush_counters(S, ring, sC);
+	return grid_barrier(gb, sTarget, sOk);
+}
+
 __global__ void __launch_bounds__(RUN_THREADS, 1)
 run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0, GridBarrier* gb, uint32_t base,
 		int finalStdp, const uint32_t* stim, uint32_t nf, uint32_t ni, uint32_t* hostFired)
@@ -626,31 +658,250 @@ run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0
 		sOk = 1;
 	}
 	__syncthreads();
-	const uint32_t nparts = (S.N + P - 1) / P;
 	for(uint32_t k = 0; k < steps; ++k) {
-		const unsigned long long c = cycle0 + k;
-		const uint32_t cur = (uint32_t) (c & 1);
-		const uint32_t ring = (uint32_t) (c % S.R);
-		if(k == 0 && stim) apply_stimulus(S, stim, nf, ni);
-		deliver_range(S, cur ^ 1u, PHASE_DELIVER | PHASE_STDP | PHASE_RESET);
-		// while the other CTAs finish the pre-phase: this step's noise of
-		// this CTA's neurons (it depends on their RNG words only)
-		grid_arrive(gb, sTarget);
-		for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) precompute_noise(S, p * P, min(S.N, p * P + P));
-		if(!grid_wait(gb, sTarget, sOk)) return;
-		uint32_t* hf = k + 1 == steps ? hostFired : nullptr;
-		for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
-			update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC, true, hf);
+		if(!persistent_step(S, P, cycle0 + k, gb, sTarget, sOk, sC, k == 0 ? stim : nullptr, nf, ni,
+				k + 1 == steps ? hostFired : nullptr)) {
+			return;
 		}
-		__syncthreads();
-		flush_counters(S, ring, sC);
-		if(!grid_barrier(gb, sTarget, sOk)) return;
 	}
 	if(steps && finalStdp) {
 		const uint32_t last = (uint32_t) ((cycle0 + steps - 1) & 1);
 		deliver_range(S, last, PHASE_STDP);
 		if(!grid_barrier(gb, sTarget, sOk)) return;
 		if(blockIdx.x == 0 && threadIdx.x == 0) S.stdpWork.count[last] = 0;
+	}
+}
+
+// The resident step loop of nemo_step: one cooperative launch that stays on
+// the GPU between nemo_step calls and runs one step per request, so that a
+// call costs a step and a round trip through host memory instead of kernel
+// launches and a stream synchronisation.
+//
+// The host writes the step's stimulus (stim, mapped host memory), its sizes
+// and then the request's sequence number to ctl->go.  Thread 0 of CTA 0
+// polls ctl->go and broadcasts the request (its sequence number) through
+// gb->cmd, which the other CTAs poll.  After the step's final barrier CTA 0
+// writes the step's fired neurons as global ids to hostIds (mapped), their
+// number and the step's synaptic events to ctl, and then the sequence
+// number to ctl->done.  The loop ends when the host asks it to stop
+// (go = the next sequence number | SERVE_STOP) or after idleNs nanoseconds
+// without a request (the host then launches it again for the next call);
+// a wait that gives up ends it with the barrier's error word set.  Step k
+// runs cycle cycle0 + k, exactly as run_kernel's step.
+constexpr uint32_t SERVE_POLL_LIMIT = 1u << 26;  // bounds the idle wait even without the timer
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+	unsigned long long t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+
+
+__device__ __forceinline__ unsigned long long ld_relaxed_sys_u64(const unsigned long long* p)
+{
+	unsigned long long v;
+	asm volatile("ld.relaxed.sys.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+	return v;
+}
+
+__device__ __forceinline__ void st_release_sys(uint32_t* p, uint32_t v)
+{
+	asm volatile("st.release.sys.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+
+// n words from device memory (just written by other CTAs: read from L2)
+// to host memory by the threads of one CTA, 16 bytes a thread where both
+// ends are 16-byte aligned
+__device__ __forceinline__ void copy_words_to_host(const uint32_t* src, uint32_t* dst, uint32_t n)
+{
+	uint32_t i0 = 0;
+	if((((uintptr_t) src | (uintptr_t) dst) & 15u) == 0) {
+		const uint4* s4 = reinterpret_cast<const uint4*>(src);
+		uint4* d4 = reinterpret_cast<uint4*>(dst);
+		for(uint32_t i = threadIdx.x; i < n / 4; i += blockDim.x) d4[i] = __ldcg(s4 + i);
+		i0 = n & ~3u;
+	}
+	for(uint32_t i = i0 + threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldcg(src + i);
+}
+
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v)
+{
+	asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+
+// The fired neurons of a step (words: its fired bit-vector) as global ids in
+// ascending local index (setFiring, src/nemo/cpu/Simulation.cpp:200-208),
+// by the threads of one CTA: each thread takes a run of words, a CTA-wide
+// scan of their counts places its ids, which are staged in shared memory
+// (or, beyond SERVE_IDS_SMEM of them, in S.firedIds) and then stored to host
+// memory in consecutive words per warp.  Returns the count.
+constexpr uint32_t SERVE_IDS_SMEM = 4096;
+
+__device__ uint32_t fired_ids_to_host(const DevSim& S, const uint32_t* words, uint32_t* host)
+{
+	__shared__ uint32_t sIds[SERVE_IDS_SMEM];
+	__shared__ uint32_t sWarp[32];
+	__shared__ uint32_t sTotal;
+	const uint32_t T = blockDim.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
+	const uint32_t per = (S.W + T - 1) / T;
+	const uint32_t w0 = min(S.W, t * per), w1 = min(S.W, w0 + per);
+	// up to WREG words per thread stay in registers for the second pass
+	constexpr uint32_t WREG = 8;
+	uint32_t wr[WREG];
+	uint32_t n = 0;
+#pragma unroll
+	for(uint32_t j = 0; j < WREG; ++j) {
+		wr[j] = w0 + j < w1 ? __ldcg(words + w0 + j) : 0u;
+		n += __popc(wr[j]);
+	}
+	for(uint32_t w = w0 + WREG; w < w1; ++w) n += __popc(__ldcg(words + w));
+	const uint32_t incl = warp_inclusive_scan(n);
+	if(lane == 31) sWarp[warp] = incl;
+	__syncthreads();
+	if(warp == 0) {
+		const uint32_t x = lane < T / 32 ? sWarp[lane] : 0u;
+		const uint32_t xi = warp_inclusive_scan(x);
+		if(lane < T / 32) sWarp[lane] = xi - x;
+		if(lane == 31) sTotal = xi;
+	}
+	__syncthreads();
+	const uint32_t total = sTotal;
+	uint32_t pos = sWarp[warp] + incl - n;
+	if(total <= SERVE_IDS_SMEM) {
+#pragma unroll
+		for(uint32_t j = 0; j < WREG; ++j) {
+			uint32_t bits = wr[j];
+			while(bits) {
+				const uint32_t b = __ffs(bits) - 1;
+				bits &= bits - 1;
+				sIds[pos++] = (w0 + j) * 32 + b;
+			}
+		}
+		for(uint32_t w = w0 + WREG; w < w1; ++w) {
+			uint32_t bits = __ldcg(words + w);
+			while(bits) {
+				const uint32_t b = __ffs(bits) - 1;
+				bits &= bits - 1;
+				sIds[pos++] = w * 32 + b;
+			}
+		}
+		__syncthreads();
+		if(S.l2gIdentity) {
+			for(uint32_t i = t; i < total; i += T) host[i] = sIds[i];
+		} else {
+			for(uint32_t i = t; i < total; i += T) host[i] = __ldg(S.l2g + sIds[i]);
+		}
+		return total;
+	}
+	for(uint32_t w = w0; w < w1; ++w) {
+		uint32_t bits = __ldcg(words + w);
+		while(bits) {
+			const uint32_t b = __ffs(bits) - 1;
+			bits &= bits - 1;
+			S.firedIds[pos++] = S.l2g[w * 32 + b];
+		}
+	}
+	__syncthreads();
+	copy_words_to_host(S.firedIds, host, total);
+	return total;
+}
+
+// A CTA other than 0 waits for CTA 0's broadcast of request `want` (1) or
+// of the end of the loop (0); gives up like a grid barrier.
+__device__ __forceinline__ uint32_t wait_request(GridBarrier* gb, uint32_t want, uint32_t& ok)
+{
+	__shared__ uint32_t sCmd;
+	if(threadIdx.x == 0) {
+		uint32_t r = 0, polls = 0;
+		for(;;) {
+			const uint32_t v = ld_acquire(&gb->cmd);
+			if(v == want) {
+				r = 1;
+				break;
+			}
+			if(v == (want | SERVE_STOP)) break;
+			if(++polls > BARRIER_SPIN_LIMIT || ld_acquire(&gb->error)) {
+				atomicExch(&gb->error, 1u);
+				ok = 0;
+				break;
+			}
+			__nanosleep(20);
+		}
+		__threadfence();
+		sCmd = r;
+	}
+	__syncthreads();
+	return sCmd;
+}
+
+__global__ void __launch_bounds__(RUN_THREADS, 1)
+serve_kernel(const DevSim S, uint32_t P, unsigned long long cycle0, GridBarrier* gb, ServeCtl* ctl, uint32_t seq0,
+		const uint32_t* stim, uint32_t* hostIds, unsigned long long idleNs)
+{
+	__shared__ CtaCounters sC;
+	__shared__ uint32_t sTarget, sOk;
+	if(threadIdx.x == 0) {
+		sC = CtaCounters{ 0, 0, 0, 0, 0, 0, 0 };
+		sTarget = 0;
+		sOk = 1;
+	}
+	__syncthreads();
+	__shared__ uint32_t sOp;
+	uint32_t want = seq0;
+	for(unsigned long long k = 0;; ++k, want = serve_next(want)) {
+		const unsigned long long c = cycle0 + k;
+		const uint32_t ring = (uint32_t) (c % S.R);
+		// CTA 0 takes the request from the host and broadcasts it (the
+		// other CTAs finished the last step at its final barrier)
+		uint32_t op;
+		if(blockIdx.x == 0) {
+			if(threadIdx.x == 0) {
+				op = 0;
+				const unsigned long long t0 = global_ns();
+				for(uint32_t polls = 0; polls < SERVE_POLL_LIMIT; ++polls) {
+					// both words in one round trip
+					const unsigned long long a = ld_relaxed_sys_u64(&ctl->req[0]);
+					const unsigned long long b = ld_relaxed_sys_u64(&ctl->req[1]);
+					if((uint32_t) (a >> 32) == want && (uint32_t) (b >> 32) == want) {
+						// the stimulus the host wrote before the request
+						asm volatile("fence.acq_rel.sys;" ::: "memory");
+						gb->nf = (uint32_t) a;
+						gb->ni = (uint32_t) b;
+						S.eventCount[ring] = 0;
+						op = 1;
+						break;
+					}
+					if((uint32_t) (a >> 32) == (want | SERVE_STOP) || global_ns() - t0 > idleNs) break;
+					if((polls & 1023u) == 1023u && ld_acquire(&gb->error)) break;
+					__nanosleep(32);
+				}
+				__threadfence();
+				st_release(&gb->cmd, op ? want : want | SERVE_STOP);
+				sOp = op;
+			}
+			__syncthreads();
+			op = sOp;
+		} else {
+			op = wait_request(gb, want, sOk);
+		}
+		if(!op) return;
+		const uint32_t nf = *(volatile uint32_t*) &gb->nf;
+		const uint32_t ni = *(volatile uint32_t*) &gb->ni;
+		if(!persistent_step(S, P, c, gb, sTarget, sOk, sC, nf + ni ? stim : nullptr, nf, ni, nullptr)) return;
+		// CTA 0 answers: the step's fired ids and events (after the step's
+		// final barrier every CTA's words and counts are in place)
+		if(blockIdx.x == 0) {
+			const uint32_t n = fired_ids_to_host(S, S.firedRing + (size_t) ring * S.W, hostIds);
+			__syncthreads();
+			if(threadIdx.x == 0) {
+				ctl->fired = n;
+				ctl->events = *(volatile unsigned long long*) &S.eventCount[ring];
+				// a release at system scope: the host that sees done sees
+				// every store the CTA made before the __syncthreads
+				st_release_sys(&ctl->done, want);
+			}
+		}
 	}
 }
 
@@ -789,6 +1040,7 @@ nemo_status_t Simulation::stepNoAlloc(const unsigned* fstim, size_t nf, const un
 	}
 	if(cudaSetDevice(m_device) != cudaSuccess) return NEMO_CUDA_ERROR;
 	if(m_device < 0 || m_device >= NO_ALLOC_MAX_DEVICES) return NEMO_API_UNSUPPORTED;
+	stopServe();
 	uint32_t*& stim = g_noAllocStimAddr[m_device];
 	if(!stim) {
 		// once per device, with the device current
@@ -1308,6 +1560,16 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	S.touchedBits = dalloc<uint32_t>(S.W);
 	S.curExt = dalloc<float>(N);
 	S.slot = dalloc<ulonglong2>(N);
+	S.l2g = dalloc<uint32_t>(N);
+	NB_CUDA(cudaMemcpy(S.l2g, m_l2g.data(), (size_t) N * 4, cudaMemcpyHostToDevice));
+	S.l2gIdentity = 1;
+	for(size_t i = 0; i < N; ++i) {
+		if(m_l2g[i] != i) {
+			S.l2gIdentity = 0;
+			break;
+		}
+	}
+	S.firedIds = dalloc<uint32_t>(N);
 	S.cycleDev = dalloc<unsigned long long>(1);
 	NB_CUDA(cudaMallocHost(&m_hCycle, 8));
 	S.R = (uint32_t) std::max<size_t>(16, std::min<size_t>(1024, (64u << 20) / ((size_t) S.W * 4)));
@@ -1318,6 +1580,10 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	NB_CUDA(cudaMallocHost(&m_hFired, (size_t) S.R * S.W * 4));
 	NB_CUDA(cudaHostAlloc(&m_hFiredMapped, (size_t) S.W * 4, cudaHostAllocMapped));
 	NB_CUDA(cudaHostGetDevicePointer(&m_dFiredMapped, m_hFiredMapped, 0));
+	NB_CUDA(cudaHostAlloc(&m_hServe, sizeof(ServeCtl), cudaHostAllocMapped));
+	memset(m_hServe, 0, sizeof(ServeCtl));
+	NB_CUDA(cudaHostGetDevicePointer(&m_dServe, m_hServe, 0));
+	NB_CUDA(cudaEventCreateWithFlags(&m_serveEnd, cudaEventDisableTiming));
 
 	if(needCalib) S.calib = device_calibration(m_device);
 	NB_CUDA(cudaDeviceGetAttribute(&m_sms, cudaDevAttrMultiProcessorCount, m_device));
@@ -1360,6 +1626,7 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 Simulation::~Simulation()
 {
 	cudaSetDevice(m_device);
+	stopServe();
 	if(m_stream) cudaStreamSynchronize(m_stream);
 	for(void* p : m_allocs) cudaFree(p);
 	if(m_graph) cudaGraphExecDestroy(m_graph);
@@ -1368,6 +1635,9 @@ Simulation::~Simulation()
 	if(m_hFired) cudaFreeHost(m_hFired);
 	if(m_hFiredMapped) cudaFreeHost(m_hFiredMapped);
 	if(m_hStim) cudaFreeHost(m_hStim);
+	if(m_hServe) cudaFreeHost(m_hServe);
+	if(m_hFiredIds) cudaFreeHost(m_hFiredIds);
+	if(m_serveEnd) cudaEventDestroy(m_serveEnd);
 	if(m_ev0) cudaEventDestroy(m_ev0);
 	if(m_ev1) cudaEventDestroy(m_ev1);
 	for(cudaEvent_t e : m_evPool) cudaEventDestroy(e);
@@ -1376,6 +1646,7 @@ Simulation::~Simulation()
 
 void Simulation::sync()
 {
+	stopServe();
 	NB_CUDA(cudaStreamSynchronize(m_stream));
 }
 
@@ -1415,13 +1686,18 @@ void Simulation::timedEnd()
 
 unsigned Simulation::runGridFor(uint32_t T) const
 {
-	int perSm = 0;
+	// run_kernel and serve_kernel (the resident loop of nemo_step) share
+	// the launch shape
+	int perSm = 0, perSmServe = 0;
 	NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, run_kernel, (int) T, m_dev.recentBytes));
+	NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmServe, serve_kernel, (int) T, m_dev.recentBytes));
+	perSm = std::min(perSm, perSmServe);
 	return perSm > 0 ? (unsigned) perSm * (unsigned) m_sms : 0u;
 }
 
 void Simulation::setLaunch(uint32_t P, uint32_t T)
 {
+	stopServe();
 	if(persistentActive()) {
 		// any multiple of 32 neurons per partition; 64 to RUN_THREADS threads
 		m_runP = std::max<uint32_t>(32, (std::min<uint32_t>(P, 1u << 30) + 31) & ~31u);
@@ -1443,6 +1719,7 @@ void Simulation::setLaunch(uint32_t P, uint32_t T)
 
 void Simulation::launchStep(bool /*fullRecord*/)
 {
+	stopServe();
 	const uint32_t cur = (uint32_t) (m_cycle & 1);
 	const uint32_t ring = (uint32_t) (m_cycle % m_dev.R);
 	const unsigned grid = (m_N + m_P - 1) / m_P;
@@ -1462,6 +1739,7 @@ void Simulation::launchStep(bool /*fullRecord*/)
 // would otherwise run (before applyStdp, that must be now)
 void Simulation::flushStdp()
 {
+	stopServe();
 	if(!m_stdpPending) return;
 	m_stdpPending = false;
 	if(!m_dev.stdp || m_cycle == 0) return;
@@ -1487,9 +1765,11 @@ void Simulation::launchRun(unsigned n, bool finalStdp, const uint32_t* stim, uin
 	// the barrier counter runs on across launches; restart it well before
 	// it could wrap
 	const uint64_t arrivals = (uint64_t) grid * (2ull * n + (finalStdp ? 1 : 0));
-	if(m_barrierBase + arrivals >= (1ull << 31)) {
+	stopServe();
+	if(m_barrierStale || m_barrierBase + arrivals >= (1ull << 31)) {
 		NB_CUDA(cudaMemsetAsync(&m_barrier->count, 0, 4, m_stream));
 		m_barrierBase = 0;
+		m_barrierStale = false;
 	}
 	uint32_t base = (uint32_t) m_barrierBase;
 	int fin = finalStdp ? 1 : 0;
@@ -1517,6 +1797,7 @@ void Simulation::checkBarrier()
 		*m_hBarrierError = 0;
 		NB_CUDA(cudaMemset(m_barrier, 0, sizeof(GridBarrier)));
 		m_barrierBase = 0;
+		m_barrierStale = false;
 		NB_THROW(NEMO_CUDA_ERROR, "persistent step loop: a grid barrier wait timed out");
 	}
 }
@@ -1526,6 +1807,7 @@ void Simulation::checkBarrier()
 // from a device cycle counter) and single launches for the rest
 void Simulation::launchSteps(unsigned n)
 {
+	stopServe();
 	if(usePersistent && m_runGrid && n > 1) {
 		launchRun(n);
 		return;
@@ -1576,6 +1858,114 @@ void Simulation::buildGraph()
 	m_graphT = m_T;
 }
 
+// ---------------------------------------------------------------------------
+// the resident step loop of nemo_step (serve_kernel)
+
+void Simulation::setResidentIdle(unsigned us)
+{
+	if(us > RESIDENT_IDLE_MAX_US) {
+		NB_THROW(NEMO_INVALID_INPUT, "resident step loop idle time %u us is above the limit of %u us", us,
+				RESIDENT_IDLE_MAX_US);
+	}
+	// a running loop keeps the idle time it was launched with
+	stopServe();
+	residentIdleUs = us;
+}
+
+bool Simulation::residentAvailable() const
+{
+	return residentIdleUs != 0 && persistentActive() && m_barrier != nullptr;
+}
+
+// Launches the loop at the current cycle for the next request; its barrier
+// counter starts from zero and is left at a value the host does not track.
+void Simulation::launchServe()
+{
+	if(!m_hFiredIds) {
+		NB_CUDA(cudaHostAlloc(&m_hFiredIds, (size_t) m_N * 4, cudaHostAllocMapped));
+		NB_CUDA(cudaHostGetDevicePointer(&m_dFiredIdsMapped, m_hFiredIds, 0));
+	}
+	// the barrier counter and the request word (count and cmd, adjacent)
+	NB_CUDA(cudaMemsetAsync(&m_barrier->count, 0, 8, m_stream));
+	m_barrierBase = 0;
+	DevSim dev = m_dev;
+	uint32_t P = m_runP;
+	unsigned long long c0 = m_cycle;
+	GridBarrier* gb = m_barrier;
+	ServeCtl* ctl = m_dServe;
+	uint32_t seq0 = m_serveSeq;
+	const uint32_t* stim = m_dStimMapped;
+	uint32_t* hf = m_dFiredIdsMapped;
+	unsigned long long idleNs = (unsigned long long) residentIdleUs * 1000ull;
+	const unsigned grid = (unsigned) std::min<uint64_t>(m_runGrid, std::max<uint64_t>(1, (m_N + P - 1) / P));
+	void* args[] = { &dev, &P, &c0, &gb, &ctl, &seq0, &stim, &hf, &idleNs };
+	NB_CUDA(cudaLaunchCooperativeKernel((const void*) serve_kernel, dim3(grid), dim3(m_runT), args, m_dev.recentBytes,
+			m_stream));
+	NB_CUDA(cudaEventRecord(m_serveEnd, m_stream));
+	m_serving = true;
+	m_barrierUsed = true;
+	m_barrierStale = true;
+}
+
+// Asks a running loop to end; work queued on the stream afterwards runs
+// once it has.  The request consumes a sequence number, so that a loop
+// still polling when the next request is written (to a new launch, queued
+// behind it) matches neither and only waits out its idle time.  Neither
+// allocates nor throws.
+void Simulation::stopServe() noexcept
+{
+	if(!m_serving) return;
+	m_serving = false;
+	std::atomic_thread_fence(std::memory_order_seq_cst);
+	reinterpret_cast<volatile ServeCtl*>(m_hServe)->req[0] = (unsigned long long) (m_serveSeq | SERVE_STOP) << 32;
+	std::atomic_thread_fence(std::memory_order_seq_cst);
+	m_serveSeq = serve_next(m_serveSeq);
+}
+
+// One step through the resident loop: the stimulus is already in m_hStim.
+void Simulation::stepResident(uint32_t nf, uint32_t ni)
+{
+	volatile ServeCtl* c = reinterpret_cast<volatile ServeCtl*>(m_hServe);
+	const uint32_t want = m_serveSeq;
+	// the stimulus (m_hStim) is in place before the request
+	std::atomic_thread_fence(std::memory_order_seq_cst);
+	c->req[1] = (unsigned long long) want << 32 | ni;
+	c->req[0] = (unsigned long long) want << 32 | nf;
+	std::atomic_thread_fence(std::memory_order_seq_cst);
+	if(!m_serving) launchServe();
+	const auto t0 = std::chrono::steady_clock::now();
+	for(uint32_t polls = 1;; ++polls) {
+		if(c->done == want) break;
+		if((polls & 63u) == 0) {
+			const cudaError_t q = cudaEventQuery(m_serveEnd);
+			if(q == cudaSuccess) {
+				if(c->done == want) break;
+				// the loop ended before this request: it was idle for too
+				// long (launch it again), or a grid barrier gave up
+				// (checkBarrier throws)
+				m_serving = false;
+				checkBarrier();
+				launchServe();
+			} else if(q != cudaErrorNotReady) {
+				NB_CUDA(q);
+			}
+			if(std::chrono::steady_clock::now() - t0 > std::chrono::seconds(RESIDENT_REPLY_LIMIT_S)) {
+				NB_THROW(NEMO_CUDA_ERROR, "resident step loop: no reply within %u s", RESIDENT_REPLY_LIMIT_S);
+			}
+		}
+#if defined(__x86_64__)
+		__builtin_ia32_pause();
+#endif
+	}
+	std::atomic_thread_fence(std::memory_order_seq_cst);
+	m_fired.assign(m_hFiredIds, m_hFiredIds + c->fired);
+	stepEvents += c->events;
+	m_serveSeq = serve_next(m_serveSeq);
+	m_cycle++;
+	m_timerSteps++;
+	m_stdpPending = true;
+}
+
 // One step with host buffers: the stimulus is staged in mapped host memory
 // that the pre-phase kernel reads, and the update writes the fired
 // bit-vector words to mapped host memory, so no copy is queued.
@@ -1605,7 +1995,8 @@ const std::vector<unsigned>& Simulation::step(const unsigned* fstim, size_t nf,
 	}
 	const size_t need = nf + 2 * cur.size();
 	if(need > m_stimCap) {
-		// no kernel reads the old buffer: every step() ends synchronised
+		// the resident step loop holds the old buffer's address: end it
+		sync();
 		if(m_hStim) cudaFreeHost(m_hStim);
 		m_hStim = nullptr;
 		m_stimCap = std::max<size_t>(need, 1024);
@@ -1619,9 +2010,14 @@ const std::vector<unsigned>& Simulation::step(const unsigned* fstim, size_t nf,
 			memcpy(&m_hStim[nf + cur.size() + i], &cur[i].second, 4);
 		}
 	}
+	if(residentAvailable()) {
+		stepResident((uint32_t) nf, (uint32_t) cur.size());
+		return m_fired;
+	}
 	// two launches (a one-step cooperative launch of the persistent loop is
 	// slower here: its launch and grid barriers cost more than a second
 	// kernel)
+	stopServe();
 	const uint32_t c = (uint32_t) (m_cycle & 1);
 	const uint32_t ring = (uint32_t) (m_cycle % m_dev.R);
 	launch_chained(deliver_kernel, m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream, m_dev, c ^ 1u,
@@ -1634,8 +2030,13 @@ const std::vector<unsigned>& Simulation::step(const unsigned* fstim, size_t nf,
 	m_stdpPending = true;
 	sync();
 	NB_CUDA(cudaGetLastError());
-	// fired neurons in ascending local index, as global ids
-	// (setFiring, src/nemo/cpu/Simulation.cpp:200-208)
+	return collectFired();
+}
+
+// the fired words of the last step() (mapped host memory) as global ids in
+// ascending local index (setFiring, src/nemo/cpu/Simulation.cpp:200-208)
+const std::vector<unsigned>& Simulation::collectFired()
+{
 	m_fired.clear();
 	for(uint32_t w = 0; w < m_dev.W; ++w) {
 		uint32_t bits = m_hFiredMapped[w];
@@ -1652,6 +2053,7 @@ const std::vector<unsigned>& Simulation::step(const unsigned* fstim, size_t nf,
 
 void Simulation::applyStdpDevice(int32_t R)
 {
+	stopServe();
 	flushStdp();
 	const bool fullPassDone = m_weightsClamped;
 	timedBegin(K_APPLY);

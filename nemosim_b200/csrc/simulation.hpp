@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #include <chrono>
@@ -24,8 +25,34 @@ constexpr unsigned RUN_THREADS = 768;    // largest block of the persistent step
 // zeroed before each launch, the error word when the host has read it).
 struct GridBarrier {
 	uint32_t count;  // arrivals so far: barrier b of the launch is complete at (b + 1) x CTAs
+	uint32_t cmd;    // resident step loop: the request being run (| stop flag: end)
 	uint32_t error;  // set when a wait gave up
-	uint32_t pad[2];
+	uint32_t nf, ni; // resident step loop: the request's stimulus sizes
+	uint32_t pad[3];
+};
+static_assert(offsetof(GridBarrier, cmd) == 4, "one memset restarts count and cmd");
+
+// go | SERVE_STOP asks the resident step loop to end; sequence numbers run
+// from 1 to 2^31 - 1 and wrap to 1.
+constexpr uint32_t SERVE_STOP = 0x80000000u;
+__host__ __device__ inline uint32_t serve_next(uint32_t seq) { return seq == 0x7fffffffu ? 1u : seq + 1u; }
+constexpr unsigned RESIDENT_IDLE_MAX_US = 100000;  // the grid barrier's wait limit is far longer
+constexpr unsigned RESIDENT_REPLY_LIMIT_S = 20;
+
+// Requests to the resident step loop of nemo_step (mapped host memory):
+// the host writes the stimulus sizes and then go; the device writes done.
+// A request is two 8-byte words, each written and read whole: the
+// sequence number in the high half of both, the stimulus sizes (nf firing
+// indices, ni (index, current) pairs) in the low halves; it is complete
+// when both carry the same sequence number.  req[0] = (seq | stop flag)
+// << 32 ends the loop.
+struct ServeCtl {
+	unsigned long long req[2];
+	uint32_t pad0[28];
+	uint32_t done;     // sequence number of the last completed step
+	uint32_t fired;    // its fired neurons (global ids in the fired-id buffer)
+	unsigned long long events;  // its synaptic events
+	uint32_t pad1[28];
 };
 
 // STDP accumulation first tests a source against a shared-memory copy of the
@@ -89,6 +116,9 @@ struct DevSim {
 	const uint16_t* dEnd16;
 	const uint32_t* dEnd32;
 	uint32_t* firedRing;      // [R][W] fired bit-vector per step
+	uint32_t* l2g;            // [N] global id of each neuron
+	uint32_t* firedIds;       // [N] staging of a step's fired global ids
+	uint32_t l2gIdentity;     // l2g[i] == i for every neuron
 	uint32_t* firedCount;     // [R]
 	unsigned long long* eventCount; // [R] synaptic events (out-degree of fired neurons)
 	unsigned long long* stdpCount;  // [R] incoming plastic synapses walked by STDP
@@ -174,6 +204,12 @@ public:
 	uint32_t threads() const { return persistentActive() ? m_runT : m_T; }
 	void setLaunch(uint32_t P, uint32_t T);
 	bool persistentActive() const { return usePersistent && m_runGrid != 0; }
+	// step() keeps the persistent loop resident on the GPU between calls
+	// (serve_kernel) and ends it after this many microseconds without a
+	// call (at most RESIDENT_IDLE_MAX_US); 0: two kernel launches per step
+	unsigned residentIdleUs = 200;
+	bool residentAvailable() const;
+	void setResidentIdle(unsigned us);
 	// time candidate launch shapes on trial steps from a saved copy of the
 	// simulation state, restore it, and keep the fastest; returns its time
 	// per step in microseconds
@@ -199,6 +235,17 @@ private:
 			uint32_t* hostFired = nullptr);
 	uint64_t m_barrierBase = 0;  // the barrier counter's value after the launches so far
 	void flushStdp();
+	// resident step loop
+	void launchServe();
+	void stopServe() noexcept;
+	void stepResident(uint32_t nf, uint32_t ni);
+	const std::vector<unsigned>& collectFired();
+	ServeCtl* m_hServe = nullptr;   // mapped pinned
+	ServeCtl* m_dServe = nullptr;
+	cudaEvent_t m_serveEnd = nullptr;  // recorded after each launch of the loop
+	bool m_serving = false;            // a launch of the loop may still be running
+	uint32_t m_serveSeq = 1;           // sequence number of the next request
+	bool m_barrierStale = false;       // the barrier counter must restart from zero
 	bool m_stdpPending = false;  // the last step's STDP accumulation has not run yet
 	void checkBarrier();
 	GridBarrier* m_barrier = nullptr;
@@ -263,6 +310,8 @@ private:
 	uint32_t* m_dStimMapped = nullptr;
 	size_t m_stimCap = 0;
 	uint32_t* m_hFiredMapped = nullptr;  // mapped pinned [W]: step()'s fired words
+	uint32_t* m_hFiredIds = nullptr;     // mapped pinned [N]: the resident loop's fired ids
+	uint32_t* m_dFiredIdsMapped = nullptr;
 	uint32_t* m_dFiredMapped = nullptr;
 	std::vector<uint32_t> m_stepScratch;
 	std::vector<std::pair<uint32_t, float>> m_stepCurrents;
