@@ -329,10 +329,11 @@ NEMO_B200_API const char* nemo_b200_neuron_type_name(unsigned i);
 NEMO_B200_API nemo_status_t nemo_b200_libm_calibration(uint64_t* log_flips, uint64_t* sin_flips,
 		uint64_t* exceptions);
 /* Test helper: evaluates the host build of the device's logf/sinf (flip
- * table, exception list and the midpoint-distance skip included) at every
- * reachable argument, 100,663,298 of them, against the host libm on all host
- * threads; *mismatches receives how many differ (0 when the emulation is
- * exact).  A few seconds. */
+ * table, exception list and the midpoint-distance skip included; the flip
+ * word read on demand and fetched up front) at every reachable argument,
+ * 100,663,298 of them, against the host libm on all host threads;
+ * *mismatches receives how many differ (0 when the emulation is exact).  A
+ * few seconds. */
 NEMO_B200_API nemo_status_t nemo_b200_libm_verify(uint64_t* mismatches);
 /* Status of the most recent call, including the constructors
  * (nemo_new_simulation and the like) that report failure only by returning

@@ -243,10 +243,11 @@ __device__ __forceinline__ void precompute_noise(const DevSim& S, uint32_t first
 		const TypeRange& T = S.types[k];
 		if(T.kind != KIND_IZHIKEVICH) continue;
 		const uint32_t nl = n - T.base;
-		if(T.param[4 * T.n + nl] == 0.0f) continue;
+		// the RNG words load alongside sigma
 		NeuronRegs R;
 		load_rng(S, n, R);
-		S.noise[n] = nb_nrand(S.calib, R.r[0], R.r[1], R.r[2], R.r[3]);
+		if(T.param[4 * T.n + nl] == 0.0f) continue;
+		S.noise[n] = nb_nrand<true>(S.calib, R.r[0], R.r[1], R.r[2], R.r[3]);
 		store_rng(S, n, R);
 	}
 }

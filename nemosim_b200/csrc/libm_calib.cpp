@@ -111,18 +111,21 @@ uint64_t libm_verify()
 	for(unsigned t = 0; t < nt; ++t) {
 		threads.emplace_back([&, t] {
 			for(uint64_t i = t; i < total; i += nt) {
-				float libm, mine;
+				// both forms: the flip word read lazily and fetched up front
+				float libm, mine, early;
 				if(i < NB_LOG_COUNT) {
 					float x = (float) i * 0x1p-24f;
 					libm = logf(x);
 					mine = nb_libm_logf(c, x);
+					early = nb_libm_logf_w(c, x, c.logFlip[nb_log_index(x) >> 5]);
 				} else {
 					float fu = nb_sin_value((uint32_t) (i - NB_LOG_COUNT));
 					float a = fu * NB_NRAND_A;
 					libm = sinf(a);
 					mine = nb_libm_sinf(c, fu, a);
+					early = nb_libm_sinf_w(c, fu, a, c.sinFlip[nb_sin_index(fu) >> 5]);
 				}
-				bad[t] += nb_fbits(libm) != nb_fbits(mine);
+				bad[t] += nb_fbits(libm) != nb_fbits(mine) || nb_fbits(libm) != nb_fbits(early);
 			}
 		});
 	}

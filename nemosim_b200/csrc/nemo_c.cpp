@@ -753,7 +753,7 @@ nemo_status_t nemo_b200_bptt_backward(nemo_b200_bptt_t h, const float* w, const 
 float nemo_b200_host_nrand(unsigned state[4])
 {
 	LibmCalib c = host_calib_view();
-	return nb_nrand(c, state[0], state[1], state[2], state[3]);
+	return nb_nrand<true>(c, state[0], state[1], state[2], state[3]);
 }
 
 } // extern "C"

@@ -242,11 +242,31 @@ NB_HD bool nb_exception(const LibmCalib& c, uint32_t key, float* out)
 	return false;
 }
 
-// logf(x) for x = 1 - b as produced by nrand (a multiple of 2^-24 in [0, 1])
+// the flip-table index of logf's argument x = 1 - b
+NB_HD uint32_t nb_log_index(float x) { return (uint32_t) NB_FMUL(x, 16777216.0f); }
+
+// logf(x) for x = 1 - b as produced by nrand (a multiple of 2^-24 in [0, 1]);
+// word: the flip-table word holding the argument's bit (fetched by the
+// caller, so that the load overlaps the evaluation)
+NB_HD float nb_libm_logf_w(const LibmCalib& c, float x, uint32_t word)
+{
+	if(x == 0.0f) return nb_bitsf(0xff800000u); // -inf
+	uint32_t idx = nb_log_index(x);
+	double d = nb_log_d((double) x);
+	float f = NB_D2F(d);
+	if(nb_near_mid(f, d, c.logNear) && ((word >> (idx & 31)) & 1u)) {
+		float e;
+		if(c.nexc && nb_exception(c, idx, &e)) return e;
+		f = nb_step_toward(f, d);
+	}
+	return f;
+}
+
+// as nb_libm_logf_w, reading the flip table only where the bit may be set
 NB_HD float nb_libm_logf(const LibmCalib& c, float x)
 {
 	if(x == 0.0f) return nb_bitsf(0xff800000u); // -inf
-	uint32_t idx = (uint32_t) NB_FMUL(x, 16777216.0f);
+	uint32_t idx = nb_log_index(x);
 	double d = nb_log_d((double) x);
 	float f = NB_D2F(d);
 	if(nb_near_mid(f, d, c.logNear) && nb_bit(c.logFlip, idx)) {
@@ -257,7 +277,21 @@ NB_HD float nb_libm_logf(const LibmCalib& c, float x)
 	return f;
 }
 
-// sinf(a) for a = float(u) * NB_NRAND_A; fu = float(u)
+// sinf(a) for a = float(u) * NB_NRAND_A; fu = float(u); word as for logf
+NB_HD float nb_libm_sinf_w(const LibmCalib& c, float fu, float a, uint32_t word)
+{
+	uint32_t idx = nb_sin_index(fu);
+	double d = nb_sin_d((double) a);
+	float f = NB_D2F(d);
+	if(nb_near_mid(f, d, c.sinNear) && ((word >> (idx & 31)) & 1u)) {
+		float e;
+		if(c.nexc && nb_exception(c, (1u << 31) | idx, &e)) return e;
+		f = nb_step_toward(f, d);
+	}
+	return f;
+}
+
+// as nb_libm_sinf_w, reading the flip table only where the bit may be set
 NB_HD float nb_libm_sinf(const LibmCalib& c, float fu, float a)
 {
 	uint32_t idx = nb_sin_index(fu);
@@ -282,7 +316,10 @@ NB_HD uint32_t nb_urand(uint32_t& s0, uint32_t& s1, uint32_t& s2, uint32_t& s3)
 	return s3;
 }
 
-// nrand of src/nemo/RNG.cpp:25-33 with the host libm reproduced
+// nrand of src/nemo/RNG.cpp:25-33 with the host libm reproduced.  EARLY
+// fetches both flip-table words before the evaluations (shorter latency,
+// more registers); the result is the same.
+template<bool EARLY = false>
 NB_HD float nb_nrand(const LibmCalib& c, uint32_t& s0, uint32_t& s1, uint32_t& s2, uint32_t& s3)
 {
 	float fu1 = NB_U2F(nb_urand(s0, s1, s2, s3));
@@ -290,13 +327,23 @@ NB_HD float nb_nrand(const LibmCalib& c, uint32_t& s0, uint32_t& s1, uint32_t& s
 	float fu2 = NB_U2F(nb_urand(s0, s1, s2, s3));
 	float b = NB_FMUL(fu2, NB_NRAND_B);
 	float x = NB_FSUB(1.0f, b);
-	float l = nb_libm_logf(c, x);
+	float l, s;
+	if(EARLY) {
+		// both flip-table words depend only on the draws
+		const uint32_t lw = c.logFlip[nb_log_index(x) >> 5];
+		const uint32_t sw = c.sinFlip[nb_sin_index(fu1) >> 5];
+		l = nb_libm_logf_w(c, x, lw);
+		s = nb_libm_sinf_w(c, fu1, a, sw);
+	} else {
+		l = nb_libm_logf(c, x);
+		s = nb_libm_sinf(c, fu1, a);
+	}
 #ifdef __CUDA_ARCH__
 	float r = __fsqrt_rn(__fmul_rn(-2.0f, l));
-	return __fmul_rn(nb_libm_sinf(c, fu1, a), r);
+	return __fmul_rn(s, r);
 #else
 	float r = __builtin_sqrtf(-2.0f * l);
-	return nb_libm_sinf(c, fu1, a) * r;
+	return s * r;
 #endif
 }
 

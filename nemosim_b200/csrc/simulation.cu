@@ -533,11 +533,12 @@ deliver_kernel(const DevSim S, uint32_t pub, uint32_t what, uint32_t offset, int
 }
 
 // Grid-wide barrier of the persistent kernel (all CTAs co-resident: it is
-// launched cooperatively).  Thread 0 of each CTA makes the CTA's writes
-// visible (the fence after the CTA barrier), arrives on a launch-wide
-// counter with a release reduction and polls the counter until every CTA
-// has arrived at this barrier: barrier b is complete when the counter
-// reaches (b + 1) x gridDim.x.  A wait gives up after BARRIER_SPIN_LIMIT
+// launched cooperatively).  After a CTA barrier, thread 0 of each CTA
+// arrives on a launch-wide counter with a release reduction (which makes
+// the writes the CTA made before its barrier visible with it) and polls the
+// counter with acquire loads until every CTA has arrived at this barrier;
+// a CTA barrier then passes the acquire on to the CTA's other threads.
+// Barrier b is complete when the counter reaches (b + 1) x gridDim.x.  A wait gives up after BARRIER_SPIN_LIMIT
 // polls (seconds; a phase takes microseconds): it sets the error word, which
 // makes every CTA leave the step loop at its next barrier, and the host
 // reports the error.
@@ -563,7 +564,6 @@ __device__ __forceinline__ void grid_arrive(GridBarrier* gb, uint32_t& target)
 	__syncthreads();
 	if(threadIdx.x == 0) {
 		target += gridDim.x;
-		__threadfence();
 		red_release_add(&gb->count, 1u);
 	}
 }
@@ -580,7 +580,6 @@ __device__ __forceinline__ bool grid_wait(GridBarrier* gb, uint32_t& target, uin
 			}
 			__nanosleep(20);
 		}
-		__threadfence();
 	}
 	__syncthreads();
 	return ok != 0;
@@ -591,7 +590,6 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, uint32_t& target, 
 	__syncthreads();
 	if(threadIdx.x == 0) {
 		target += gridDim.x;
-		__threadfence();
 		red_release_add(&gb->count, 1u);
 		uint32_t polls = 0;
 		while(ld_acquire(&gb->count) < target) {
@@ -602,7 +600,6 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, uint32_t& target, 
 			}
 			__nanosleep(20);
 		}
-		__threadfence();
 	}
 	__syncthreads();
 	return ok != 0;
@@ -828,7 +825,6 @@ __device__ __forceinline__ uint32_t wait_request(GridBarrier* gb, uint32_t want,
 			}
 			__nanosleep(20);
 		}
-		__threadfence();
 		sCmd = r;
 	}
 	__syncthreads();
@@ -876,7 +872,6 @@ serve_kernel(const DevSim S, uint32_t P, unsigned long long cycle0, GridBarrier*
 					if((polls & 1023u) == 1023u && ld_acquire(&gb->error)) break;
 					__nanosleep(32);
 				}
-				__threadfence();
 				st_release(&gb->cmd, op ? want : want | SERVE_STOP);
 				sOp = op;
 			}
