@@ -232,6 +232,52 @@ __device__ __forceinline__ void store_neuron(const DevSim& S, const TypeRange& T
 	}
 }
 
+// Staging of precompute_noise's inputs in shared memory: each thread copies
+// the RNG words and sigma of neuron first + threadIdx.x (an Izhikevich
+// neuron) with asynchronous copies that complete while the pre-phase runs
+// (a CTA with at most NOISE_STAGE neurons of one partition).
+constexpr uint32_t NOISE_STAGE = RUN_THREADS;
+
+__device__ __forceinline__ void cp_async4(void* dst, const void* src)
+{
+	const uint32_t d = (uint32_t) __cvta_generic_to_shared(dst);
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void stage_noise_inputs(const DevSim& S, uint32_t first, uint32_t last, uint32_t* sRng,
+		float* sSigma)
+{
+	const uint32_t n = first + threadIdx.x;
+	if(n < last) {
+		uint32_t k = 0;
+		while(k + 1 < S.ntypes && n >= S.types[k + 1].base) ++k;
+		const TypeRange& T = S.types[k];
+		if(T.kind == KIND_IZHIKEVICH) {
+			cp_async4(sSigma + threadIdx.x, T.param + 4 * T.n + (n - T.base));
+#pragma unroll
+			for(uint32_t j = 0; j < 4; ++j) cp_async4(sRng + j * NOISE_STAGE + threadIdx.x, S.rng + j * S.N + n);
+		}
+	}
+	asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// precompute_noise from the staged inputs (after cp.async.wait_all and a
+// CTA barrier)
+__device__ __forceinline__ void precompute_noise_staged(const DevSim& S, uint32_t first, uint32_t last,
+		const uint32_t* sRng, const float* sSigma)
+{
+	const uint32_t n = first + threadIdx.x;
+	if(n >= last) return;
+	uint32_t k = 0;
+	while(k + 1 < S.ntypes && n >= S.types[k + 1].base) ++k;
+	if(S.types[k].kind != KIND_IZHIKEVICH || sSigma[threadIdx.x] == 0.0f) return;
+	NeuronRegs R;
+#pragma unroll
+	for(uint32_t j = 0; j < 4; ++j) R.r[j] = sRng[j * NOISE_STAGE + threadIdx.x];
+	S.noise[n] = nb_nrand<true>(S.calib, R.r[0], R.r[1], R.r[2], R.r[3]);
+	store_rng(S, n, R);
+}
+
 // nrand of the coming update for the Izhikevich neurons [first, last) of a
 // CTA with sigma != 0 (the same draws the update would make, in the same
 // order), for the update's pre flag.

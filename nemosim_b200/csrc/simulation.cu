@@ -568,11 +568,16 @@ __device__ __forceinline__ void grid_arrive(GridBarrier* gb, uint32_t& target)
 	}
 }
 
+// The counter is compared with its target by signed difference, so that it
+// may wrap: a resident step loop runs for as long as it is used (at 285 CTAs
+// and two barriers a step, 2^32 arrivals are 7.5M steps).
+__device__ __forceinline__ bool reached(uint32_t value, uint32_t target) { return (int32_t) (value - target) >= 0; }
+
 __device__ __forceinline__ bool grid_wait(GridBarrier* gb, uint32_t& target, uint32_t& ok)
 {
 	if(threadIdx.x == 0) {
 		uint32_t polls = 0;
-		while(ld_acquire(&gb->count) < target) {
+		while(!reached(ld_acquire(&gb->count), target)) {
 			if(++polls > BARRIER_SPIN_LIMIT || ld_acquire(&gb->error)) {
 				atomicExch(&gb->error, 1u);
 				ok = 0;
@@ -592,7 +597,7 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, uint32_t& target, 
 		target += gridDim.x;
 		red_release_add(&gb->count, 1u);
 		uint32_t polls = 0;
-		while(ld_acquire(&gb->count) < target) {
+		while(!reached(ld_acquire(&gb->count), target)) {
 			if(++polls > BARRIER_SPIN_LIMIT || ld_acquire(&gb->error)) {
 				atomicExch(&gb->error, 1u);
 				ok = 0;
@@ -625,15 +630,30 @@ __device__ __forceinline__ bool persistent_step(const DevSim& S, uint32_t P, uns
 		uint32_t& sTarget, uint32_t& sOk, CtaCounters& sC, const uint32_t* stim, uint32_t nf, uint32_t ni,
 		uint32_t* hostFired)
 {
+	__shared__ uint32_t sRng[4 * NOISE_STAGE];
+	__shared__ float sSigma[NOISE_STAGE];
 	const uint32_t nparts = (S.N + P - 1) / P;
 	const uint32_t cur = (uint32_t) (c & 1);
 	const uint32_t ring = (uint32_t) (c % S.R);
+	// one partition of at most one neuron per thread: its noise inputs are
+	// copied to shared memory while the pre-phase runs
+	const bool staged = nparts <= gridDim.x && P <= blockDim.x && P <= NOISE_STAGE;
+	if(staged && blockIdx.x < nparts) {
+		stage_noise_inputs(S, blockIdx.x * P, min(S.N, blockIdx.x * P + P), sRng, sSigma);
+	}
 	if(stim) apply_stimulus(S, stim, nf, ni);
 	deliver_range(S, cur ^ 1u, PHASE_DELIVER | PHASE_STDP | PHASE_RESET);
+	if(staged) asm volatile("cp.async.wait_all;" ::: "memory");
 	// while the other CTAs finish the pre-phase: this step's noise of this
 	// CTA's neurons (it depends on their RNG words only)
 	grid_arrive(gb, sTarget);
-	for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) precompute_noise(S, p * P, min(S.N, p * P + P));
+	if(staged) {
+		if(blockIdx.x < nparts) {
+			precompute_noise_staged(S, blockIdx.x * P, min(S.N, blockIdx.x * P + P), sRng, sSigma);
+		}
+	} else {
+		for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) precompute_noise(S, p * P, min(S.N, p * P + P));
+	}
 	if(!grid_wait(gb, sTarget, sOk)) return false;
 	for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
 		update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC, true, hostFired);
