@@ -463,10 +463,15 @@ __device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uin
 		S.stdpWork.count[pub ^ 1u] = 0;
 	}
 	const uint64_t* hist = S.hist + (size_t) pub * S.N;
-	// CTAs [0, gs) take the STDP list, [gs, gridDim.x) the deliveries
+	// CTAs [0, gs) take the STDP list, [gs, gridDim.x) the deliveries, in
+	// proportion to their work: an STDP entry costs about STDP_ENTRY_COST
+	// delivery entries (measured per CTA at 100k x 1000: with a weight of 2
+	// the STDP CTAs took 12 us and the delivery CTAs 8 us)
+	constexpr unsigned long long STDP_ENTRY_COST = 3;
 	uint32_t gs = ns ? gridDim.x : 0u;
 	if(nd && ns) {
-		gs = (uint32_t) ((unsigned long long) gridDim.x * 2ull * ns / ((unsigned long long) nd + 2ull * ns));
+		gs = (uint32_t) ((unsigned long long) gridDim.x * STDP_ENTRY_COST * ns
+				/ ((unsigned long long) nd + STDP_ENTRY_COST * ns));
 		gs = max(1u, min(gridDim.x - 1u, gs));
 		if(gridDim.x == 1) gs = 0;  // one CTA: it does both, deliveries first
 	}
