@@ -330,8 +330,9 @@ NEMO_B200_API nemo_status_t nemo_b200_libm_calibration(uint64_t* log_flips, uint
 		uint64_t* exceptions);
 /* Test helper: evaluates the host build of the device's logf/sinf (flip
  * table, exception list and the midpoint-distance skip included; the flip
- * word read on demand and fetched up front) at every reachable argument,
- * 100,663,298 of them, against the host libm on all host threads;
+ * word read on demand and fetched up front), and reads the result tables
+ * the two-launch update uses, at every reachable argument, 100,663,298 of
+ * them, against the host libm on all host threads;
  * *mismatches receives how many differ (0 when the emulation is exact).  A
  * few seconds. */
 NEMO_B200_API nemo_status_t nemo_b200_libm_verify(uint64_t* mismatches);

@@ -130,7 +130,12 @@ __device__ __forceinline__ bool update_izhikevich(const LibmCalib& calib, Neuron
 	const float a = R.p[0], b = R.p[1], sigma = R.p[4];
 	float I = __fadd_rn(__fadd_rn(cE, cI), ext);
 	if(sigma != 0.0f) {
-		const float z = R.pre ? R.noise : nb_nrand(calib, R.r[0], R.r[1], R.r[2], R.r[3]);
+		// the update's own draw (two-launch step: many neurons per thread,
+		// bound by instruction issue) reads the libm results from the
+		// tables; precompute_noise (one neuron per thread in the shadow of a
+		// barrier, bound by latency) evaluates them, which is faster there
+		// and keeps the tables out of L2.  Both give the same bits.
+		const float z = R.pre ? R.noise : nb_nrand_table(calib, R.r[0], R.r[1], R.r[2], R.r[3]);
 		I = __fadd_rn(I, __fmul_rn(sigma, z));
 	}
 	float u = R.x[0], v = R.x[1];

@@ -22,7 +22,7 @@ namespace {
 struct Exc { uint32_t key, val; };
 
 void calibrate_range(bool isLog, uint32_t wbegin, uint32_t wend, uint32_t count,
-		std::vector<uint32_t>& bits, uint64_t& flips, double& near, std::vector<Exc>& exc)
+		std::vector<uint32_t>& bits, uint64_t& flips, double& near, std::vector<Exc>& exc, float* vals)
 {
 	for(uint32_t w = wbegin; w < wend; ++w) {
 		uint32_t word = 0;
@@ -33,13 +33,15 @@ void calibrate_range(bool isLog, uint32_t wbegin, uint32_t wend, uint32_t count,
 			double d;
 			if(isLog) {
 				float x = (float) idx * 0x1p-24f;
-				if(x == 0.0f) continue; // special-cased on the device
 				libm = logf(x);
+				vals[idx] = libm;
+				if(x == 0.0f) continue; // special-cased by the emulation
 				d = nb_log_d((double) x);
 			} else {
 				float fu = nb_sin_value(idx);
 				float a = fu * NB_NRAND_A;
 				libm = sinf(a);
+				vals[idx] = libm;
 				d = nb_sin_d((double) a);
 			}
 			mine = (float) d;
@@ -58,10 +60,11 @@ void calibrate_range(bool isLog, uint32_t wbegin, uint32_t wend, uint32_t count,
 }
 
 void calibrate(bool isLog, uint32_t count, std::vector<uint32_t>& bits, uint64_t& flips,
-		double& near, std::vector<Exc>& exc)
+		double& near, std::vector<Exc>& exc, std::vector<float>& vals)
 {
 	uint32_t nwords = (count + 31) / 32;
 	bits.assign(nwords, 0);
+	vals.assign(count, 0.0f);
 	unsigned nt = std::max(1u, std::thread::hardware_concurrency());
 	std::vector<std::thread> threads;
 	std::vector<uint64_t> tflips(nt, 0);
@@ -70,7 +73,7 @@ void calibrate(bool isLog, uint32_t count, std::vector<uint32_t>& bits, uint64_t
 	uint32_t chunk = (nwords + nt - 1) / nt;
 	for(unsigned t = 0; t < nt; ++t) {
 		uint32_t b = std::min(nwords, t * chunk), e = std::min(nwords, (t + 1) * chunk);
-		threads.emplace_back([&, t, b, e] { calibrate_range(isLog, b, e, count, bits, tflips[t], tnear[t], texc[t]); });
+		threads.emplace_back([&, t, b, e] { calibrate_range(isLog, b, e, count, bits, tflips[t], tnear[t], texc[t], vals.data()); });
 	}
 	for(auto& th : threads) th.join();
 	flips = 0;
@@ -90,8 +93,8 @@ const CalibTables& libm_calibration()
 	static std::once_flag once;
 	std::call_once(once, [] {
 		std::vector<Exc> exc;
-		calibrate(true, NB_LOG_COUNT, tables.logFlip, tables.logFlips, tables.logNear, exc);
-		calibrate(false, NB_SIN_COUNT, tables.sinFlip, tables.sinFlips, tables.sinNear, exc);
+		calibrate(true, NB_LOG_COUNT, tables.logFlip, tables.logFlips, tables.logNear, exc, tables.logVal);
+		calibrate(false, NB_SIN_COUNT, tables.sinFlip, tables.sinFlips, tables.sinNear, exc, tables.sinVal);
 		std::sort(exc.begin(), exc.end(), [](const Exc& a, const Exc& b) { return a.key < b.key; });
 		for(const Exc& e : exc) {
 			tables.excKey.push_back(e.key);
@@ -111,21 +114,25 @@ uint64_t libm_verify()
 	for(unsigned t = 0; t < nt; ++t) {
 		threads.emplace_back([&, t] {
 			for(uint64_t i = t; i < total; i += nt) {
-				// both forms: the flip word read lazily and fetched up front
-				float libm, mine, early;
+				// both forms: the flip word read lazily and fetched up front;
+				// and the result table at the index nb_nrand_table uses
+				float libm, mine, early, table;
 				if(i < NB_LOG_COUNT) {
 					float x = (float) i * 0x1p-24f;
 					libm = logf(x);
 					mine = nb_libm_logf(c, x);
 					early = nb_libm_logf_w(c, x, c.logFlip[nb_log_index(x) >> 5]);
+					table = c.logVal[nb_log_index(x)];
 				} else {
 					float fu = nb_sin_value((uint32_t) (i - NB_LOG_COUNT));
 					float a = fu * NB_NRAND_A;
 					libm = sinf(a);
 					mine = nb_libm_sinf(c, fu, a);
 					early = nb_libm_sinf_w(c, fu, a, c.sinFlip[nb_sin_index(fu) >> 5]);
+					table = c.sinVal[nb_sin_index(fu)];
 				}
-				bad[t] += nb_fbits(libm) != nb_fbits(mine) || nb_fbits(libm) != nb_fbits(early);
+				bad[t] += nb_fbits(libm) != nb_fbits(mine) || nb_fbits(libm) != nb_fbits(early)
+						|| nb_fbits(libm) != nb_fbits(table);
 			}
 		});
 	}
@@ -146,6 +153,8 @@ LibmCalib host_calib_view()
 	c.nexc = (uint32_t) t.excKey.size();
 	c.logNear = t.logNear;
 	c.sinNear = t.sinNear;
+	c.logVal = t.logVal.data();
+	c.sinVal = t.sinVal.data();
 	return c;
 }
 

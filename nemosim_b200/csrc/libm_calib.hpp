@@ -15,6 +15,7 @@ struct CalibTables {
 	std::vector<uint32_t> excKey, excVal;    // arguments a one-ulp step cannot fix
 	uint64_t logFlips = 0, sinFlips = 0;
 	double logNear = 0.5, sinNear = 0.5;     // see LibmCalib
+	std::vector<float> logVal, sinVal;       // the host libm's result at every reachable argument
 };
 
 // Computed once per process against the host libm (thread-safe).

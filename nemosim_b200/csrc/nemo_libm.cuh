@@ -200,6 +200,10 @@ struct LibmCalib {
 	uint32_t nexc;
 	// largest nb_mid_gaps of any flipped argument (0.5 reads every argument)
 	double logNear, sinNear;
+	// the host libm's logf and sinf at every reachable argument, by index
+	// (NB_LOG_COUNT and NB_SIN_COUNT floats)
+	const float* logVal;
+	const float* sinVal;
 };
 
 // f = float(d) and its neighbour toward d bound the interval holding d;
@@ -338,6 +342,27 @@ NB_HD float nb_nrand(const LibmCalib& c, uint32_t& s0, uint32_t& s1, uint32_t& s
 		l = nb_libm_logf(c, x);
 		s = nb_libm_sinf(c, fu1, a);
 	}
+#ifdef __CUDA_ARCH__
+	float r = __fsqrt_rn(__fmul_rn(-2.0f, l));
+	return __fmul_rn(s, r);
+#else
+	float r = __builtin_sqrtf(-2.0f * l);
+	return s * r;
+#endif
+}
+
+// nrand of src/nemo/RNG.cpp:25-33 reading the host libm's logf and sinf
+// results from the calibration tables (both arguments come from finite
+// sets, indexed as for the flip tables): two loads instead of the
+// evaluations, the same bits as nb_nrand.
+NB_HD float nb_nrand_table(const LibmCalib& c, uint32_t& s0, uint32_t& s1, uint32_t& s2, uint32_t& s3)
+{
+	float fu1 = NB_U2F(nb_urand(s0, s1, s2, s3));
+	float fu2 = NB_U2F(nb_urand(s0, s1, s2, s3));
+	float b = NB_FMUL(fu2, NB_NRAND_B);
+	float x = NB_FSUB(1.0f, b);
+	const float l = c.logVal[nb_log_index(x)];
+	const float s = c.sinVal[nb_sin_index(fu1)];
 #ifdef __CUDA_ARCH__
 	float r = __fsqrt_rn(__fmul_rn(-2.0f, l));
 	return __fmul_rn(s, r);

@@ -1154,6 +1154,12 @@ LibmCalib device_calibration(int device)
 		NB_CUDA(cudaMemcpy(dKey, t.excKey.data(), nexc * 4, cudaMemcpyHostToDevice));
 		NB_CUDA(cudaMemcpy(dVal, t.excVal.data(), nexc * 4, cudaMemcpyHostToDevice));
 	}
+	// the host libm's results at every reachable argument (67 MB + 336 MB)
+	float *dLogVal, *dSinVal;
+	NB_CUDA(cudaMalloc(&dLogVal, t.logVal.size() * 4));
+	NB_CUDA(cudaMalloc(&dSinVal, t.sinVal.size() * 4));
+	NB_CUDA(cudaMemcpy(dLogVal, t.logVal.data(), t.logVal.size() * 4, cudaMemcpyHostToDevice));
+	NB_CUDA(cudaMemcpy(dSinVal, t.sinVal.data(), t.sinVal.size() * 4, cudaMemcpyHostToDevice));
 	LibmCalib c;
 	c.logFlip = dLog;
 	c.sinFlip = dSin;
@@ -1162,6 +1168,8 @@ LibmCalib device_calibration(int device)
 	c.nexc = (uint32_t) nexc;
 	c.logNear = t.logNear;
 	c.sinNear = t.sinNear;
+	c.logVal = dLogVal;
+	c.sinVal = dSinVal;
 	cache[device] = c;
 	return c;
 }
