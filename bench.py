@@ -472,7 +472,11 @@ def run_batch(args, local):
     batch = nb.Batch(nets, conf)
     del nets
     build_s = time.perf_counter() - t0
-    tuned_us = batch.autotune(20)
+    if args.batch_launch:
+        batch.set_launch(*(int(x) for x in args.batch_launch.split(",")))
+        tuned_us = None
+    else:
+        tuned_us = batch.autotune(20)
     launch = batch.launch()
     neurons = sum(sp["n"] for sp in specs)
     with ClockSampler(local) as clk:
@@ -603,6 +607,8 @@ def main():
     ap.add_argument("--batch-max-fanout", type=int, default=1000)
     ap.add_argument("--batch-ms", type=int, default=1000)
     ap.add_argument("--batch-seed", type=int, default=0)
+    ap.add_argument("--batch-launch", default="",
+                    help="neurons per CTA and threads per CTA of the batch's step loop (instead of the autotuner)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
