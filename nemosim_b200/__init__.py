@@ -12,6 +12,8 @@ lists.
 """
 from __future__ import annotations
 
+import array
+
 import ctypes as C
 
 import numpy as np
@@ -45,6 +47,29 @@ def _f32(x):
 
 _EMPTY_U32 = np.zeros(1, np.uint32)
 _EMPTY_F32 = np.zeros(1, np.float32)
+
+# nemo_step bound with plain pointer arguments for Simulation.step, which is
+# called once per simulated millisecond: the ndpointer checks of the general
+# binding cost more than the call
+_STEP_PROTO = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_size_t,
+                          C.c_void_p, C.c_void_p)
+_step_fn = None
+
+
+def _nemo_step():
+    global _step_fn
+    if _step_fn is None:
+        _step_fn = _STEP_PROTO(("nemo_step", lib()))
+    return _step_fn
+
+
+def _u32_buffer(x):
+    """x as a buffer of unsigned 32-bit ints (array.array for a list)."""
+    return array.array("I", x) if isinstance(x, list) else _u32(x)
+
+
+def _address(buf) -> int:
+    return buf.buffer_info()[0] if isinstance(buf, array.array) else buf.ctypes.data
 
 
 def version() -> str:
@@ -231,21 +256,20 @@ class Simulation:
 
     def step(self, fstim=None, istim=None):
         """One 1 ms cycle; returns the fired neuron ids (src/api/python/__init__.py.in step)."""
-        f = _u32(fstim) if fstim is not None and len(fstim) else None
+        f = _u32_buffer(fstim) if fstim is not None and len(fstim) else None
         if istim:
-            inid = _u32([p[0] for p in istim])
-            icur = _f32([p[1] for p in istim])
+            inid = _u32_buffer([p[0] for p in istim])
+            icur = array.array("f", [p[1] for p in istim])
         else:
             inid = icur = None
-        fired = C.POINTER(C.c_uint)()
+        fired = C.c_void_p()
         n = C.c_size_t()
-        _check(lib().nemo_step(self._h, f if f is not None else _EMPTY_U32, 0 if f is None else len(f),
-                               inid if inid is not None else _EMPTY_U32,
-                               icur if icur is not None else _EMPTY_F32, 0 if inid is None else len(inid),
-                               C.byref(fired), C.byref(n)))
+        _check(_nemo_step()(self._h, _address(f) if f is not None else None, 0 if f is None else len(f),
+                            _address(inid) if inid is not None else None, _address(icur) if icur is not None else None,
+                            0 if inid is None else len(inid), C.addressof(fired), C.addressof(n)))
         if n.value == 0:
             return []
-        return np.ctypeslib.as_array(fired, shape=(n.value,)).tolist()
+        return array.array("I", C.string_at(fired.value, 4 * n.value)).tolist()
 
     def step_no_alloc(self, fstim=None, istim=None, capacity: int = 1 << 16):
         """step() through nemo_b200_step_no_alloc, which allocates nothing (an
