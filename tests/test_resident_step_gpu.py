@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 import nemosim_b200 as nb
+import oracle as O
 from tests import nets
 
 pytestmark = pytest.mark.gpu
@@ -146,3 +147,27 @@ def test_idle_time_limit_is_enforced():
         a.set_resident_step(100001)
     a.set_resident_step(100000)
     assert len(a.step([1, 2, 3])) >= 3
+
+
+def test_mixed_neuron_types_match_the_oracle():
+    """IF_curr_exp, Izhikevich and Poisson neurons (Pareto out-degree,
+    mixed-sign weights) stepped through the resident loop with firing and
+    current stimuli: the same fired neurons as the oracle's step, and the
+    same neuron state."""
+    (np_, tp, idp) = nets.mixed_network(nb)
+    (no_, to, ido) = nets.mixed_network(O)
+    sim, ref = nb.Simulation(np_, nb.Configuration()), O.Simulation(no_, O.Configuration())
+    n = len(idp[0]) + len(idp[1]) + 100
+    rng = np.random.default_rng(8)
+    fired = 0
+    for t in range(300):
+        f = rng.choice(n, 3, replace=False).tolist() if t % 4 == 0 else None
+        i = [(int(a), float(v)) for a, v in zip(rng.choice(n, 5), rng.normal(0, 10, 5))] if t % 6 == 0 else None
+        got = list(sim.step(f, i))
+        assert got == list(ref.step(f, i)), t
+        fired += len(got)
+    assert fired > 100
+    for t, ns, m in [(tp[0], 4, len(idp[0])), (tp[1], 2, len(idp[1]))]:
+        a = np.asarray(sim.type_state(t, ns, m), np.float32)
+        b = np.asarray(ref.type_state(t, ns, m), np.float32)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)) or np.array_equal(a, b, equal_nan=True)
