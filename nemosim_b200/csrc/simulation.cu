@@ -330,7 +330,12 @@ __device__ __forceinline__ void flush_counters(const DevSim& S, uint32_t ring, C
 
 // One step's neuron update: CTA c owns the partition of P consecutive
 // neurons starting at c * P (P a multiple of 32).
-__global__ void __launch_bounds__(1024)
+// Two instances: up to 1024 threads per CTA (64 registers), and up to 256
+// threads with at least 5 CTAs per SM (48 registers, 40 warps per SM) for
+// the shapes a large network's update takes, where more resident warps hide
+// more of each neuron's chain of loads.
+template<unsigned MAXT, unsigned MINB>
+__global__ void __launch_bounds__(MAXT, MINB)
 update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t ring, uint32_t offset, int fromDev,
 		uint32_t* hostFired = nullptr)
 {
@@ -343,6 +348,13 @@ update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t ring, uint32_t 
 	update_range(S, first, min(S.N, first + P), cur, ring, sC, false, hostFired);
 	__syncthreads();
 	flush_counters(S, ring, sC);
+}
+
+// the update_kernel instance for the two-launch step's threads per CTA
+using UpdateKernel = void (*)(const DevSim, uint32_t, uint32_t, uint32_t, uint32_t, int, uint32_t*);
+static UpdateKernel update_kernel_for(uint32_t threads)
+{
+	return threads <= 256 ? update_kernel<256, 5> : update_kernel<1024, 1>;
 }
 
 // 64-bit integer reduction into an accumulator word (its result unused)
@@ -1756,7 +1768,7 @@ void Simulation::launchStep(bool /*fullRecord*/)
 			(uint32_t) (PHASE_DELIVER | PHASE_STDP | PHASE_RESET), 0u, 0, nullptr, 0u, 0u);
 	timedEnd();
 	timedBegin(K_STEP);
-	launch_chained(update_kernel, grid, m_T, 0, m_stream, m_dev, m_P, cur, ring, 0u, 0, nullptr);
+	launch_chained(update_kernel_for(m_T), grid, m_T, 0, m_stream, m_dev, m_P, cur, ring, 0u, 0, nullptr);
 	timedEnd();
 	m_cycle++;
 	m_timerSteps++;
@@ -1872,7 +1884,7 @@ void Simulation::buildGraph()
 	for(unsigned k = 0; k < GRAPH_STEPS; ++k) {
 		launch_chained(deliver_kernel, m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream, m_dev, 0u,
 				(uint32_t) (PHASE_DELIVER | PHASE_STDP | PHASE_RESET), k, 1, nullptr, 0u, 0u);
-		launch_chained(update_kernel, grid, m_T, 0, m_stream, m_dev, m_P, 0u, 0u, k, 1, nullptr);
+		launch_chained(update_kernel_for(m_T), grid, m_T, 0, m_stream, m_dev, m_P, 0u, 0u, k, 1, nullptr);
 	}
 	advance_cycle_kernel<<<1, 1, 0, m_stream>>>(m_dev.cycleDev, GRAPH_STEPS);
 	NB_CUDA(cudaStreamEndCapture(m_stream, &g));
@@ -2051,7 +2063,7 @@ const std::vector<unsigned>& Simulation::step(const unsigned* fstim, size_t nf,
 	launch_chained(deliver_kernel, m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream, m_dev, c ^ 1u,
 			(uint32_t) (PHASE_DELIVER | PHASE_STDP | PHASE_RESET), 0u, 0,
 			need ? (const uint32_t*) m_dStimMapped : nullptr, (uint32_t) nf, (uint32_t) cur.size());
-	launch_chained(update_kernel, (m_N + m_P - 1) / m_P, m_T, 0, m_stream, m_dev, m_P, c, ring, 0u, 0,
+	launch_chained(update_kernel_for(m_T), (m_N + m_P - 1) / m_P, m_T, 0, m_stream, m_dev, m_P, c, ring, 0u, 0,
 			m_dFiredMapped);
 	m_cycle++;
 	m_timerSteps++;
