@@ -14,8 +14,9 @@
  * reference signatures carry only C types are exported under their reference
  * names.  The two that take reference C++ objects
  * (cuda_simulation(const network::Generator*, const ConfigurationImpl*) and
- * cuda_set_configuration(ConfigurationImpl*, int)) are bound through the
- * adapter shown in INTEGRATION.md, which forwards to Part 1.
+ * cuda_set_configuration(ConfigurationImpl*, int)) are bound through a
+ * small C++ adapter compiled on the reference side, which forwards to
+ * Part 1.
  *
  * Part 3 is extensions with no counterpart in the reference: bulk
  * construction, device-resident multi-step runs and bulk read-back.
@@ -296,6 +297,16 @@ NEMO_B200_API nemo_status_t nemo_b200_set_persistent(nemo_simulation_t, int on);
  * the GPU waits up to idle_us for it.  0 turns it off (two launches per
  * nemo_step).  Default 200.  Results are identical either way. */
 NEMO_B200_API nemo_status_t nemo_b200_set_resident_step(nemo_simulation_t, unsigned idle_us);
+/* Bounded waits of the persistent and resident step loops: every wait of a
+ * CTA on the others (a grid barrier, the resident loop's request broadcast)
+ * gives up after `polls` unsuccessful polls, sets the loop's error word and
+ * ends the launch; the call that ran it returns NEMO_CUDA_ERROR and the
+ * simulation's state is undefined from then on (delete it).  Default
+ * 16,777,216 polls (seconds); 0 gives up at the first unsuccessful poll,
+ * which lets a test exercise the error path without waiting.  A resident
+ * loop that is running keeps the limit it was launched with; this call
+ * ends it first. */
+NEMO_B200_API nemo_status_t nemo_b200_set_wait_limit(nemo_simulation_t, unsigned polls);
 /* Statistics of the last nemo_b200_run: its device time in ms (CUDA events
  * on the simulation's stream), and per kernel kind (0 = update kernel and
  * 1 = deliver kernel of the two-launch step, 2 = applyStdp, 3 = persistent
@@ -393,7 +404,10 @@ NEMO_B200_API nemo_status_t nemo_b200_bptt_backward(nemo_b200_bptt_t, const floa
  * NEMO_API_UNSUPPORTED.  Errors are reported by the status code only
  * (formatting a message would allocate): nemo_strerror is not updated.  The
  * first call on a device looks up the static buffer's device address and
- * should come before any stream capture.  The static buffers are shared:
+ * should come before any stream capture.  Every call takes the two-launch
+ * step and first ends the resident step loop of nemo_step if it runs, so a
+ * call costs about one two-launch step, more than a resident nemo_step.
+ * The static buffers are shared:
  * calls that overlap in time, from several threads or on several
  * simulations, race and must be serialised by the caller. */
 #define NEMO_B200_NO_ALLOC_STIMULUS_MAX 65536

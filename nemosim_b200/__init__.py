@@ -399,6 +399,11 @@ class Simulation:
         extension; 200 by default, 0 = two kernel launches per step)."""
         _check(lib().nemo_b200_set_resident_step(self._h, int(idle_us)))
 
+    def set_wait_limit(self, polls: int):
+        """Polls of each grid-barrier or request wait before it gives up and
+        the call reports NEMO_CUDA_ERROR (an extension; 0: at once)."""
+        _check(lib().nemo_b200_set_wait_limit(self._h, int(polls)))
+
     def run_stats(self) -> dict:
         """Statistics of the last run() (an extension): device ms, per-kernel
         ms and launches (when profiling; "step" and "stdp" are the update and

@@ -629,6 +629,12 @@ nemo_status_t nemo_b200_set_resident_step(nemo_simulation_t s, unsigned idle_us)
 	CALL(S(s).setResidentIdle(idle_us));
 }
 
+nemo_status_t nemo_b200_set_wait_limit(nemo_simulation_t s, unsigned polls)
+{
+	NULLCHECK(s);
+	CALL(S(s).setWaitLimit(polls));
+}
+
 nemo_status_t nemo_b200_run_stats(nemo_simulation_t s, float* runMs, float kernelMs[4], unsigned launches[4],
 		uint64_t* fired, uint64_t* events, uint64_t* stdpEntries, uint64_t* plastic)
 {

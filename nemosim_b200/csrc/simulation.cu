@@ -555,11 +555,11 @@ deliver_kernel(const DevSim S, uint32_t pub, uint32_t what, uint32_t offset, int
 // the writes the CTA made before its barrier visible with it) and polls the
 // counter with acquire loads until every CTA has arrived at this barrier;
 // a CTA barrier then passes the acquire on to the CTA's other threads.
-// Barrier b is complete when the counter reaches (b + 1) x gridDim.x.  A wait gives up after BARRIER_SPIN_LIMIT
-// polls (seconds; a phase takes microseconds): it sets the error word, which
-// makes every CTA leave the step loop at its next barrier, and the host
-// reports the error.
-constexpr uint32_t BARRIER_SPIN_LIMIT = 1u << 24;
+// Barrier b is complete when the counter reaches (b + 1) x gridDim.x.  A wait
+// gives up after S.waitLimit unsuccessful polls (BARRIER_SPIN_LIMIT, seconds,
+// unless nemo_b200_set_wait_limit lowered it; a phase takes microseconds): it
+// sets the error word, which makes every CTA leave the step loop at its next
+// barrier, and the host reports the error.
 
 __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p)
 {
@@ -590,12 +590,12 @@ __device__ __forceinline__ void grid_arrive(GridBarrier* gb, uint32_t& target)
 // and two barriers a step, 2^32 arrivals are 7.5M steps).
 __device__ __forceinline__ bool reached(uint32_t value, uint32_t target) { return (int32_t) (value - target) >= 0; }
 
-__device__ __forceinline__ bool grid_wait(GridBarrier* gb, uint32_t& target, uint32_t& ok)
+__device__ __forceinline__ bool grid_wait(GridBarrier* gb, uint32_t& target, uint32_t& ok, uint32_t limit)
 {
 	if(threadIdx.x == 0) {
 		uint32_t polls = 0;
 		while(!reached(ld_acquire(&gb->count), target)) {
-			if(++polls > BARRIER_SPIN_LIMIT || ld_acquire(&gb->error)) {
+			if(++polls > limit || ld_acquire(&gb->error)) {
 				atomicExch(&gb->error, 1u);
 				ok = 0;
 				break;
@@ -607,7 +607,7 @@ __device__ __forceinline__ bool grid_wait(GridBarrier* gb, uint32_t& target, uin
 	return ok != 0;
 }
 
-__device__ __forceinline__ bool grid_barrier(GridBarrier* gb, uint32_t& target, uint32_t& ok)
+__device__ __forceinline__ bool grid_barrier(GridBarrier* gb, uint32_t& target, uint32_t& ok, uint32_t limit)
 {
 	__syncthreads();
 	if(threadIdx.x == 0) {
@@ -615,7 +615,7 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, uint32_t& target, 
 		red_release_add(&gb->count, 1u);
 		uint32_t polls = 0;
 		while(!reached(ld_acquire(&gb->count), target)) {
-			if(++polls > BARRIER_SPIN_LIMIT || ld_acquire(&gb->error)) {
+			if(++polls > limit || ld_acquire(&gb->error)) {
 				atomicExch(&gb->error, 1u);
 				ok = 0;
 				break;
@@ -671,13 +671,13 @@ __device__ __forceinline__ bool persistent_step(const DevSim& S, uint32_t P, uns
 	} else {
 		for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) precompute_noise(S, p * P, min(S.N, p * P + P));
 	}
-	if(!grid_wait(gb, sTarget, sOk)) return false;
+	if(!grid_wait(gb, sTarget, sOk, S.waitLimit)) return false;
 	for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
 		update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC, true, hostFired);
 	}
 	__syncthreads();
 	flush_counters(S, ring, sC);
-	return grid_barrier(gb, sTarget, sOk);
+	return grid_barrier(gb, sTarget, sOk, S.waitLimit);
 }
 
 __global__ void __launch_bounds__(RUN_THREADS, 1)
@@ -701,7 +701,7 @@ run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0
 	if(steps && finalStdp) {
 		const uint32_t last = (uint32_t) ((cycle0 + steps - 1) & 1);
 		deliver_range(S, last, PHASE_STDP);
-		if(!grid_barrier(gb, sTarget, sOk)) return;
+		if(!grid_barrier(gb, sTarget, sOk, S.waitLimit)) return;
 		if(blockIdx.x == 0 && threadIdx.x == 0) S.stdpWork.count[last] = 0;
 	}
 }
@@ -843,7 +843,7 @@ __device__ uint32_t fired_ids_to_host(const DevSim& S, const uint32_t* words, ui
 
 // A CTA other than 0 waits for CTA 0's broadcast of request `want` (1) or
 // of the end of the loop (0); gives up like a grid barrier.
-__device__ __forceinline__ uint32_t wait_request(GridBarrier* gb, uint32_t want, uint32_t& ok)
+__device__ __forceinline__ uint32_t wait_request(GridBarrier* gb, uint32_t want, uint32_t& ok, uint32_t limit)
 {
 	__shared__ uint32_t sCmd;
 	if(threadIdx.x == 0) {
@@ -855,7 +855,7 @@ __device__ __forceinline__ uint32_t wait_request(GridBarrier* gb, uint32_t want,
 				break;
 			}
 			if(v == (want | SERVE_STOP)) break;
-			if(++polls > BARRIER_SPIN_LIMIT || ld_acquire(&gb->error)) {
+			if(++polls > limit || ld_acquire(&gb->error)) {
 				atomicExch(&gb->error, 1u);
 				ok = 0;
 				break;
@@ -915,7 +915,7 @@ serve_kernel(const DevSim S, uint32_t P, unsigned long long cycle0, GridBarrier*
 			__syncthreads();
 			op = sOp;
 		} else {
-			op = wait_request(gb, want, sOk);
+			op = wait_request(gb, want, sOk, S.waitLimit);
 		}
 		if(!op) return;
 		const uint32_t nf = *(volatile uint32_t*) &gb->nf;
@@ -1126,6 +1126,25 @@ nemo_status_t Simulation::stepNoAlloc(const unsigned* fstim, size_t nf, const un
 		return NEMO_CUDA_ERROR;
 	}
 	if(cudaStreamSynchronize(m_stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) return NEMO_CUDA_ERROR;
+	// a persistent or resident loop that ran before this call (the stream
+	// synchronisation waited for it) and gave up at a wait has left the
+	// simulation state undefined: report it as checkBarrier does, without
+	// throwing or allocating (the word is read into pinned host memory)
+	if(m_barrierUsed) {
+		m_barrierUsed = false;
+		if(cudaMemcpyAsync(m_hBarrierError, &m_barrier->error, 4, cudaMemcpyDeviceToHost, m_stream) != cudaSuccess
+				|| cudaStreamSynchronize(m_stream) != cudaSuccess) {
+			return NEMO_CUDA_ERROR;
+		}
+		if(*m_hBarrierError) {
+			*m_hBarrierError = 0;
+			cudaMemsetAsync(m_barrier, 0, sizeof(GridBarrier), m_stream);
+			cudaStreamSynchronize(m_stream);
+			m_barrierBase = 0;
+			m_barrierStale = false;
+			return NEMO_CUDA_ERROR;
+		}
+	}
 	// fired neurons in ascending local index, as global ids
 	// (setFiring, src/nemo/cpu/Simulation.cpp:200-208)
 	size_t count = 0;
@@ -1299,6 +1318,7 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	DevSim& S = m_dev;
 	S.N = N;
 	S.W = (N + 31) / 32;
+	S.waitLimit = BARRIER_SPIN_LIMIT;
 
 	// neuron layout: kinds in order of first appearance (for one network this
 	// is its type order, src/nemo/cpu/Simulation.cpp:58-73), then network
@@ -1910,6 +1930,13 @@ void Simulation::setResidentIdle(unsigned us)
 	// a running loop keeps the idle time it was launched with
 	stopServe();
 	residentIdleUs = us;
+}
+
+void Simulation::setWaitLimit(uint32_t polls)
+{
+	// a running loop keeps the limit it was launched with
+	stopServe();
+	m_dev.waitLimit = polls;
 }
 
 bool Simulation::residentAvailable() const

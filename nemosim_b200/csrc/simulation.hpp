@@ -37,6 +37,8 @@ static_assert(offsetof(GridBarrier, cmd) == 4, "one memset restarts count and cm
 constexpr uint32_t SERVE_STOP = 0x80000000u;
 __host__ __device__ inline uint32_t serve_next(uint32_t seq) { return seq == 0x7fffffffu ? 1u : seq + 1u; }
 constexpr unsigned RESIDENT_IDLE_MAX_US = 100000;  // the grid barrier's wait limit is far longer
+// polls of a grid-barrier or request wait before it gives up (seconds)
+constexpr uint32_t BARRIER_SPIN_LIMIT = 1u << 24;
 constexpr unsigned RESIDENT_REPLY_LIMIT_S = 20;
 
 // Requests to the resident step loop of nemo_step (mapped host memory):
@@ -139,6 +141,7 @@ struct DevSim {
 	unsigned long long* cycleDev; // step counter read by kernels replayed from a CUDA graph
 	StdpParams sp;
 	LibmCalib calib;
+	uint32_t waitLimit;       // polls of a grid-barrier or request wait before it gives up
 };
 
 class Simulation {
@@ -210,6 +213,11 @@ public:
 	unsigned residentIdleUs = 200;
 	bool residentAvailable() const;
 	void setResidentIdle(unsigned us);
+	// polls of each grid-barrier or request wait of the persistent and
+	// resident loops before it gives up and the call reports
+	// NEMO_CUDA_ERROR (BARRIER_SPIN_LIMIT by default; 0: give up at the
+	// first unsuccessful poll); lets a test make the waits run out
+	void setWaitLimit(uint32_t polls);
 	// time candidate launch shapes on trial steps from a saved copy of the
 	// simulation state, restore it, and keep the fastest; returns its time
 	// per step in microseconds

@@ -200,3 +200,107 @@ def stdp_analytic(mod, reward, epochs=4):
             ws.append(got)
         history.append(ws)
     return history
+
+
+def input_network(mod, ncount, izhikevich):
+    """addNeurons of src/test/Input.cpp:9-22: Input neurons 0..ncount-1 (no
+    parameters, no state), optionally as many Izhikevich neurons after them."""
+    net = mod.Network()
+    inp = net.add_neuron_type("Input")
+    net.add_neuron(inp, np.arange(ncount, dtype=np.uint32))
+    if izhikevich:
+        iz = net.add_neuron_type("Izhikevich")
+        net.add_neuron(iz, np.arange(ncount, 2 * ncount, dtype=np.uint32),
+                       0.02, 0.2, -65.0, 8.0, 0.0, f32(0.2) * f32(-65.0), -65.0)
+    return net
+
+
+def input_create(mod, ncount, izhikevich):
+    """create (src/test/Input.cpp:29-37): a network of Input neurons steps."""
+    sim = mod.Simulation(input_network(mod, ncount, izhikevich), mod.Configuration())
+    assert sim.step() == []
+
+
+def input_simple(mod, ncount, izhikevich, steps=1000, seed=0):
+    """simple (src/test/Input.cpp:41-63): Input neurons fire exactly when
+    stimulated, in stimulus order.  Returns the fire stream."""
+    sim = mod.Simulation(input_network(mod, ncount, izhikevich), mod.Configuration())
+    rng = np.random.default_rng(seed)
+    stream = []
+    for _ in range(steps):
+        p = 0.5 * rng.random()
+        fstim = np.flatnonzero(rng.random(ncount) < p).tolist()
+        fired = sim.step(fstim)
+        assert fired == fstim
+        stream.append(fired)
+    return stream
+
+
+def clamp_network(mod):
+    """Four plastic synapses whose weights start outside the STDP limits of
+    clamp_configuration (above the excitatory maximum, below the excitatory
+    minimum, beyond the inhibitory maximum, inside the inhibitory minimum),
+    a plastic zero weight, and one static synapse out of range."""
+    net = mod.Network()
+    iz = net.add_neuron_type("Izhikevich")
+    net.add_neuron(iz, np.arange(8, dtype=np.uint32), *nets.exc_neuron_args())
+    ws = [15.0, 0.5, -15.0, -0.5, 0.0, 15.0]
+    plastic = [1, 1, 1, 1, 1, 0]
+    net.add_synapse(np.zeros(6, np.uint32), np.arange(1, 7, dtype=np.uint32), np.ones(6, np.uint32),
+                    np.array(ws, f32), np.array(plastic, np.uint8))
+    return net
+
+
+def clamp_configuration(mod):
+    """STDP limits E [2, 10], I [-2, -10] (setStdpFunction's six-argument
+    form, src/nemo/Configuration.cpp:92-100)"""
+    conf = mod.Configuration()
+    pre = np.array([f32(0.1) * np.exp(f32(-dt) / f32(20.0), dtype=f32) for dt in range(1, 21)], f32)
+    post = np.array([f32(-0.12) * np.exp(f32(-dt) / f32(20.0), dtype=f32) for dt in range(1, 21)], f32)
+    conf.set_stdp_function(pre, post, 2.0, 10.0, -2.0, -10.0)
+    return conf
+
+
+def first_call_clamp(mod, reward):
+    """The first applyStdp visits every plastic synapse and clamps weights
+    that start outside the limits even where nothing accumulated
+    (ConnectivityMatrix::applyStdp, src/nemo/ConnectivityMatrix.cpp:241-294;
+    StdpProcess::updatedWeight, src/nemo/StdpProcess.cpp:128-138); a zero
+    weight stays zero and static synapses are not touched.  Returns the
+    weights after the call."""
+    sim = mod.Simulation(clamp_network(mod), clamp_configuration(mod))
+    sim.step()
+    sim.apply_stdp(reward)
+    ws = [sim.get_synapse_weight(sim.get_synapses_from(0)[k]) for k in range(6)]
+    assert ws == [10.0, 2.0, -10.0, -2.0, 0.0, 15.0], ws
+    return ws
+
+
+def zero_reward_clears(mod):
+    """applyStdp(0) clears the accumulators and leaves the weights (all
+    within limits) unchanged: an applyStdp(1.0) straight after it changes
+    nothing, while on a twin simulation without it the same call changes
+    weights (src/nemo/ConnectivityMatrix.cpp:251-259).  Returns the weights
+    of the twin after 50 more steps and applyStdp(0.8)."""
+    def make():
+        s = mod.Simulation(stdp_analytic_network(mod), nets.stdp_test_configuration(mod))
+        for ms in range(100):
+            fstim = list(range(GROUP)) if ms == 10 else list(range(GROUP, 2 * GROUP)) if ms == 20 else None
+            s.step(fstim)
+        return s
+
+    def weights(s):
+        return [s.get_synapse_weight(s.get_synapses_from(k)[0]) for k in range(GROUP)]
+
+    cleared, twin = make(), make()
+    cleared.apply_stdp(0.0)
+    assert weights(cleared) == [INIT_W] * GROUP
+    cleared.apply_stdp(1.0)
+    assert weights(cleared) == [INIT_W] * GROUP
+    twin.apply_stdp(1.0)
+    assert weights(twin) != [INIT_W] * GROUP
+    for s in (cleared, twin):
+        for ms in range(50):
+            s.step(list(range(GROUP)) if ms == 10 else list(range(GROUP, 2 * GROUP)) if ms == 20 else None)
+        s.apply_stdp(0.8)
+    return weights(cleared), weights(twin)

@@ -57,6 +57,21 @@ def test_stdp_analytic(reward):
     kat.stdp_analytic(O, reward)
 
 
+@pytest.mark.parametrize("ncount,iz", [(1, False), (1000, False), (1, True), (1000, True)])
+def test_input_neurons(ncount, iz):
+    kat.input_create(O, ncount, iz)
+    kat.input_simple(O, ncount, iz, steps=300)
+
+
+@pytest.mark.parametrize("reward", [1.0, 0.0])
+def test_first_call_clamp(reward):
+    kat.first_call_clamp(O, reward)
+
+
+def test_zero_reward_clears_accumulators():
+    kat.zero_reward_clears(O)
+
+
 def test_ring_delay_80_rejected():
     """The CPU backend rejects delays above 64 (src/nemo/cpu/Simulation.cpp:52-56)."""
     with pytest.raises(O.NemoError):

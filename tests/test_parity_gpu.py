@@ -88,6 +88,27 @@ def test_poisson_rate(others):
     assert kat.poisson_rate(nb, 10000, others) == kat.poisson_rate(O, 10000, others)
 
 
+@pytest.mark.parametrize("ncount,iz", [(1, False), (1000, False), (1, True), (1000, True)])
+def test_input_neurons(ncount, iz):
+    """The Input type (src/test/Input.cpp:41-79): it fires exactly when
+    stimulated; the fire stream equals the oracle's"""
+    kat.input_create(nb, ncount, iz)
+    assert kat.input_simple(nb, ncount, iz) == kat.input_simple(O, ncount, iz)
+
+
+@pytest.mark.parametrize("reward", [1.0, 0.0])
+def test_first_call_clamp(reward):
+    """The first applyStdp clamps weights that start outside the limits,
+    with any reward (zero included)"""
+    assert kat.first_call_clamp(nb, reward) == kat.first_call_clamp(O, reward)
+
+
+def test_zero_reward_clears_accumulators():
+    """applyStdp(0) clears the accumulators, keeps the weights, and later
+    calls continue as on the oracle"""
+    assert kat.zero_reward_clears(nb) == kat.zero_reward_clears(O)
+
+
 # ---------------------------------------------------------------------------
 # bit-exact parity with the oracle on noisy networks
 

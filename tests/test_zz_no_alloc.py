@@ -3,6 +3,8 @@ two stimulated steps in a row give the same fired neurons and leave the
 same simulation state, and its size, index and capacity errors leave the
 simulation as it was (or, for the fired-list capacity, step exactly as
 nemo_step does).  This file is collected last and needs no other test."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -79,3 +81,56 @@ def test_small_fired_capacity_reports_overflow_after_stepping():
     assert fired == expected[:1]
     assert sim.elapsed_simulation() == 1
     assert same_state(ref, sim)
+
+
+class _MallInfo2(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_size_t) for name in
+                ("arena", "ordblks", "smblks", "hblks", "hblkhd", "usmblks", "fsmblks", "uordblks", "fordblks",
+                 "keepcost")]
+
+
+def test_call_allocates_nothing():
+    """The entry point's defining property, measured: after a warm-up call
+    (which looks up the static buffer's device address and loads the
+    stimulus kernel), a stimulated call leaves the device's free memory
+    (cudaMemGetInfo) and the host heap in use (glibc mallinfo2, all arenas)
+    exactly as they were.  The call is made through a plain C function
+    pointer with every argument prepared beforehand, and Python's garbage
+    collector is paused, so that nothing but the call itself runs between
+    the two readings."""
+    import gc
+
+    import torch
+
+    libc = ctypes.CDLL("libc.so.6")
+    libc.mallinfo2.restype = _MallInfo2
+    step = ctypes.CDLL(nb.library_path()).nemo_b200_step_no_alloc
+    step.restype = ctypes.c_int
+    step.argtypes = [ctypes.c_void_p] * 9
+    _, sim = twins()
+    fstim = np.array([3, 17, 500], np.uint32)
+    inidx = np.array([5, 700, 5], np.uint32)
+    icur = np.array([10.0, -3.0, 12.5], np.float32)
+    fired = np.zeros(1 << 16, np.uint32)
+    nfired = ctypes.c_size_t()
+    args = (ctypes.c_void_p(sim._h), ctypes.c_void_p(fstim.ctypes.data), ctypes.c_void_p(len(fstim)),
+            ctypes.c_void_p(inidx.ctypes.data), ctypes.c_void_p(icur.ctypes.data), ctypes.c_void_p(len(inidx)),
+            ctypes.c_void_p(fired.ctypes.data), ctypes.c_void_p(len(fired)),
+            ctypes.c_void_p(ctypes.addressof(nfired)))
+    assert step(*args) == NEMO_OK  # warm-up
+    assert step(*args) == NEMO_OK
+    torch.cuda.mem_get_info(0)
+    gc.disable()
+    try:
+        free0 = torch.cuda.mem_get_info(0)[0]
+        rc_device = step(*args)
+        free1 = torch.cuda.mem_get_info(0)[0]
+        heap0 = libc.mallinfo2().uordblks
+        rc_host = step(*args)
+        heap1 = libc.mallinfo2().uordblks
+    finally:
+        gc.enable()
+    assert rc_device == NEMO_OK and rc_host == NEMO_OK
+    assert free1 == free0, f"device free memory changed by {free1 - free0} bytes"
+    assert heap1 == heap0, f"host heap in use changed by {heap1 - heap0} bytes"
+    assert 3 in fired[:nfired.value]
