@@ -629,6 +629,36 @@ nemo_status_t nemo_b200_set_resident_step(nemo_simulation_t s, unsigned idle_us)
 	CALL(S(s).setResidentIdle(idle_us));
 }
 
+nemo_status_t nemo_b200_set_pipelined(nemo_simulation_t s, int on)
+{
+	NULLCHECK(s);
+	CALL(S(s).pipelined = on != 0);
+}
+
+nemo_status_t nemo_b200_set_spare_ctas(nemo_simulation_t s, unsigned ctas)
+{
+	NULLCHECK(s);
+	CALL(S(s).setSpareCtas(ctas));
+}
+
+nemo_status_t nemo_b200_get_spare_ctas(nemo_simulation_t s, unsigned* ctas)
+{
+	NULLCHECK(s);
+	NULLCHECK(ctas);
+	CALL(*ctas = S(s).spareCtas());
+}
+
+nemo_status_t nemo_b200_trace_phases(nemo_simulation_t s, unsigned steps, uint64_t* out, size_t cap,
+		unsigned* ctas, unsigned* owners)
+{
+	NULLCHECK(s);
+	NULLCHECK(out);
+	CALL({
+		const unsigned g = S(s).tracePhases(steps, out, cap, owners);
+		if(ctas) *ctas = g;
+	});
+}
+
 nemo_status_t nemo_b200_set_wait_limit(nemo_simulation_t s, unsigned polls)
 {
 	NULLCHECK(s);
