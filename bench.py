@@ -264,30 +264,26 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def phase_summary(trace, owners) -> dict:
+def phase_summary(trace) -> dict:
     """Per-phase times of the persistent step loop from its %globaltimer
-    trace ([steps, CTAs, 6] ns; the first `owners` CTAs own partitions):
-    each point relative to the step's start (the earliest CTA), as the
-    median over the steps (the first and the last two, which publish
-    differently, left out) of the median or the last CTA."""
+    trace ([steps, CTAs, 5] ns): each point relative to the step's start
+    (the earliest CTA), as the median over the steps (the first and the
+    last left out) of the median or the last CTA."""
     t = trace.astype(np.int64)
-    if t.shape[0] > 6:
-        t = t[1:-2]
+    if t.shape[0] > 4:
+        t = t[1:-1]
     rel = (t - t[:, :, :1].min(axis=1, keepdims=True)) / 1e3
-    own = rel[:, :owners]
 
     def over_steps(x):
         return round(float(np.median(x)), 2)
     return {
-        "arrivals_delivered_median_cta": over_steps(np.median(rel[:, :, 1], axis=1)),
-        "arrivals_delivered_last_cta": over_steps(rel[:, :, 1].max(axis=1)),
-        "barrier_seen_median_owner": over_steps(np.median(own[:, :, 2], axis=1)),
-        "update_done_median_owner": over_steps(np.median(own[:, :, 3], axis=1)),
-        "update_done_last_owner": over_steps(own[:, :, 3].max(axis=1)),
-        "claimed_work_done_median_cta": over_steps(np.median(rel[:, :, 4], axis=1)),
-        "claimed_work_done_last_cta": over_steps(rel[:, :, 4].max(axis=1)),
-        "step_end_last_cta": over_steps(rel[:, :, 5].max(axis=1)),
-        "steps": int(t.shape[0]), "ctas": int(t.shape[1]), "owners": int(owners),
+        "prephase_done_median_cta": over_steps(np.median(rel[:, :, 1], axis=1)),
+        "prephase_done_last_cta": over_steps(rel[:, :, 1].max(axis=1)),
+        "barrier_seen_median_cta": over_steps(np.median(rel[:, :, 2], axis=1)),
+        "update_done_median_cta": over_steps(np.median(rel[:, :, 3], axis=1)),
+        "update_done_last_cta": over_steps(rel[:, :, 3].max(axis=1)),
+        "step_end_last_cta": over_steps(rel[:, :, 4].max(axis=1)),
+        "steps": int(t.shape[0]), "ctas": int(t.shape[1]),
     }
 
 
@@ -304,8 +300,6 @@ def run_b200(args, rank, world, local):
         sim.set_graphs(False)
     if args.no_persistent:
         sim.set_persistent(False)
-    if args.no_pipelined:
-        sim.set_pipelined(False)
     build_s = time.perf_counter() - t0
     W = args.window
 
@@ -367,8 +361,7 @@ def run_b200(args, rank, world, local):
     # where a step's time goes: one traced launch of the persistent loop
     phases = None
     if persistent:
-        tr, owners = sim.trace_phases(W)
-        phases = phase_summary(tr, owners)
+        phases = phase_summary(sim.trace_phases(W))
 
     # e2e through the C ABI with host buffers, the calls a C caller makes:
     # nemo_step once per ms (a one-neuron firing stimulus from host memory,
@@ -453,7 +446,7 @@ def run_b200(args, rank, world, local):
             "clocks": clk.summary(),
             "build_s": build_s,
             "phases_us": phases,
-            "launch": {"partition": launch[0], "threads": launch[1], "spare_ctas": sim.spare_ctas(),
+            "launch": {"partition": launch[0], "threads": launch[1],
                        "autotuned_us_per_step": tuned_us,
                        "step_loop": "persistent cooperative launch per period" if persistent
                        else "two launches per step" + ("" if args.no_graphs else ", CUDA graphs of 100 steps")},
@@ -633,8 +626,6 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--no-persistent", action="store_true")
-    ap.add_argument("--no-pipelined", action="store_true",
-                    help="the persistent loop makes every delivery before its arrival step's update")
     ap.add_argument("--workload", choices=["headline", "batch256", "bptt"], default="headline",
                     help="headline: the 100k x 1k STDP network (default); batch256: batched networks "
                          "against sequential runs; bptt: differentiable mode against PyTorch autograd")

@@ -297,36 +297,19 @@ NEMO_B200_API nemo_status_t nemo_b200_set_persistent(nemo_simulation_t, int on);
  * the GPU waits up to idle_us for it.  0 turns it off (two launches per
  * nemo_step).  Default 200.  Results are identical either way. */
 NEMO_B200_API nemo_status_t nemo_b200_set_resident_step(nemo_simulation_t, unsigned idle_us);
-/* How the persistent step loop of nemo_b200_run makes the deliveries of
- * delay 2 and more: published two steps ahead and made while the next
- * step's neuron update runs, between two applyStdp calls (on, the default),
- * or all before the update of their arrival step (off).  Only the delay-1
- * deliveries, whose sources fired in the step just before, then stay
- * between two updates.  Results are identical. */
-NEMO_B200_API nemo_status_t nemo_b200_set_pipelined(nemo_simulation_t, int on);
-/* CTAs of the persistent and resident step loops beyond those that own a
- * partition of neurons (the grid never exceeds the co-resident CTAs): they
- * take their share of the deliveries arriving at each step and then the
- * work no neuron update waits for (the STDP accumulation, the deliveries
- * made ahead) while the owners update.  Default: one per SM when the
- * co-resident CTAs are more than twice the SMs; the autotuner chooses among
- * none, one and two per SM.  Results are identical for every value. */
-NEMO_B200_API nemo_status_t nemo_b200_set_spare_ctas(nemo_simulation_t, unsigned ctas);
-NEMO_B200_API nemo_status_t nemo_b200_get_spare_ctas(nemo_simulation_t, unsigned* ctas);
 /* Phase trace: runs `steps` steps (then their STDP accumulation, as
  * nemo_b200_run does before an applyStdp) in one launch of the persistent
- * step loop with %globaltimer read by every CTA at 6 points of each step:
- * its start, its arrival after the deliveries arriving at that step, the
- * release of that barrier and the end of its neuron update (CTAs that own
- * partitions; others repeat the previous value), its arrival at the step's
- * final barrier after the work no update waits for, and that barrier's
- * release.  out[(step x ctas + cta) x 6 + point] in ns; *ctas receives the
- * launch's CTAs, *owners how many own partitions (the first ones).  The
- * simulation advances by `steps` steps, as nemo_b200_run would.  Needs the
- * persistent loop (NEMO_API_UNSUPPORTED otherwise) and allocates the
- * device buffer for the call. */
+ * step loop with %globaltimer read by every CTA at 5 points of each step:
+ * its start, its arrival at the barrier after the pre-phase (the
+ * deliveries arriving at that step and the last step's STDP accumulation),
+ * that barrier's release, the end of its neuron update, and the release of
+ * the step's final barrier.  out[(step x ctas + cta) x 5 + point] in ns;
+ * *ctas receives the launch's CTAs.  The simulation advances by `steps`
+ * steps, as nemo_b200_run would.  Needs the persistent loop
+ * (NEMO_API_UNSUPPORTED otherwise) and allocates the device buffer for the
+ * call. */
 NEMO_B200_API nemo_status_t nemo_b200_trace_phases(nemo_simulation_t, unsigned steps, uint64_t* out, size_t cap,
-		unsigned* ctas, unsigned* owners);
+		unsigned* ctas);
 /* Bounded waits of the persistent and resident step loops: every wait of a
  * CTA on the others (a grid barrier, the resident loop's request broadcast)
  * gives up after `polls` unsuccessful polls, sets the loop's error word and

@@ -399,30 +399,14 @@ class Simulation:
         extension; 200 by default, 0 = two kernel launches per step)."""
         _check(lib().nemo_b200_set_resident_step(self._h, int(idle_us)))
 
-    def set_pipelined(self, on: bool = True):
-        """run()'s persistent loop makes the deliveries of delay 2 and more
-        a step ahead, while the next update runs (an extension; on by
-        default)."""
-        _check(lib().nemo_b200_set_pipelined(self._h, int(on)))
-
-    def set_spare_ctas(self, ctas: int):
-        """CTAs of the persistent loops beyond the partitions' owners (an
-        extension; chosen by the autotuner)."""
-        _check(lib().nemo_b200_set_spare_ctas(self._h, int(ctas)))
-
-    def spare_ctas(self) -> int:
-        v = C.c_uint()
-        _check(lib().nemo_b200_get_spare_ctas(self._h, C.byref(v)))
-        return v.value
-
-    def trace_phases(self, steps: int = 100):
+    def trace_phases(self, steps: int = 100) -> np.ndarray:
         """Phase trace of one launch of the persistent loop (an extension):
-        returns (times [steps, ctas, 6] in ns, owners)."""
-        cap = steps * 8192 * 6
+        %globaltimer [steps, CTAs, 5] in ns."""
+        cap = steps * 8192 * 5
         out = np.zeros(cap, np.uint64)
-        ctas, owners = C.c_uint(), C.c_uint()
-        _check(lib().nemo_b200_trace_phases(self._h, steps, out, cap, C.byref(ctas), C.byref(owners)))
-        return out[: steps * ctas.value * 6].reshape(steps, ctas.value, 6), owners.value
+        ctas = C.c_uint()
+        _check(lib().nemo_b200_trace_phases(self._h, steps, out, cap, C.byref(ctas)))
+        return out[: steps * ctas.value * 5].reshape(steps, ctas.value, 5)
 
     def set_wait_limit(self, polls: int):
         """Polls of each grid-barrier or request wait before it gives up and

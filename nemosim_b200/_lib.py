@@ -102,10 +102,8 @@ SIGNATURES = {
     "nemo_b200_set_persistent": (st, [vp, C.c_int]),
     "nemo_b200_set_resident_step": (st, [vp, C.c_uint]),
     "nemo_b200_set_wait_limit": (st, [vp, C.c_uint]),
-    "nemo_b200_set_pipelined": (st, [vp, C.c_int]),
-    "nemo_b200_trace_phases": (st, [vp, C.c_uint, u64p, sz, PU, PU]),
-    "nemo_b200_set_spare_ctas": (st, [vp, C.c_uint]),
-    "nemo_b200_get_spare_ctas": (st, [vp, PU]),
+    "nemo_b200_trace_phases": (st, [vp, C.c_uint, u64p, sz, PU]),
+
     "nemo_b200_run_stats": (st, [vp, PF, PF, PU] + [C.POINTER(C.c_uint64)] * 4),
     "nemo_b200_set_launch": (st, [vp, C.c_uint, C.c_uint]),
     "nemo_b200_get_launch": (st, [vp, PU, PU]),

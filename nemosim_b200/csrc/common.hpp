@@ -24,23 +24,41 @@ std::string format(const char* fmt, ...) __attribute__((format(printf, 1, 2)));
 
 #define NB_THROW(code, ...) throw ::nemo_b200::Error((code), ::nemo_b200::format(__VA_ARGS__))
 
-// The compiled-in neuron types.  Parameter/state counts, membrane-potential
-// index and RNG use follow the .ini descriptors
-// (src/nemo/plugins/{Izhikevich,IF_curr_exp,PoissonSource,Input}.ini) and
-// the index headers (src/nemo/plugins/Izhikevich.h, IF_curr_exp.h).
-enum NeuronKind { KIND_IZHIKEVICH = 0, KIND_IF_CURR_EXP = 1, KIND_POISSON = 2, KIND_INPUT = 3 };
-
-struct NeuronTypeDesc {
-	const char* name;
-	NeuronKind kind;
-	unsigned nparam;
-	unsigned nstate;
-	unsigned mpot;     // state index of the membrane potential
+// A neuron type as its .ini descriptor describes it
+// (src/nemo/NeuronType.cpp:91-156), bound to the kernel of this backend
+// that updates it (src/nemo/cuda/Neurons.cpp:43 binds the CUDA plugin of
+// the type instead).  KIND_NONE: the backend has no kernel for the type.
+enum NeuronKind {
+	KIND_NONE = -1,
+	KIND_IZHIKEVICH = 0,
+	KIND_IF_CURR_EXP = 1,
+	KIND_POISSON = 2,
+	KIND_INPUT = 3,
+	KIND_COUNT = 4
 };
 
-extern const NeuronTypeDesc NEURON_TYPES[4];
-const NeuronTypeDesc* find_neuron_type(const std::string& name);
+struct NeuronTypeDesc {
+	std::string name;
+	NeuronKind kind = KIND_NONE;
+	unsigned nparam = 0;
+	unsigned nstate = 0;
+	unsigned mpot = 0;        // state index of the membrane potential
+	bool nrand = false;       // uses the normal RNG
+	unsigned history = 1;     // state history length
+	bool rcmSources = false, rcmDelays = false, rcmForward = false, rcmWeights = false;
+	bool cpu = false, cuda = false;  // [backends]
+	std::string pluginDir;    // directory of the .ini file
+};
 
+// The kernels compiled into the step loop, by kind: the name of the type
+// each implements and the parameter, state and RNG layout it expects
+// (src/nemo/plugins/Izhikevich.h, IF_curr_exp.h; the .ini descriptors).
+struct KernelLayout {
+	const char* name;
+	unsigned nparam, nstate;
+	bool nrand;
+};
+extern const KernelLayout KERNELS[KIND_COUNT];
 // Q(31-f).f with f = 20 (src/nemo/ConfigurationImpl.cpp:22)
 constexpr unsigned FRACTIONAL_BITS = 20;
 // longest firing history / STDP window (src/nemo/StdpFunction.cpp:151)

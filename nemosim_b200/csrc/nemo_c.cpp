@@ -17,6 +17,7 @@
 #include "bptt.hpp"
 #include "handles.hpp"
 #include "network.hpp"
+#include "plugins.hpp"
 #include "simulation.hpp"
 
 using namespace nemo_b200;
@@ -64,15 +65,11 @@ const char* nemo_version(void) { return "0.7.2-b200"; }
 
 const char* nemo_strerror(void) { return g_lastError.c_str(); }
 
+/* src/nemo/nemo_c.cpp:77-80, Plugin::addPath */
 nemo_status_t nemo_add_plugin_path(const char* dir)
 {
 	NULLCHECK(dir);
-	CALL({
-		struct stat st;
-		if(stat(dir, &st) != 0 || !S_ISDIR(st.st_mode)) {
-			NB_THROW(NEMO_INVALID_INPUT, "%s is not a directory", dir);
-		}
-	});
+	CALL(addPluginPath(dir));
 }
 
 nemo_status_t nemo_cuda_device_count(unsigned* count)
@@ -629,32 +626,13 @@ nemo_status_t nemo_b200_set_resident_step(nemo_simulation_t s, unsigned idle_us)
 	CALL(S(s).setResidentIdle(idle_us));
 }
 
-nemo_status_t nemo_b200_set_pipelined(nemo_simulation_t s, int on)
-{
-	NULLCHECK(s);
-	CALL(S(s).pipelined = on != 0);
-}
-
-nemo_status_t nemo_b200_set_spare_ctas(nemo_simulation_t s, unsigned ctas)
-{
-	NULLCHECK(s);
-	CALL(S(s).setSpareCtas(ctas));
-}
-
-nemo_status_t nemo_b200_get_spare_ctas(nemo_simulation_t s, unsigned* ctas)
-{
-	NULLCHECK(s);
-	NULLCHECK(ctas);
-	CALL(*ctas = S(s).spareCtas());
-}
-
 nemo_status_t nemo_b200_trace_phases(nemo_simulation_t s, unsigned steps, uint64_t* out, size_t cap,
-		unsigned* ctas, unsigned* owners)
+		unsigned* ctas)
 {
 	NULLCHECK(s);
 	NULLCHECK(out);
 	CALL({
-		const unsigned g = S(s).tracePhases(steps, out, cap, owners);
+		const unsigned g = S(s).tracePhases(steps, out, cap);
 		if(ctas) *ctas = g;
 	});
 }
@@ -714,9 +692,9 @@ nemo_status_t nemo_b200_step_events(nemo_simulation_t s, uint64_t* events)
 	CALL(*events = S(s).stepEvents);
 }
 
-unsigned nemo_b200_neuron_type_count(void) { return 4; }
+unsigned nemo_b200_neuron_type_count(void) { return KIND_COUNT; }
 
-const char* nemo_b200_neuron_type_name(unsigned i) { return i < 4 ? NEURON_TYPES[i].name : ""; }
+const char* nemo_b200_neuron_type_name(unsigned i) { return i < KIND_COUNT ? KERNELS[i].name : ""; }
 
 nemo_status_t nemo_b200_libm_calibration(uint64_t* logFlips, uint64_t* sinFlips, uint64_t* exceptions)
 {

@@ -1,5 +1,6 @@
 // network.cpp -- host-side network and configuration objects.
 #include "network.hpp"
+#include "plugins.hpp"
 
 #include <stdarg.h>
 #include <stdio.h>
@@ -19,21 +20,6 @@ std::string format(const char* fmt, ...)
 	return std::string(buf);
 }
 
-const NeuronTypeDesc NEURON_TYPES[4] = {
-	{ "Izhikevich", KIND_IZHIKEVICH, 5, 2, 1 },    // Izhikevich.ini:2-4
-	{ "IF_curr_exp", KIND_IF_CURR_EXP, 9, 4, 0 },  // IF_curr_exp.ini:14-24
-	{ "PoissonSource", KIND_POISSON, 1, 0, 0 },    // PoissonSource.ini:1-3
-	{ "Input", KIND_INPUT, 0, 0, 0 },              // Input.ini:1-3
-};
-
-const NeuronTypeDesc* find_neuron_type(const std::string& name)
-{
-	for(const NeuronTypeDesc& d : NEURON_TYPES) {
-		if(name == d.name) return &d;
-	}
-	return nullptr;
-}
-
 /* src/nemo/fixedpoint.cpp:17-28 */
 int32_t fx_toFix(float f)
 {
@@ -45,18 +31,16 @@ int32_t fx_toFix(float f)
 	return (int32_t) (f * (float) (1 << FRACTIONAL_BITS));
 }
 
-/* NetworkImpl::addNeuronType, src/nemo/NetworkImpl.cpp:37-48 */
+/* NetworkImpl::addNeuronType, src/nemo/NetworkImpl.cpp:37-48: a type seen
+ * before in this network keeps its id; a new one is read from its .ini
+ * descriptor (parseNeuronType) */
 unsigned Network::addNeuronType(const std::string& name)
 {
 	for(unsigned t = 0; t < types.size(); ++t) {
 		if(name == types[t].desc->name) return t;
 	}
-	const NeuronTypeDesc* d = find_neuron_type(name);
-	if(!d) {
-		NB_THROW(NEMO_INVALID_INPUT, "Could not find neuron type configuration file %s.ini", name.c_str());
-	}
 	NeuronCollection c;
-	c.desc = d;
+	c.desc = std::make_shared<const NeuronTypeDesc>(parseNeuronType(name));
 	types.push_back(c);
 	return (unsigned) types.size() - 1;
 }

@@ -5,6 +5,7 @@
 
 #include <stdint.h>
 
+#include <memory>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -15,7 +16,7 @@
 namespace nemo_b200 {
 
 struct NeuronCollection {
-	const NeuronTypeDesc* desc = nullptr;
+	std::shared_ptr<const NeuronTypeDesc> desc;
 	std::vector<unsigned> gidx;  // insertion order
 	std::vector<float> args;     // row-major: size() x (nparam + nstate)
 	unsigned nargs() const { return desc->nparam + desc->nstate; }

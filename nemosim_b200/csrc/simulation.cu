@@ -10,6 +10,7 @@
 #include "kernels.cuh"
 #include "hugevec.hpp"
 #include "libm_calib.hpp"
+#include "plugins.hpp"
 
 namespace nemo_b200 {
 
@@ -152,12 +153,11 @@ __device__ __forceinline__ void write_chunks(uint4* list, uint32_t pos, unsigned
 constexpr uint32_t BUCKET = 32;  // entries per bucket of a work list
 
 // group g = entries [e, e + len) = [start, start + len) of the list's array
-// of parity p
-__device__ __forceinline__ void write_group(const WorkList& L, uint32_t p, uint32_t g, uint32_t e,
-		unsigned long long start, uint32_t len)
+__device__ __forceinline__ void write_group(const WorkList& L, uint32_t g, uint32_t e, unsigned long long start,
+		uint32_t len)
 {
-	L.group[p][g] = make_uint4((uint32_t) start, (uint32_t) (start >> 32), len, e);
-	for(uint32_t b = (e + BUCKET - 1) / BUCKET; b * BUCKET < e + len; ++b) L.bucket[p][b] = g;
+	L.group[g] = make_uint4((uint32_t) start, (uint32_t) (start >> 32), len, e);
+	for(uint32_t b = (e + BUCKET - 1) / BUCKET; b * BUCKET < e + len; ++b) L.bucket[b] = g;
 }
 
 // End of source n's delay-d group (its synapses of delay <= d) within its
@@ -174,22 +174,9 @@ __device__ __forceinline__ uint32_t delay_end(const DevSim& S, uint32_t n, uint3
 struct CtaCounters {
 	uint32_t fired;
 	unsigned long long events, stdp;
-	unsigned long long resD, resA, resS;     // the warps' reservations, summed
-	unsigned long long baseD, baseA, baseS;  // the CTA's place in the delivery / ahead / STDP lists
+	unsigned long long resD, resS;    // the warps' reservations, summed
+	unsigned long long baseD, baseS;  // the CTA's place in the delivery / STDP lists
 };
-
-__device__ __forceinline__ void clear_counters(CtaCounters& C)
-{
-	C.fired = 0;
-	C.events = C.stdp = 0;
-	C.resD = C.resA = C.resS = 0;
-	C.baseD = C.baseA = C.baseS = 0;
-}
-
-// What a step's update publishes (every update publishes the delay-1
-// groups arriving next step and its STDP targets):
-constexpr uint32_t PUB_NEXT = 1;   // the groups of delay 2 and more arriving next step (into dlvWork)
-constexpr uint32_t PUB_AHEAD = 2;  // the groups of delay 2 and more arriving in two steps (into preWork)
 
 // Neuron update of step t (src/nemo/cpu/Simulation.cpp:94-111 minus the
 // delivery and STDP loops) for the neurons [first, last) of one CTA (first a
@@ -198,24 +185,18 @@ constexpr uint32_t PUB_AHEAD = 2;  // the groups of delay 2 and more arriving in
 // cur = t & 1.
 // hostFired: also write the fired bit-vector words there (host memory)
 __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, uint32_t last, uint32_t cur,
-		uint32_t ring, CtaCounters& C, uint32_t pub, bool preNoise = false, uint32_t* hostFired = nullptr)
+		uint32_t ring, CtaCounters& C, bool preNoise = false, uint32_t* hostFired = nullptr)
 {
 	const uint32_t tid = threadIdx.x, lane = tid & 31;
 	const uint64_t* histPrev = S.hist + (size_t) (cur ^ 1u) * S.N;
 	uint64_t* histCur = S.hist + (size_t) cur * S.N;
-	ulonglong2* slot = S.slot + (size_t) cur * S.N;
-	// which delays the published sets hold: bit k of the new history (fired
-	// k steps ago) with delay k + 1 arrives next step, with delay k + 2 in
-	// two steps
-	const uint64_t nextMask = (pub & PUB_NEXT) ? ~0ull : 1ull;
-	const bool ahead = (pub & PUB_AHEAD) != 0;
 
 	for(uint32_t base = first; base < last; base += blockDim.x) {
 		const uint32_t n = base + tid;
 		bool fired = false, target = false;
 		uint32_t fw = 0, outdeg = 0, indeg = 0;
 		unsigned long long ob = 0, rb = 0;
-		uint64_t pendN = 0, pendA = 0;
+		uint64_t pend = 0;
 		bool hist_nonzero = false;
 		uint32_t g1End = 0, gpD = 0, gpBeg = 0, gpEnd = 0;
 		if(n < last) {
@@ -226,7 +207,7 @@ __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, ui
 			// every load of this neuron before its first store: this step's
 			// synaptic input, stimulus, history, CSR spans, delay groups,
 			// parameters, state and RNG words
-			const ulonglong2 acc = slot[n];
+			const ulonglong2 acc = S.slot[n];
 			const float ext = S.curExt[n];
 			fw = S.fstim[n >> 5];
 			const uint64_t hp = histPrev[n];
@@ -241,17 +222,16 @@ __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, ui
 			load_neuron(S, T, nl, n, R, preNoise);
 			// the delay-group ends this neuron will most likely publish, loaded
 			// before the arithmetic: its delay-1 group (if it fires now) and
-			// the first group pending from its earlier spikes (of the set
-			// published ahead when there is one)
-			const uint64_t pendPrev = ahead ? ((hp << 1) & (dm >> 1)) : ((hp << 1) & dm & nextMask);
+			// the first group pending from its earlier spikes
+			const uint64_t pendPrev = (hp << 1) & dm;
 			if(dm & 1ull) g1End = delay_end(S, n, 1);
 			if(pendPrev) {
-				gpD = (uint32_t) __ffsll((long long) pendPrev) + (ahead ? 1u : 0u);
+				gpD = (uint32_t) __ffsll((long long) pendPrev);
 				gpBeg = delay_end(S, n, gpD - 1);
 				gpEnd = delay_end(S, n, gpD);
 			}
 
-			if(acc.x | acc.y) slot[n] = make_ulonglong2(0, 0);
+			if(acc.x | acc.y) S.slot[n] = make_ulonglong2(0, 0);
 			if(__float_as_uint(ext) != 0u) S.curExt[n] = 0.0f;
 			// wfx_toFloat of the int64 sums (src/nemo/fixedpoint.cpp:40-49)
 			const float cE = wfx_to_float((long long) acc.x);
@@ -266,10 +246,8 @@ __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, ui
 			if(fired) outdeg = (uint32_t) (o1 - o0);
 			// groups arriving next step: delay d of a source that fired d - 1
 			// steps ago (bit d - 1 of the history; dm holds only the delays
-			// the source has and deliverSpikes accepts); ahead: delay d >= 2
-			// of a source that fired d - 2 steps ago
-			pendN = h & dm & nextMask;
-			if(ahead) pendA = h & (dm >> 1);
+			// the source has and deliverSpikes accepts)
+			pend = h & dm;
 			// STDP target: fired |post| steps ago (ConnectivityMatrix.cpp:206)
 			if(S.stdp && (h & S.sp.postFireMask)) {
 				rb = r0;
@@ -285,73 +263,54 @@ __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, ui
 			S.recent[(size_t) cur * S.recentWords + (n >> 5)] = rbits;
 			if(fw) S.fstim[n >> 5] = 0u;
 		}
+		// the delay groups that arrive next step and the incoming plastic
+		// synapses of this step's STDP targets, both reserved at once
 		// range [e0, e1) of this neuron's delay-d group in its row
 		auto group = [&](uint32_t d, uint32_t& e0, uint32_t& e1) {
 			if(d == 1) { e0 = 0; e1 = g1End; }
 			else if(d == gpD) { e0 = gpBeg; e1 = gpEnd; }
 			else { e0 = delay_end(S, n, d - 1); e1 = delay_end(S, n, d); }
 		};
-		uint32_t ngD = 0, neD = 0, ngA = 0, neA = 0;
-		for(uint64_t b = pendN; b; b &= b - 1) {
+		uint32_t ngD = 0, neD = 0;
+		for(uint64_t b = pend; b; b &= b - 1) {
 			uint32_t e0, e1;
 			group((uint32_t) __ffsll((long long) b), e0, e1);
 			neD += e1 - e0;
 			++ngD;
 		}
-		for(uint64_t b = pendA; b; b &= b - 1) {
-			uint32_t e0, e1;
-			group((uint32_t) __ffsll((long long) b) + 1u, e0, e1);
-			neA += e1 - e0;
-			++ngA;
-		}
 		const uint32_t ngS = target ? 1u : 0u, neS = target ? indeg : 0u;
-		// reserve the lists for the whole CTA: warps add their totals to
+		// reserve both lists for the whole CTA: warps add their totals to
 		// shared counters, one thread reserves the CTA's share of each
-		// global list (so that warps do not queue on global addresses)
+		// global list (so that warps do not queue on two global addresses)
 		const uint32_t igD = warp_inclusive_scan(ngD), ieD = warp_inclusive_scan(neD);
-		const uint32_t igA = warp_inclusive_scan(ngA), ieA = warp_inclusive_scan(neA);
 		const uint32_t igS = warp_inclusive_scan(ngS), ieS = warp_inclusive_scan(neS);
-		unsigned long long wD = 0, wA = 0, wS = 0;
+		unsigned long long wD = 0, wS = 0;
 		if(lane == 31) {
 			if(igD | ieD) wD = atomicAdd(&C.resD, ((unsigned long long) igD << 32) | ieD);
-			if(igA | ieA) wA = atomicAdd(&C.resA, ((unsigned long long) igA << 32) | ieA);
 			if(igS | ieS) wS = atomicAdd(&C.resS, ((unsigned long long) igS << 32) | ieS);
 		}
 		__syncthreads();
 		if(tid == 0) {
 			C.baseD = C.resD ? atomicAdd(&S.dlvWork.count[cur], C.resD) : 0ull;
-			C.baseA = C.resA ? atomicAdd(&S.preWork.count[cur], C.resA) : 0ull;
 			C.baseS = C.resS ? atomicAdd(&S.stdpWork.count[cur], C.resS) : 0ull;
 			C.resD = 0;
-			C.resA = 0;
 			C.resS = 0;
 		}
 		__syncthreads();
 		wD = __shfl_sync(0xffffffffu, wD, 31);
-		wA = __shfl_sync(0xffffffffu, wA, 31);
 		wS = __shfl_sync(0xffffffffu, wS, 31);
 		if(ngD) {
 			uint32_t gD = (uint32_t) (C.baseD >> 32) + (uint32_t) (wD >> 32) + igD - ngD;
 			uint32_t eD = (uint32_t) C.baseD + (uint32_t) wD + ieD - neD;
-			for(uint64_t b = pendN; b; b &= b - 1) {
+			for(uint64_t b = pend; b; b &= b - 1) {
 				uint32_t e0, e1;
 				group((uint32_t) __ffsll((long long) b), e0, e1);
-				write_group(S.dlvWork, cur, gD++, eD, ob + e0, e1 - e0);
+				write_group(S.dlvWork, gD++, eD, ob + e0, e1 - e0);
 				eD += e1 - e0;
 			}
 		}
-		if(ngA) {
-			uint32_t gA = (uint32_t) (C.baseA >> 32) + (uint32_t) (wA >> 32) + igA - ngA;
-			uint32_t eA = (uint32_t) C.baseA + (uint32_t) wA + ieA - neA;
-			for(uint64_t b = pendA; b; b &= b - 1) {
-				uint32_t e0, e1;
-				group((uint32_t) __ffsll((long long) b) + 1u, e0, e1);
-				write_group(S.preWork, cur, gA++, eA, ob + e0, e1 - e0);
-				eA += e1 - e0;
-			}
-		}
 		if(ngS) {
-			write_group(S.stdpWork, cur, (uint32_t) (C.baseS >> 32) + (uint32_t) (wS >> 32) + igS - ngS,
+			write_group(S.stdpWork, (uint32_t) (C.baseS >> 32) + (uint32_t) (wS >> 32) + igS - ngS,
 					(uint32_t) C.baseS + (uint32_t) wS + ieS - neS, rb, indeg);
 		}
 		// targets touched in this STDP period, for applyStdp
@@ -399,10 +358,10 @@ update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t ring, uint32_t 
 	chain_wait_then_release();
 	if(fromDev) step_indices(S, offset, cur, ring);
 	__shared__ CtaCounters sC;
-	if(threadIdx.x == 0) clear_counters(sC);
+	if(threadIdx.x == 0) sC = CtaCounters{ 0, 0, 0, 0, 0, 0, 0 };
 	__syncthreads();
 	const uint32_t first = blockIdx.x * P;
-	update_range(S, first, min(S.N, first + P), cur, ring, sC, PUB_NEXT, false, hostFired);
+	update_range(S, first, min(S.N, first + P), cur, ring, sC, false, hostFired);
 	__syncthreads();
 	flush_counters(S, ring, sC);
 }
@@ -420,30 +379,34 @@ __device__ __forceinline__ void red_add_u64(unsigned long long* p, unsigned long
 	asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
 }
 
-// The entries [E0, E1) of a work list (its groups and bucket index of one
-// parity, ng groups) processed by one warp in rounds of 32 x K, each lane
-// finding the group of its entry by a binary search over 32 consecutive
-// group descriptors (one per lane).
+// One warp's share of a work list: the entries [E0, E1) of the list's
+// ne entries, in rounds of 32 x K, each lane finding the group of its entry
+// by a binary search over 32 consecutive group descriptors (one per lane).
 //  KIND 0 (delivery): add each synapse's weight into its target's
-//          accumulator in `slot` (the arrival step's): the E (w >= 0) or I
-//          (w < 0) int64 sum, as deliverSpikesOne (src/nemo/cpu/
-//          Simulation.cpp:293-307); integer addition is associative, so the
-//          sums do not depend on the order of the reductions
+//          accumulator: the E (w >= 0) or I (w < 0) int64 sum, as
+//          deliverSpikesOne (src/nemo/cpu/Simulation.cpp:293-307); integer
+//          addition is associative, so the sums do not depend on the order
+//          of the reductions
 //  KIND 1 (STDP): accumulation over the incoming plastic synapses of a
 //          target (ConnectivityMatrix::accumulateStdp,
 //          ConnectivityMatrix.cpp:193-227) with the history `hist` of the
 //          step that published the list
 template<int KIND, int K>
-__device__ __forceinline__ void process_range(const DevSim& S, const uint4* group, const uint32_t* bucket,
-		uint32_t ng, uint32_t E0, uint32_t E1, ulonglong2* slot, const uint64_t* hist, const uint32_t* recent)
+__device__ __forceinline__ void process_list(const DevSim& S, const WorkList& L, uint32_t ng, uint32_t ne,
+		const uint64_t* hist, const uint32_t* recent, uint32_t warp, uint32_t nwarps)
 {
+	if(ne == 0) return;
 	const uint32_t lane = threadIdx.x & 31;
-	uint32_t g = bucket[E0 / BUCKET];
+	const uint32_t per = (ne + nwarps - 1) / nwarps;
+	const uint32_t E0 = warp * per;
+	if(E0 >= ne) return;
+	const uint32_t E1 = min(ne, E0 + per);
+	uint32_t g = L.bucket[E0 / BUCKET];
 	for(;;) {
 		// descriptors g .. g + 31; lanes past the last group hold an offset
 		// above every entry
 		const bool valid = g + lane < ng;
-		const uint4 d = valid ? group[g + lane] : make_uint4(0, 0, 0, 0xffffffffu);
+		const uint4 d = valid ? L.group[g + lane] : make_uint4(0, 0, 0, 0xffffffffu);
 		const uint32_t lastLane = min(31u, ng - 1 - g);
 		const uint32_t coverEnd = __shfl_sync(0xffffffffu, d.w + d.z, lastLane);
 		const uint32_t lo = max(E0, __shfl_sync(0xffffffffu, d.w, 0)), hi = min(E1, coverEnd);
@@ -469,7 +432,7 @@ __device__ __forceinline__ void process_range(const DevSim& S, const uint4* grou
 				for(int j = 0; j < K; ++j) {
 					if(base + lane + 32 * j < hi) {
 						const int32_t w = (int32_t) sy[j].y;
-						unsigned long long* a = reinterpret_cast<unsigned long long*>(slot + (sy[j].x & (MAX_NEURONS - 1)));
+						unsigned long long* a = reinterpret_cast<unsigned long long*>(S.slot + (sy[j].x & (MAX_NEURONS - 1)));
 						red_add_u64(a + (w >= 0 ? 0 : 1), (unsigned long long) (long long) w);
 					}
 				}
@@ -506,37 +469,7 @@ __device__ __forceinline__ void process_range(const DevSim& S, const uint4* grou
 	}
 }
 
-// One warp's even share of the ne entries of a list (warp `warp` of `nwarps`)
-template<int KIND, int K>
-__device__ __forceinline__ void process_list(const DevSim& S, const WorkList& L, uint32_t p, uint32_t ng,
-		uint32_t ne, ulonglong2* slot, const uint64_t* hist, const uint32_t* recent, uint32_t warp, uint32_t nwarps)
-{
-	if(ne == 0) return;
-	const uint32_t per = (ne + nwarps - 1) / nwarps;
-	const uint32_t E0 = warp * per;
-	if(E0 >= ne) return;
-	process_range<KIND, K>(S, L.group[p], L.bucket[p], ng, E0, min(ne, E0 + per), slot, hist, recent);
-}
-
-// Chunks of CH entries of a list claimed by the warp from a counter until
-// none is left: warps that arrive early take more.
-template<int KIND, int K, uint32_t CH>
-__device__ __forceinline__ void process_claimed(const DevSim& S, const WorkList& L, uint32_t p, uint32_t ng,
-		uint32_t ne, ulonglong2* slot, const uint64_t* hist, const uint32_t* recent, unsigned long long* counter)
-{
-	if(ne == 0) return;
-	const uint32_t lane = threadIdx.x & 31;
-	for(;;) {
-		unsigned long long e0 = 0;
-		if(lane == 0) e0 = atomicAdd(counter, (unsigned long long) CH);
-		e0 = __shfl_sync(0xffffffffu, e0, 0);
-		if(e0 >= ne) return;
-		process_range<KIND, K>(S, L.group[p], L.bucket[p], ng, (uint32_t) e0, (uint32_t) min((unsigned long long) ne,
-				e0 + CH), slot, hist, recent);
-	}
-}
-
-// what a pre-phase of the two-launch step does
+// what a pre-phase does
 constexpr uint32_t PHASE_DELIVER = 1;  // the published delay groups
 constexpr uint32_t PHASE_STDP = 2;     // the published STDP groups
 constexpr uint32_t PHASE_RESET = 4;    // empty the lists the next update publishes into
@@ -558,8 +491,6 @@ __device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uin
 		S.stdpWork.count[pub ^ 1u] = 0;
 	}
 	const uint64_t* hist = S.hist + (size_t) pub * S.N;
-	// the arrivals go to the accumulators of the step after the publishing one
-	ulonglong2* slot = S.slot + (size_t) (pub ^ 1u) * S.N;
 	// CTAs [0, gs) take the STDP list, [gs, gridDim.x) the deliveries, in
 	// proportion to their work: an STDP entry costs about STDP_ENTRY_COST
 	// delivery entries (measured per CTA at 100k x 1000: with a weight of 2
@@ -576,8 +507,8 @@ __device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uin
 	const bool doDlv = nd && (blockIdx.x >= gs || gridDim.x == 1);
 	if(doDlv) {
 		const uint32_t first = gridDim.x == 1 ? 0u : gs;
-		process_list<0, 8>(S, S.dlvWork, pub, (uint32_t) (cd >> 32), nd, slot, nullptr, nullptr,
-				(blockIdx.x - first) * wpc + lw, (gridDim.x - first) * wpc);
+		process_list<0, 8>(S, S.dlvWork, (uint32_t) (cd >> 32), nd, hist, nullptr, (blockIdx.x - first) * wpc + lw,
+				(gridDim.x - first) * wpc);
 	}
 	// the sources' "fired in the last 64 steps" bits, copied to shared
 	// memory with asynchronous 16-byte copies
@@ -595,7 +526,7 @@ __device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uin
 	__syncthreads();
 	if(doStdp) {
 		const uint32_t cstdp = gridDim.x == 1 ? 1u : gs;
-		process_list<1, 4>(S, S.stdpWork, pub, (uint32_t) (cs >> 32), ns, nullptr, hist, filter ? sRecent : nullptr,
+		process_list<1, 4>(S, S.stdpWork, (uint32_t) (cs >> 32), ns, hist, filter ? sRecent : nullptr,
 				blockIdx.x * wpc + lw, cstdp * wpc);
 	}
 	__syncthreads();  // the shared copy is rewritten by the next call
@@ -712,153 +643,82 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, uint32_t& target, 
 	return ok != 0;
 }
 
-// One step of the persistent loops at cycle t (c).  Its CTAs are the owners
-// of the partitions (CTA c owns partitions c, c + gridDim.x, ... of P
-// neurons) and, beyond them, spare CTAs.
-//
-//  1. Every CTA takes its even share of the deliveries arriving now
-//     (dlvWork of the last update) into the accumulators of step t, then
-//     arrives at a grid barrier.
-//  2. The owners compute this step's noise while the barrier completes,
-//     wait for it and update their neurons, which publishes the delay-1
-//     groups arriving next step, the STDP targets and, by `pub`, the other
-//     delays arriving next step (PUB_NEXT, into dlvWork) or the other
-//     delays arriving in two steps (PUB_AHEAD, into preWork).
-//  3. The spare CTAs at once, and the owners after their update, claim in
-//     chunks the work that no update waits for: the STDP accumulation of
-//     the last step (stdpWork) and, with `ahead`, the deliveries arriving
-//     next step that the last update published ahead (preWork, into the
-//     accumulators of step t + 1).  A grid barrier ends the step.
-//
-// Deliveries read the weights when they are made, so a delivery made ahead
-// is made only when no applyStdp can come between it and its arrival
-// (run_kernel chooses `ahead` and `pub` per step).  Every delivery group is
-// made exactly once; the sums are integer and do not depend on the order of
-// the reductions, and every STDP entry is updated by one lane, so the
-// results are those of deliver_kernel + update_kernel per step.  Returns
-// false when a barrier wait gave up.
+// Persistent step loop: `steps` consecutive steps from cycle `cycle0` in one
+// cooperative launch, each step's pre-phase and update separated by grid
+// barriers, then the STDP accumulation of the last step (so applyStdp may
+// follow directly; its deliveries stay pending for the next step).  CTA c
+// owns the partitions c, c + gridDim.x, ... of P neurons; the pre-phases
+// spread the work lists over all CTAs of the grid.  After each pre-phase
+// the CTAs compute the step's noise while the barrier completes.
+// Identical results to deliver_kernel + update_kernel per step.
+// base: the barrier counter's value when the launch starts.  Without
+// finalStdp the last step's STDP accumulation is left to the next
+// pre-phase, as after a two-launch step.  stim (the first step's stimulus,
+// apply_stimulus) and hostFired (the last step's fired words) serve
+// nemo_step.
+// One step of the persistent loop at cycle c (the pre-phase, the noise in
+// the shadow of its barrier, the update), ending at a grid barrier; false
+// when a barrier wait gave up.
 __device__ __forceinline__ bool persistent_step(const DevSim& S, uint32_t P, unsigned long long c, GridBarrier* gb,
 		uint32_t& sTarget, uint32_t& sOk, CtaCounters& sC, const uint32_t* stim, uint32_t nf, uint32_t ni,
-		uint32_t* hostFired, uint32_t pub, bool ahead, uint32_t row = ~0u)
+		uint32_t* hostFired, uint32_t row = ~0u)
 {
 	trace_mark(S, row, 0);
 	__shared__ uint32_t sRng[4 * NOISE_STAGE];
 	__shared__ float sSigma[NOISE_STAGE];
-	extern __shared__ __align__(16) uint32_t sRecent[];
 	const uint32_t nparts = (S.N + P - 1) / P;
-	const uint32_t cur = (uint32_t) (c & 1), prev = cur ^ 1u;
+	const uint32_t cur = (uint32_t) (c & 1);
 	const uint32_t ring = (uint32_t) (c % S.R);
-	const bool owner = blockIdx.x < nparts;
 	// one partition of at most one neuron per thread: its noise inputs are
-	// copied to shared memory while the deliveries run
+	// copied to shared memory while the pre-phase runs
 	const bool staged = nparts <= gridDim.x && P <= blockDim.x && P <= NOISE_STAGE;
-	if(staged && owner) stage_noise_inputs(S, blockIdx.x * P, min(S.N, blockIdx.x * P + P), sRng, sSigma);
-	// the sources' "fired in the last 64 steps" bits for the STDP filter
-	const unsigned long long cs = S.stdpWork.count[prev];
-	const bool filter = cs != 0 && S.recentBytes != 0;
-	if(filter) {
-		const uint32_t* g = S.recent + (size_t) prev * S.recentWords;
-		for(uint32_t q = threadIdx.x; q < S.recentWords / 4; q += blockDim.x) {
-			const uint32_t dst = (uint32_t) __cvta_generic_to_shared(sRecent + 4 * q);
-			asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(g + 4 * q) : "memory");
-		}
-		asm volatile("cp.async.commit_group;" ::: "memory");
+	if(staged && blockIdx.x < nparts) {
+		stage_noise_inputs(S, blockIdx.x * P, min(S.N, blockIdx.x * P + P), sRng, sSigma);
 	}
 	if(stim) apply_stimulus(S, stim, nf, ni);
-	// empty the lists this step's update publishes into (their last readers
-	// finished in the last step) and the next step's claim counters (their
-	// last users finished in the step before)
-	if(blockIdx.x == 0 && threadIdx.x == 0) {
-		S.dlvWork.count[cur] = 0;
-		S.preWork.count[cur] = 0;
-		S.stdpWork.count[cur] = 0;
-		S.claim[2 * prev] = 0;
-		S.claim[2 * prev + 1] = 0;
-	}
-	{
-		const unsigned long long cd = S.dlvWork.count[prev];
-		const uint32_t wpc = blockDim.x >> 5;
-		process_list<0, 8>(S, S.dlvWork, prev, (uint32_t) (cd >> 32), (uint32_t) cd, S.slot + (size_t) cur * S.N,
-				nullptr, nullptr, blockIdx.x * wpc + (threadIdx.x >> 5), gridDim.x * wpc);
-	}
-	if(staged || filter) asm volatile("cp.async.wait_all;" ::: "memory");
+	deliver_range(S, cur ^ 1u, PHASE_DELIVER | PHASE_STDP | PHASE_RESET);
+	if(staged) asm volatile("cp.async.wait_all;" ::: "memory");
+	// while the other CTAs finish the pre-phase: this step's noise of this
+	// CTA's neurons (it depends on their RNG words only)
 	grid_arrive(gb, sTarget);
 	trace_mark(S, row, 1);
-	if(owner) {
-		// while the other CTAs finish the deliveries: this step's noise of
-		// this CTA's neurons (it depends on their RNG words only)
-		if(staged) {
+	if(staged) {
+		if(blockIdx.x < nparts) {
 			precompute_noise_staged(S, blockIdx.x * P, min(S.N, blockIdx.x * P + P), sRng, sSigma);
-		} else {
-			for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) precompute_noise(S, p * P, min(S.N, p * P + P));
 		}
-		if(!grid_wait(gb, sTarget, sOk, S.waitLimit)) return false;
-		trace_mark(S, row, 2);
-		for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
-			update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC, pub, true, hostFired);
-		}
-		__syncthreads();
-		flush_counters(S, ring, sC);
-		trace_mark(S, row, 3);
+	} else {
+		for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) precompute_noise(S, p * P, min(S.N, p * P + P));
 	}
-	{
-		const unsigned long long ca = ahead ? S.preWork.count[prev] : 0ull;
-		unsigned long long* claim = S.claim + 2 * cur;
-		process_claimed<1, 4, 256>(S, S.stdpWork, prev, (uint32_t) (cs >> 32), (uint32_t) cs, nullptr,
-				S.hist + (size_t) prev * S.N, filter ? sRecent : nullptr, claim);
-		process_claimed<0, 8, 256>(S, S.preWork, prev, (uint32_t) (ca >> 32), (uint32_t) ca,
-				S.slot + (size_t) prev * S.N, nullptr, nullptr, claim + 1);
+	if(!grid_wait(gb, sTarget, sOk, S.waitLimit)) return false;
+	trace_mark(S, row, 2);
+	for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
+		update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC, true, hostFired);
 	}
-	grid_arrive(gb, sTarget);
+	__syncthreads();
+	flush_counters(S, ring, sC);
+	trace_mark(S, row, 3);
+	const bool ok = grid_barrier(gb, sTarget, sOk, S.waitLimit);
 	trace_mark(S, row, 4);
-	const bool ok = grid_wait(gb, sTarget, sOk, S.waitLimit);
-	trace_mark(S, row, 5);
 	return ok;
 }
 
-// What step k of a launch of n steps does (pipelined: deliveries of delay 2
-// and more made a step ahead).  Step k makes ahead the deliveries arriving
-// at k + 1 only when k + 1 is in the launch (applyStdp may follow the last
-// step) and step k - 1 published them ahead; a step publishes ahead exactly
-// what the next step makes ahead, and publishes for the next step every
-// delay that no step makes ahead.  The first step starts from, and the last
-// step leaves, the state of the two-launch step.
-__device__ __forceinline__ void step_mode(uint32_t k, uint32_t n, int pipelined, uint32_t& pub, bool& ahead)
-{
-	ahead = pipelined && k >= 1 && k + 2 <= n;
-	const bool aheadNext = pipelined && k + 3 <= n;
-	pub = (ahead ? 0u : PUB_NEXT) | (aheadNext ? PUB_AHEAD : 0u);
-}
-
-// Persistent step loop: `steps` consecutive steps from cycle `cycle0` in one
-// cooperative launch (persistent_step), then the STDP accumulation of the
-// last step, so that applyStdp may follow directly; its deliveries stay
-// pending for the next step, so they read the weights applyStdp leaves.
-// base: the barrier counter's value when the launch starts.  Without
-// finalStdp the last step's STDP accumulation is left to the next step, as
-// after a two-launch step.  stim (the first step's stimulus,
-// apply_stimulus) and hostFired (the last step's fired words) serve
-// nemo_step.  Two instances: up to 768 threads per CTA (80 registers), and
-// up to 256 threads with four CTAs per SM (64 registers).
-template<unsigned MAXT, unsigned MINB>
-__global__ void __launch_bounds__(MAXT, MINB)
+// TRACE: the instance with the phase trace (tracePhases)
+template<bool TRACE>
+__global__ void __launch_bounds__(RUN_THREADS, 1)
 run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0, GridBarrier* gb, uint32_t base,
-		int finalStdp, const uint32_t* stim, uint32_t nf, uint32_t ni, uint32_t* hostFired, int pipelined)
+		int finalStdp, const uint32_t* stim, uint32_t nf, uint32_t ni, uint32_t* hostFired)
 {
 	__shared__ CtaCounters sC;
 	__shared__ uint32_t sTarget, sOk;
 	if(threadIdx.x == 0) {
-		clear_counters(sC);
+		sC = CtaCounters{ 0, 0, 0, 0, 0, 0, 0 };
 		sTarget = base;
 		sOk = 1;
 	}
 	__syncthreads();
 	for(uint32_t k = 0; k < steps; ++k) {
-		uint32_t pub;
-		bool ahead;
-		step_mode(k, steps, pipelined, pub, ahead);
 		if(!persistent_step(S, P, cycle0 + k, gb, sTarget, sOk, sC, k == 0 ? stim : nullptr, nf, ni,
-				k + 1 == steps ? hostFired : nullptr, pub, ahead, S.trace && k < S.traceSteps ? k : ~0u)) {
+				k + 1 == steps ? hostFired : nullptr, TRACE && k < S.traceSteps ? k : ~0u)) {
 			return;
 		}
 	}
@@ -1026,15 +886,14 @@ __device__ __forceinline__ uint32_t wait_request(GridBarrier* gb, uint32_t want,
 	return sCmd;
 }
 
-template<unsigned MAXT, unsigned MINB>
-__global__ void __launch_bounds__(MAXT, MINB)
+__global__ void __launch_bounds__(RUN_THREADS, 1)
 serve_kernel(const DevSim S, uint32_t P, unsigned long long cycle0, GridBarrier* gb, ServeCtl* ctl, uint32_t seq0,
 		const uint32_t* stim, uint32_t* hostIds, unsigned long long idleNs)
 {
 	__shared__ CtaCounters sC;
 	__shared__ uint32_t sTarget, sOk;
 	if(threadIdx.x == 0) {
-		clear_counters(sC);
+		sC = CtaCounters{ 0, 0, 0, 0, 0, 0, 0 };
 		sTarget = 0;
 		sOk = 1;
 	}
@@ -1079,11 +938,7 @@ serve_kernel(const DevSim S, uint32_t P, unsigned long long cycle0, GridBarrier*
 		if(!op) return;
 		const uint32_t nf = *(volatile uint32_t*) &gb->nf;
 		const uint32_t ni = *(volatile uint32_t*) &gb->ni;
-		// applyStdp may come between any two requests: nothing is made ahead
-		if(!persistent_step(S, P, c, gb, sTarget, sOk, sC, nf + ni ? stim : nullptr, nf, ni, nullptr, PUB_NEXT,
-				false)) {
-			return;
-		}
+		if(!persistent_step(S, P, c, gb, sTarget, sOk, sC, nf + ni ? stim : nullptr, nf, ni, nullptr)) return;
 		// CTA 0 answers: the step's fired ids and events (after the step's
 		// final barrier every CTA's words and counts are in place)
 		if(blockIdx.x == 0) {
@@ -1098,21 +953,6 @@ serve_kernel(const DevSim S, uint32_t P, unsigned long long cycle0, GridBarrier*
 			}
 		}
 	}
-}
-
-// The instances of the persistent loops for a block size
-using RunKernel = void (*)(const DevSim, uint32_t, uint32_t, unsigned long long, GridBarrier*, uint32_t, int,
-		const uint32_t*, uint32_t, uint32_t, uint32_t*, int);
-using ServeKernel = void (*)(const DevSim, uint32_t, unsigned long long, GridBarrier*, ServeCtl*, uint32_t,
-		const uint32_t*, uint32_t*, unsigned long long);
-constexpr uint32_t RUN_THREADS_SMALL = 256;
-static RunKernel run_kernel_for(uint32_t threads)
-{
-	return threads <= RUN_THREADS_SMALL ? run_kernel<RUN_THREADS_SMALL, 4> : run_kernel<RUN_THREADS, 1>;
-}
-static ServeKernel serve_kernel_for(uint32_t threads)
-{
-	return threads <= RUN_THREADS_SMALL ? serve_kernel<RUN_THREADS_SMALL, 4> : serve_kernel<RUN_THREADS, 1>;
 }
 
 // Turns the targets touched since the last applyStdp (a bit-vector) into
@@ -1468,6 +1308,11 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 			NB_THROW(NEMO_API_UNSUPPORTED, "A batched network may not have a maximum delay of exactly 64 ms");
 		}
 		if(net.duplicate) NB_THROW(NEMO_INVALID_INPUT, "Duplicate neuron index %u", net.duplicateIdx);
+		// each type's kernel (where the reference loads the type's CUDA
+		// plugin, src/nemo/cuda/Neurons.cpp:43)
+		for(const NeuronCollection& c : net.types) {
+			if(c.size()) checkKernelBinding(*c.desc);
+		}
 		totalN += n;
 		maxDelay = std::max(maxDelay, net.maxDelay);
 	}
@@ -1529,7 +1374,15 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	bool needCalib = false;
 	for(NeuronKind kind : kinds) {
 		HostType ht;
-		ht.desc = &NEURON_TYPES[kind];
+		for(const Network* np : nets) {
+			for(const NeuronCollection& c : np->types) {
+				if(c.size() && c.desc->kind == kind) {
+					ht.desc = *c.desc;
+					break;
+				}
+			}
+			if(ht.desc.kind == kind) break;
+		}
 		ht.netType = 0;
 		ht.base = l;
 		ht.n = 0;
@@ -1538,7 +1391,7 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 				if(nets[i]->types[t].desc->kind == kind) ht.n += (unsigned) nets[i]->types[t].size();
 			}
 		}
-		const unsigned np = ht.desc->nparam, ns = ht.desc->nstate, na = np + ns;
+		const unsigned np = ht.desc.nparam, ns = ht.desc.nstate, na = np + ns;
 		std::vector<float> param((size_t) np * ht.n), state((size_t) ns * ht.n);
 		unsigned i0 = 0;
 		for(size_t i = 0; i < nets.size(); ++i) {
@@ -1760,24 +1613,13 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 		if(Sn >= (1ull << 32) || plastic >= (1ull << 32) || dlvGroups >= (1ull << 32)) {
 			NB_THROW(NEMO_API_UNSUPPORTED, "network too large for the work lists");
 		}
-		// one array for a list consumed before the next step publishes into
-		// it, one per parity for a list consumed while it does
-		auto makeList = [&](WorkList& L, uint64_t groups, uint64_t entries, bool twoArrays) {
+		auto makeList = [&](WorkList& L, uint64_t groups, uint64_t entries) {
+			L.group = dalloc<uint4>(groups);
 			L.count = dalloc<unsigned long long>(2);
-			for(int p = 0; p < 2; ++p) {
-				if(p == 1 && !twoArrays) {
-					L.group[1] = L.group[0];
-					L.bucket[1] = L.bucket[0];
-					break;
-				}
-				L.group[p] = dalloc<uint4>(groups);
-				L.bucket[p] = dalloc<uint32_t>(entries / BUCKET + 1);
-			}
+			L.bucket = dalloc<uint32_t>(entries / BUCKET + 1);
 		};
-		makeList(S.dlvWork, dlvGroups, Sn, false);
-		makeList(S.preWork, dlvGroups, Sn, true);
-		makeList(S.stdpWork, N, plastic, true);
-		S.claim = dalloc<unsigned long long>(4);
+		makeList(S.dlvWork, dlvGroups, Sn);
+		makeList(S.stdpWork, N, plastic);
 		uint64_t capA = 0;
 		for(unsigned n = 0; n < N; ++n) capA += (rcmPtr[n + 1] - rcmPtr[n] + CHUNK - 1) / CHUNK;
 		S.applyChunks = dalloc<uint4>(capA);
@@ -1808,7 +1650,7 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	S.fstim = dalloc<uint32_t>(S.W);
 	S.touchedBits = dalloc<uint32_t>(S.W);
 	S.curExt = dalloc<float>(N);
-	S.slot = dalloc<ulonglong2>(2 * (size_t) N);
+	S.slot = dalloc<ulonglong2>(N);
 	S.l2g = dalloc<uint32_t>(N);
 	NB_CUDA(cudaMemcpy(S.l2g, m_l2g.data(), (size_t) N * 4, cudaMemcpyHostToDevice));
 	S.l2gIdentity = 1;
@@ -1854,14 +1696,10 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	{
 		int coop = 0;
 		NB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, m_device));
-		// the default shape: CTAs of 256 threads, four per SM, one of them
-		// spare on each SM when the network fills the others
-		m_runT = RUN_THREADS_SMALL;
+		m_runT = 384;  // the default shape: two CTAs of 384 threads per SM
 		m_runGrid = coop ? runGridFor(m_runT) : 0;
 		if(m_runGrid) {
-			m_runD = m_runGrid > 2u * (unsigned) m_sms ? (unsigned) m_sms : 0u;
-			const size_t owners = m_runGrid - m_runD;
-			const size_t per = (N + owners - 1) / owners;
+			const size_t per = (N + m_runGrid - 1) / m_runGrid;
 			m_runP = (uint32_t) std::max<size_t>(32, (per + 31) & ~(size_t) 31);
 			m_barrier = dalloc<GridBarrier>(1);
 			NB_CUDA(cudaMallocHost(&m_hBarrierError, 4));
@@ -1942,25 +1780,10 @@ unsigned Simulation::runGridFor(uint32_t T) const
 	// run_kernel and serve_kernel (the resident loop of nemo_step) share
 	// the launch shape
 	int perSm = 0, perSmServe = 0;
-	NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, run_kernel_for(T), (int) T, m_dev.recentBytes));
-	NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmServe, serve_kernel_for(T), (int) T,
-			m_dev.recentBytes));
+	NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, run_kernel<false>, (int) T, m_dev.recentBytes));
+	NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmServe, serve_kernel, (int) T, m_dev.recentBytes));
 	perSm = std::min(perSm, perSmServe);
 	return perSm > 0 ? (unsigned) perSm * (unsigned) m_sms : 0u;
-}
-
-// CTAs of a launch of the persistent loops: the owners of the partitions
-// (at most the co-resident CTAs) and up to m_runD spare CTAs
-unsigned Simulation::runGridSize() const
-{
-	const uint64_t nparts = ((uint64_t) m_N + m_runP - 1) / m_runP;
-	return (unsigned) std::min<uint64_t>(m_runGrid, std::max<uint64_t>(1, nparts + m_runD));
-}
-
-void Simulation::setSpareCtas(uint32_t D)
-{
-	stopServe();
-	m_runD = std::min<uint32_t>(D, 1u << 20);
 }
 
 void Simulation::setLaunch(uint32_t P, uint32_t T)
@@ -2027,7 +1850,9 @@ void Simulation::launchRun(unsigned n, bool finalStdp, const uint32_t* stim, uin
 	uint32_t P = m_runP, steps = n;
 	unsigned long long c0 = m_cycle;
 	GridBarrier* gb = m_barrier;
-	const unsigned grid = runGridSize();
+	// no more CTAs than partitions (a CTA without one only takes part in the
+	// delivery phase, which the other CTAs' warps cover as well)
+	const unsigned grid = (unsigned) std::min<uint64_t>(m_runGrid, std::max<uint64_t>(1, (m_N + P - 1) / P));
 	// the barrier counter runs on across launches; restart it well before
 	// it could wrap
 	const uint64_t arrivals = (uint64_t) grid * (2ull * n + (finalStdp ? 1 : 0));
@@ -2039,12 +1864,10 @@ void Simulation::launchRun(unsigned n, bool finalStdp, const uint32_t* stim, uin
 	}
 	uint32_t base = (uint32_t) m_barrierBase;
 	int fin = finalStdp ? 1 : 0;
-	int pipe = pipelined ? 1 : 0;
-	void* args[] = { &dev, &P, &steps, &c0, &gb, &base, &fin, &stim, &nf, &ni, &hostFired, &pipe };
-	NB_CUDA(cudaMemsetAsync(m_dev.claim, 0, 4 * sizeof(unsigned long long), m_stream));
+	void* args[] = { &dev, &P, &steps, &c0, &gb, &base, &fin, &stim, &nf, &ni, &hostFired };
 	timedBegin(K_RUN);
-	NB_CUDA(cudaLaunchCooperativeKernel((const void*) run_kernel_for(m_runT), dim3(grid), dim3(m_runT), args,
-			m_dev.recentBytes, m_stream));
+	const void* kernel = m_dev.trace ? (const void*) run_kernel<true> : (const void*) run_kernel<false>;
+	NB_CUDA(cudaLaunchCooperativeKernel(kernel, dim3(grid), dim3(m_runT), args, m_dev.recentBytes, m_stream));
 	timedEnd();
 	m_barrierBase += arrivals;
 	m_cycle += n;
@@ -2172,11 +1995,10 @@ void Simulation::launchServe()
 	const uint32_t* stim = m_dStimMapped;
 	uint32_t* hf = m_dFiredIdsMapped;
 	unsigned long long idleNs = (unsigned long long) residentIdleUs * 1000ull;
-	const unsigned grid = runGridSize();
+	const unsigned grid = (unsigned) std::min<uint64_t>(m_runGrid, std::max<uint64_t>(1, (m_N + P - 1) / P));
 	void* args[] = { &dev, &P, &c0, &gb, &ctl, &seq0, &stim, &hf, &idleNs };
-	NB_CUDA(cudaMemsetAsync(m_dev.claim, 0, 4 * sizeof(unsigned long long), m_stream));
-	NB_CUDA(cudaLaunchCooperativeKernel((const void*) serve_kernel_for(m_runT), dim3(grid), dim3(m_runT), args,
-			m_dev.recentBytes, m_stream));
+	NB_CUDA(cudaLaunchCooperativeKernel((const void*) serve_kernel, dim3(grid), dim3(m_runT), args, m_dev.recentBytes,
+			m_stream));
 	NB_CUDA(cudaEventRecord(m_serveEnd, m_stream));
 	m_serving = true;
 	m_barrierUsed = true;
@@ -2508,28 +2330,21 @@ float Simulation::autotune(unsigned trialSteps)
 	trialSteps = std::max(1u, trialSteps);
 	// the state that trial steps modify
 	std::vector<std::pair<void*, size_t>> regions;
-	for(const HostType& t : m_types) regions.emplace_back(t.dState, (size_t) t.n * t.desc->nstate * 4);
+	for(const HostType& t : m_types) regions.emplace_back(t.dState, (size_t) t.n * t.desc.nstate * 4);
 	regions.emplace_back(m_dev.rng, (size_t) 4 * m_N * 4);
 	regions.emplace_back(m_dev.hist, (size_t) 2 * m_N * 8);
 	regions.emplace_back(m_dev.recent, (size_t) 2 * m_dev.recentWords * 4);
 	regions.emplace_back(m_dev.fstim, (size_t) m_dev.W * 4);
 	regions.emplace_back(m_dev.curExt, (size_t) m_N * 4);
-	regions.emplace_back(m_dev.slot, (size_t) 2 * m_N * 16);
-	// the work lists published by the last step (pending for the next;
-	// between launches nothing is pending in the list of deliveries made
-	// ahead)
+	regions.emplace_back(m_dev.slot, (size_t) m_N * 16);
+	// the work lists published by the last step (pending for the next)
 	for(const WorkList* L : { &m_dev.dlvWork, &m_dev.stdpWork }) {
 		unsigned long long c[2];
 		NB_CUDA(cudaMemcpy(c, L->count, 16, cudaMemcpyDeviceToHost));
-		for(int p = 0; p < 2; ++p) {
-			const bool shared = L->group[1] == L->group[0];
-			const uint64_t groups = shared ? std::max(c[0] >> 32, c[1] >> 32) : c[p] >> 32;
-			const uint64_t entries = shared ? std::max(c[0] & 0xffffffffull, c[1] & 0xffffffffull)
-					: c[p] & 0xffffffffull;
-			regions.emplace_back(L->group[p], (size_t) groups * 16);
-			regions.emplace_back(L->bucket[p], (size_t) (entries / BUCKET + 1) * 4);
-			if(shared) break;
-		}
+		const uint64_t groups = std::max(c[0] >> 32, c[1] >> 32);
+		const uint64_t entries = std::max(c[0] & 0xffffffffull, c[1] & 0xffffffffull);
+		regions.emplace_back(L->group, (size_t) groups * 16);
+		regions.emplace_back(L->bucket, (size_t) (entries / BUCKET + 1) * 4);
 		regions.emplace_back(L->count, 16);
 	}
 	if(m_dev.stdp) regions.emplace_back(m_dev.rcmAcc, (size_t) lastPlastic * 4);
@@ -2563,30 +2378,17 @@ float Simulation::autotune(unsigned trialSteps)
 		m_stdpPending = stdpPending;
 	};
 
-	// candidate shapes: partition size, threads per CTA, spare CTAs of the
-	// persistent loops
-	struct Shape {
-		uint32_t P, T, D;
-		bool operator==(const Shape& o) const { return P == o.P && T == o.T && D == o.D; }
-	};
-	std::vector<Shape> cands;
+	std::vector<std::pair<uint32_t, uint32_t>> cands;
 	const bool pers = persistentActive();
 	if(pers) {
-		// persistent loop: 256 to RUN_THREADS threads per CTA, 1 or 2
-		// partitions per owner, none to two spare CTAs per SM
-		for(uint32_t T : {RUN_THREADS_SMALL, 384u, RUN_THREADS}) {
+		// persistent loop: 256 to RUN_THREADS threads per CTA, 1 to 4 partitions per CTA
+		for(uint32_t T : {256u, 384u, RUN_THREADS}) {
 			const unsigned g = runGridFor(T);
 			if(!g) continue;
-			for(unsigned dps : {0u, 1u, 2u}) {
-				const uint32_t D = dps * (uint32_t) m_sms;
-				if(D && D * 2 > g) continue;
-				for(unsigned k : {1u, 2u}) {
-					const size_t owners = (size_t) k * (g - D);
-					uint32_t P = (uint32_t) ((m_N + owners - 1) / owners);
-					P = std::max<uint32_t>(32, (P + 31) & ~31u);
-					const Shape c{ P, T, D };
-					if(std::find(cands.begin(), cands.end(), c) == cands.end()) cands.push_back(c);
-				}
+			for(unsigned k : {1u, 2u, 4u}) {
+				uint32_t P = (uint32_t) ((m_N + (size_t) k * g - 1) / ((size_t) k * g));
+				P = std::max<uint32_t>(32, (P + 31) & ~31u);
+				if(std::find(cands.begin(), cands.end(), std::make_pair(P, T)) == cands.end()) cands.emplace_back(P, T);
 			}
 		}
 	} else {
@@ -2596,18 +2398,16 @@ float Simulation::autotune(unsigned trialSteps)
 			P = std::max<uint32_t>(32, std::min<uint32_t>(MAX_PARTITION, (P + 31) & ~31u));
 			for(uint32_t T : {128u, 256u, 512u, 1024u}) {
 				if(T > std::max<uint32_t>(128, P)) continue;
-				const Shape c{ P, T, m_runD };
-				if(std::find(cands.begin(), cands.end(), c) == cands.end()) cands.push_back(c);
+				if(std::find(cands.begin(), cands.end(), std::make_pair(P, T)) == cands.end()) cands.emplace_back(P, T);
 			}
 		}
 	}
-	const uint32_t P0 = partition(), T0 = threads(), D0 = m_runD;
+	const uint32_t P0 = partition(), T0 = threads();
 	float best = -1;
-	uint32_t bestP = P0, bestT = T0, bestD = D0;
+	uint32_t bestP = P0, bestT = T0;
 	try {
 		for(auto& c : cands) {
-			setLaunch(c.P, c.T);
-			m_runD = c.D;
+			setLaunch(c.first, c.second);
 			// untimed warm-up of this shape
 			if(pers) launchRun(1);
 			else launchStep(false);
@@ -2627,7 +2427,6 @@ float Simulation::autotune(unsigned trialSteps)
 				best = ms;
 				bestP = partition();
 				bestT = threads();
-				bestD = m_runD;
 			}
 			restore();
 		}
@@ -2636,7 +2435,6 @@ float Simulation::autotune(unsigned trialSteps)
 		sync();
 		for(void* b : backup) if(b) cudaFree(b);
 		setLaunch(P0, T0);
-		m_runD = D0;
 		profiling = prof;
 		throw;
 	}
@@ -2644,15 +2442,14 @@ float Simulation::autotune(unsigned trialSteps)
 	for(void* b : backup) if(b) cudaFree(b);
 	profiling = prof;
 	setLaunch(bestP, bestT);
-	m_runD = bestD;
 	return best * 1e3f / trialSteps;
 }
 
-unsigned Simulation::tracePhases(unsigned steps, uint64_t* out, size_t cap, unsigned* owners)
+unsigned Simulation::tracePhases(unsigned steps, uint64_t* out, size_t cap)
 {
 	NB_CUDA(cudaSetDevice(m_device));
 	if(!persistentActive()) NB_THROW(NEMO_API_UNSUPPORTED, "the phase trace needs the persistent step loop");
-	const unsigned grid = runGridSize();
+	const unsigned grid = (unsigned) std::min<uint64_t>(m_runGrid, std::max<uint64_t>(1, (m_N + m_runP - 1) / m_runP));
 	const size_t n = (size_t) steps * grid * TRACE_MARKS;
 	if(cap < n) NB_THROW(NEMO_BUFFER_OVERFLOW, "trace buffer too small: %zu values needed", n);
 	sync();
@@ -2677,7 +2474,6 @@ unsigned Simulation::tracePhases(unsigned steps, uint64_t* out, size_t cap, unsi
 	if(err == cudaSuccess) err = cudaMemcpy(out, d, n * 8, cudaMemcpyDeviceToHost);
 	cudaFree(d);
 	NB_CUDA(err);
-	if(owners) *owners = (unsigned) std::min<uint64_t>(grid, ((uint64_t) m_N + m_runP - 1) / m_runP);
 	return grid;
 }
 
@@ -2685,7 +2481,7 @@ float Simulation::getNeuronState(unsigned g, unsigned var)
 {
 	const HostType* t; unsigned i;
 	locate(g, &t, &i);
-	if(var >= t->desc->nstate) NB_THROW(NEMO_INVALID_INPUT, "Invalid state variable index %u", var);
+	if(var >= t->desc.nstate) NB_THROW(NEMO_INVALID_INPUT, "Invalid state variable index %u", var);
 	float v;
 	NB_CUDA(cudaSetDevice(m_device));
 	NB_CUDA(cudaMemcpyAsync(&v, t->dState + (size_t) var * t->n + i, 4, cudaMemcpyDeviceToHost, m_stream));
@@ -2697,7 +2493,7 @@ float Simulation::getNeuronParameter(unsigned g, unsigned p)
 {
 	const HostType* t; unsigned i;
 	locate(g, &t, &i);
-	if(p >= t->desc->nparam) NB_THROW(NEMO_INVALID_INPUT, "Invalid parameter index %u", p);
+	if(p >= t->desc.nparam) NB_THROW(NEMO_INVALID_INPUT, "Invalid parameter index %u", p);
 	float v;
 	NB_CUDA(cudaSetDevice(m_device));
 	NB_CUDA(cudaMemcpyAsync(&v, t->dParam + (size_t) p * t->n + i, 4, cudaMemcpyDeviceToHost, m_stream));
@@ -2709,14 +2505,14 @@ float Simulation::getMembranePotential(unsigned g)
 {
 	const HostType* t; unsigned i;
 	locate(g, &t, &i);
-	return getNeuronState(g, t->desc->mpot);
+	return getNeuronState(g, t->desc.mpot);
 }
 
 void Simulation::setNeuron(unsigned g, unsigned nargs, const float* args)
 {
 	const HostType* t; unsigned i;
 	locate(g, &t, &i);
-	unsigned np = t->desc->nparam, ns = t->desc->nstate;
+	unsigned np = t->desc.nparam, ns = t->desc.nstate;
 	if(nargs != np + ns) {
 		NB_THROW(NEMO_INVALID_INPUT,
 				"Unexpected number of parameters/state variables when modifying neuron. Expected %u, found %u", np + ns, nargs);
@@ -2735,7 +2531,7 @@ void Simulation::setNeuronState(unsigned g, unsigned var, float v)
 {
 	const HostType* t; unsigned i;
 	locate(g, &t, &i);
-	if(var >= t->desc->nstate) NB_THROW(NEMO_INVALID_INPUT, "Invalid state variable index %u", var);
+	if(var >= t->desc.nstate) NB_THROW(NEMO_INVALID_INPUT, "Invalid state variable index %u", var);
 	NB_CUDA(cudaSetDevice(m_device));
 	NB_CUDA(cudaMemcpyAsync(t->dState + (size_t) var * t->n + i, &v, 4, cudaMemcpyHostToDevice, m_stream));
 	sync();
@@ -2745,7 +2541,7 @@ void Simulation::setNeuronParameter(unsigned g, unsigned p, float v)
 {
 	const HostType* t; unsigned i;
 	locate(g, &t, &i);
-	if(p >= t->desc->nparam) NB_THROW(NEMO_INVALID_INPUT, "Invalid parameter index %u", p);
+	if(p >= t->desc.nparam) NB_THROW(NEMO_INVALID_INPUT, "Invalid parameter index %u", p);
 	NB_CUDA(cudaSetDevice(m_device));
 	NB_CUDA(cudaMemcpyAsync(t->dParam + (size_t) p * t->n + i, &v, 4, cudaMemcpyHostToDevice, m_stream));
 	sync();
@@ -2826,10 +2622,10 @@ void Simulation::getNetTypeState(unsigned net, unsigned netType, float* out, siz
 	const NetTypeRange& r = m_netTypes[net][netType];
 	if(r.count == 0) return;
 	const HostType& t = m_types[r.hostType];
-	size_t n = (size_t) r.count * t.desc->nstate;
+	size_t n = (size_t) r.count * t.desc.nstate;
 	if(cap < n) NB_THROW(NEMO_BUFFER_OVERFLOW, "state buffer too small");
 	NB_CUDA(cudaSetDevice(m_device));
-	for(unsigned v = 0; v < t.desc->nstate; ++v) {
+	for(unsigned v = 0; v < t.desc.nstate; ++v) {
 		NB_CUDA(cudaMemcpyAsync(out + (size_t) v * r.count, t.dState + (size_t) v * t.n + r.offset,
 				(size_t) r.count * 4, cudaMemcpyDeviceToHost, m_stream));
 	}

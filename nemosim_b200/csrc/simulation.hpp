@@ -82,14 +82,11 @@ struct StdpParams {
 // spreads their entries evenly over all warps of the GPU: group i is
 // {start lo, start hi, length, first entry}, its entries numbered
 // consecutively after those of groups 0..i-1, and bucket[b] is the group
-// that holds entry 32 b.  Everything is indexed by the parity of the
-// publishing step.  A list that is consumed before the next step publishes
-// into it has one group and bucket array (both pointers equal); a list
-// consumed while the next step publishes has two.
+// that holds entry 32 b.
 struct WorkList {
-	uint4* group[2];
-	unsigned long long* count;  // [2] groups << 32 | entries
-	uint32_t* bucket[2];
+	uint4* group;
+	unsigned long long* count;  // [2] by the parity of the publishing step: groups << 32 | entries
+	uint32_t* bucket;
 };
 
 // Everything a kernel needs, passed by value.  Neuron arrays use the
@@ -110,7 +107,7 @@ struct DevSim {
 	uint32_t recentBytes;     // bytes of shared memory for the copy of one recent bit-vector (0 = none)
 	uint32_t* fstim;          // [W] pending firing stimulus
 	float* curExt;            // [N] pending current stimulus
-	ulonglong2* slot;         // [2][N] int64 E and I fixed-point sums (two's complement) of the arrivals, by arrival-step parity
+	ulonglong2* slot;         // [N] int64 E and I fixed-point sums (two's complement) of this step's arrivals
 	const unsigned long long* outPtr; // [N+1] outgoing synapses per source, sorted by delay
 	uint2* syn;               // [S] {target | (delay - 1) << 26, weight}
 	// delay groups: bit d - 1 of delayMask[n] is set when source n has
@@ -132,13 +129,10 @@ struct DevSim {
 	const uint32_t* rcmSrc;   // source | (delay - 1) << 26
 	const uint32_t* rcmFwd;   // index into syn
 	int32_t* rcmAcc;          // STDP accumulator per incoming plastic synapse
-	// work published by a step's update for the next step: the delay groups
-	// arriving next step, delivered before the next update (dlvWork); the
-	// delay groups of delay 2 and more arriving in two steps, delivered
-	// while the next update runs (preWork); the incoming plastic synapses of
-	// its STDP targets, accumulated while the next update runs (stdpWork)
-	WorkList dlvWork, preWork, stdpWork;
-	unsigned long long* claim; // [2][2] by step parity: entries of stdpWork / preWork claimed so far
+	// work published by a step's update for the next pre-phase: the delay
+	// groups arriving next step (ranges of syn) and the incoming plastic
+	// synapses of its STDP targets (ranges of the reverse matrix)
+	WorkList dlvWork, stdpWork;
 	// incoming plastic synapses of the targets touched since the last
 	// applyStdp: {start lo, start hi, length, target}
 	uint4* applyChunks;
@@ -156,10 +150,9 @@ struct DevSim {
 };
 
 // the trace points of a step: its start, the CTA's arrival after the
-// deliveries arriving now, the barrier's release (owners), the end of the
-// update (owners), the end of the claimed work with the arrival at the
-// step's final barrier, and that barrier's release
-constexpr uint32_t TRACE_MARKS = 6;
+// pre-phase, the release of the barrier after it, the end of the CTA's
+// update, and the release of the step's final barrier
+constexpr uint32_t TRACE_MARKS = 5;
 
 class Simulation {
 public:
@@ -217,22 +210,12 @@ public:
 	// persistent loop's co-resident CTAs
 	bool usePersistent = true;
 
-	// the persistent loop publishes the deliveries of delay 2 and more two
-	// steps ahead and makes them while the next update runs (results are
-	// identical either way)
-	bool pipelined = true;
-
-		// launch shape of the active step loop (persistent or two-launch):
+	// launch shape of the active step loop (persistent or two-launch):
 	// partition size (neurons per partition; a CTA owns one or more) and
 	// threads per CTA; results do not depend on them
 	uint32_t partition() const { return persistentActive() ? m_runP : m_P; }
 	uint32_t threads() const { return persistentActive() ? m_runT : m_T; }
 	void setLaunch(uint32_t P, uint32_t T);
-	// CTAs of the persistent loops beyond the partitions' owners: they take
-	// their share of the arrivals, then claim the STDP accumulation and the
-	// deliveries made ahead while the owners update their neurons
-	void setSpareCtas(uint32_t D);
-	uint32_t spareCtas() const { return m_runD; }
 	bool persistentActive() const { return usePersistent && m_runGrid != 0; }
 	// step() keeps the persistent loop resident on the GPU between calls
 	// (serve_kernel) and ends it after this many microseconds without a
@@ -252,13 +235,12 @@ public:
 	// one launch of the persistent loop over `steps` steps (then its STDP
 	// accumulation, as in run()) with the phase trace on: out receives
 	// steps x CTAs x TRACE_MARKS %globaltimer values (ns); returns the CTAs
-	// and, in *owners, how many of them own partitions
-	unsigned tracePhases(unsigned steps, uint64_t* out, size_t cap, unsigned* owners);
+	unsigned tracePhases(unsigned steps, uint64_t* out, size_t cap);
 	uint64_t stepEvents = 0;  // synaptic events of all step() calls so far
 
 private:
 	struct HostType {
-		const NeuronTypeDesc* desc;
+		NeuronTypeDesc desc;  // copied from the network
 		unsigned netType;
 		unsigned base, n;
 		float* dParam = nullptr;
@@ -293,9 +275,7 @@ private:
 	bool m_barrierUsed = false;           // a persistent launch ran since the last checkBarrier
 	unsigned m_runGrid = 0;  // co-resident CTAs of run_kernel at m_runT threads (0: no cooperative launch)
 	uint32_t m_runP = 0;     // neurons per partition of run_kernel
-	uint32_t m_runT = 256;
-	uint32_t m_runD = 0;     // CTAs of the persistent loops beyond the partitions' owners
-	unsigned runGridSize() const;  // CTAs of a launch of the persistent loops
+	uint32_t m_runT = 384;
 	unsigned runGridFor(uint32_t T) const;
 	void buildGraph();
 	static constexpr unsigned GRAPH_STEPS = 100;

@@ -232,37 +232,22 @@ def test_persistent_loop_matches_two_launch_step():
     assert same_bits(a.type_state(0, 2, 3000), b.type_state(0, 2, 3000))
 
 
-@pytest.mark.parametrize("spare", [0, 148, 296])
-def test_pipelined_loop_matches_unpipelined(spare):
-    """The persistent loop that makes the deliveries of delay 2 and more a
-    step ahead, while the next update runs (the default), equals the loop
-    that makes every delivery before its arrival step's update: across
-    applyStdp periods of 1 to 100 steps (no delivery is made ahead across an
-    applyStdp), remainders, interleaved nemo_step calls, and any number of
-    spare CTAs."""
+def test_phase_trace_advances_like_run():
+    """The phase trace runs the persistent loop like run() does: the
+    simulation continues identically afterwards, and every CTA's marks are
+    in order within each step."""
     a = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
     b = nb.Simulation(nb.example_random(3000, 150, 20, True), nets.standard_stdp(nb))
-    b.set_pipelined(False)
-    a.set_spare_ctas(spare)
-    assert a.spare_ctas() == spare
-    for steps, period in [(537, 100), (250, 0), (333, 70), (5, 1), (101, 2), (9, 3), (40, 4)]:
-        ra = a.run(steps, period, 1.0)
-        rb = b.run(steps, period, 1.0)
-        assert np.array_equal(ra[0], rb[0]) and np.array_equal(ra[2], rb[2]), (steps, period)
-        assert a.step([7]) == b.step([7])
+    a.run(100, 100, 1.0)
+    b.run(100, 100, 1.0)
+    tr = a.trace_phases(100)
+    b.run(100, 100, 1.0)
+    assert tr.shape[0] == 100 and tr.shape[2] == 5
+    assert np.all(np.diff(tr.astype(np.int64), axis=2) >= 0)
+    ra = a.run(200, 100, 1.0)
+    rb = b.run(200, 100, 1.0)
+    assert np.array_equal(ra[2], rb[2])
     assert np.array_equal(a.weights_fx(450000), b.weights_fx(450000))
-    assert same_bits(a.type_state(0, 2, 3000), b.type_state(0, 2, 3000))
-
-
-def test_pipelined_loop_matches_oracle_with_frequent_apply():
-    """Pipelined persistent loop against the oracle with long delays and an
-    applyStdp every 7 steps (spikes in flight across every call)."""
-    sims = (nb.Simulation(nb.example_random(1500, 150, 40, True), nets.standard_stdp(nb, n=20)),
-            O.Simulation(O.example_random(1500, 150, 40, True), nets.standard_stdp(O, n=20)))
-    sims[0].set_spare_ctas(296)
-    p, o = run_both(sims, 700, stdp_period=7, reward=0.8)
-    assert_streams_equal(p, o)
-    assert np.array_equal(sims[0].weights_fx(1500 * 150), sims[1].weights_fx(1500 * 150))
 
 
 @pytest.mark.parametrize("persistent", [True, False])
