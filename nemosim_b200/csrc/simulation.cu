@@ -379,6 +379,11 @@ __device__ __forceinline__ void red_add_u64(unsigned long long* p, unsigned long
 	asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
 }
 
+__device__ __forceinline__ void red_add_s32(int32_t* p, int32_t v)
+{
+	asm volatile("red.relaxed.gpu.global.add.s32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+
 // One warp's share of a work list: the entries [E0, E1) of the list's
 // ne entries, in rounds of 32 x K, each lane finding the group of its entry
 // by a binary search over 32 consecutive group descriptors (one per lane).
@@ -438,15 +443,9 @@ __device__ __forceinline__ void process_list(const DevSim& S, const WorkList& L,
 				}
 			} else {
 				uint32_t sd[K];
-				int32_t acc[K];
 				uint64_t h[K];
 #pragma unroll
-				for(int j = 0; j < K; ++j) {
-					if(base + lane + 32 * j < hi) {
-						sd[j] = __ldcs(S.rcmSrc + idx[j]);
-						acc[j] = __ldcs(S.rcmAcc + idx[j]);
-					}
-				}
+				for(int j = 0; j < K; ++j) if(base + lane + 32 * j < hi) sd[j] = __ldcs(S.rcmSrc + idx[j]);
 #pragma unroll
 				for(int j = 0; j < K; ++j) {
 					// a source that fired in none of the last 64 steps has history 0
@@ -459,7 +458,9 @@ __device__ __forceinline__ void process_list(const DevSim& S, const WorkList& L,
 					if(base + lane + 32 * j < hi) {
 						const uint32_t delay = (sd[j] >> 26) + 1;
 						const int32_t dw = stdp_weight_change(S.sp, h[j] >> (delay & 63));
-						if(dw != 0) __stcs(S.rcmAcc + idx[j], (int32_t) ((uint32_t) acc[j] + (uint32_t) dw));
+						// one lane owns each accumulator in a step: an int32
+						// reduction (wrapping) needs no load of the old value
+						if(dw != 0) red_add_s32(S.rcmAcc + idx[j], dw);
 					}
 				}
 			}
@@ -492,14 +493,15 @@ __device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uin
 	}
 	const uint64_t* hist = S.hist + (size_t) pub * S.N;
 	// CTAs [0, gs) take the STDP list, [gs, gridDim.x) the deliveries, in
-	// proportion to their work: an STDP entry costs about STDP_ENTRY_COST
-	// delivery entries (measured per CTA at 100k x 1000: with a weight of 2
-	// the STDP CTAs took 12 us and the delivery CTAs 8 us)
-	constexpr unsigned long long STDP_ENTRY_COST = 3;
+	// proportion to their work: an STDP entry (a load, a dependent history
+	// load for a recently active source, a reduction where its change is
+	// nonzero) costs about 2.5 deliveries (at 100k x 1000 a period took
+	// 2.5% less than with 3 and 2.4% less than with 2)
+	constexpr unsigned long long STDP_ENTRY_COST_X2 = 5;  // twice the cost, for half steps
 	uint32_t gs = ns ? gridDim.x : 0u;
 	if(nd && ns) {
-		gs = (uint32_t) ((unsigned long long) gridDim.x * STDP_ENTRY_COST * ns
-				/ ((unsigned long long) nd + STDP_ENTRY_COST * ns));
+		gs = (uint32_t) ((unsigned long long) gridDim.x * STDP_ENTRY_COST_X2 * ns
+				/ (2ull * nd + STDP_ENTRY_COST_X2 * ns));
 		gs = max(1u, min(gridDim.x - 1u, gs));
 		if(gridDim.x == 1) gs = 0;  // one CTA: it does both, deliveries first
 	}
@@ -702,9 +704,11 @@ __device__ __forceinline__ bool persistent_step(const DevSim& S, uint32_t P, uns
 	return ok;
 }
 
-// TRACE: the instance with the phase trace (tracePhases)
-template<bool TRACE>
-__global__ void __launch_bounds__(RUN_THREADS, 1)
+// TRACE: the instance with the phase trace (tracePhases).  MAXT, MINB: up
+// to 768 threads, one CTA per SM (80 registers), or up to 512 threads, two
+// CTAs per SM (64 registers).
+template<bool TRACE, unsigned MAXT, unsigned MINB>
+__global__ void __launch_bounds__(MAXT, MINB)
 run_kernel(const DevSim S, uint32_t P, uint32_t steps, unsigned long long cycle0, GridBarrier* gb, uint32_t base,
 		int finalStdp, const uint32_t* stim, uint32_t nf, uint32_t ni, uint32_t* hostFired)
 {
@@ -886,7 +890,8 @@ __device__ __forceinline__ uint32_t wait_request(GridBarrier* gb, uint32_t want,
 	return sCmd;
 }
 
-__global__ void __launch_bounds__(RUN_THREADS, 1)
+template<unsigned MAXT, unsigned MINB>
+__global__ void __launch_bounds__(MAXT, MINB)
 serve_kernel(const DevSim S, uint32_t P, unsigned long long cycle0, GridBarrier* gb, ServeCtl* ctl, uint32_t seq0,
 		const uint32_t* stim, uint32_t* hostIds, unsigned long long idleNs)
 {
@@ -955,6 +960,21 @@ serve_kernel(const DevSim S, uint32_t P, unsigned long long cycle0, GridBarrier*
 	}
 }
 
+// The instances of the persistent loops for a block size
+constexpr uint32_t RUN_THREADS_PAIR = 512;
+static const void* run_kernel_for(uint32_t threads, bool trace)
+{
+	if(threads <= RUN_THREADS_PAIR) {
+		return trace ? (const void*) run_kernel<true, RUN_THREADS_PAIR, 2> : (const void*) run_kernel<false, RUN_THREADS_PAIR, 2>;
+	}
+	return trace ? (const void*) run_kernel<true, RUN_THREADS, 1> : (const void*) run_kernel<false, RUN_THREADS, 1>;
+}
+static const void* serve_kernel_for(uint32_t threads)
+{
+	return threads <= RUN_THREADS_PAIR ? (const void*) serve_kernel<RUN_THREADS_PAIR, 2>
+			: (const void*) serve_kernel<RUN_THREADS, 1>;
+}
+
 // Turns the targets touched since the last applyStdp (a bit-vector) into
 // chunks of their incoming plastic synapses, and clears the bit-vector: one
 // thread per neuron, one reservation per warp.
@@ -1001,15 +1021,23 @@ apply_touched_kernel(const DevSim S, int32_t reward)
 		int32_t w[ILP];
 #pragma unroll
 		for(uint32_t j = 0; j < ILP; ++j) acc[j] = lane + 32 * j < len ? __ldcs(S.rcmAcc + start + lane + 32 * j) : 0;
+		// the old weight from the reverse-ordered copy (coalesced); only a
+		// changed weight is written to the forward matrix (scattered)
 #pragma unroll
-		for(uint32_t j = 0; j < ILP; ++j) if(acc[j]) fwd[j] = __ldcs(S.rcmFwd + start + lane + 32 * j);
-#pragma unroll
-		for(uint32_t j = 0; j < ILP; ++j) if(acc[j]) w[j] = (int32_t) S.syn[fwd[j]].y;
+		for(uint32_t j = 0; j < ILP; ++j) {
+			if(acc[j]) {
+				fwd[j] = __ldcs(S.rcmFwd + start + lane + 32 * j);
+				w[j] = __ldcs(S.rcmW + start + lane + 32 * j);
+			}
+		}
 #pragma unroll
 		for(uint32_t j = 0; j < ILP; ++j) {
 			if(!acc[j]) continue;
 			const int32_t nw2 = stdp_updated_weight(S.sp, w[j], fx_mul_dev(reward, acc[j]));
-			if(nw2 != w[j]) S.syn[fwd[j]].y = (uint32_t) nw2;
+			if(nw2 != w[j]) {
+				S.rcmW[start + lane + 32 * j] = nw2;
+				S.syn[fwd[j]].y = (uint32_t) nw2;
+			}
 			S.rcmAcc[start + lane + 32 * j] = 0;
 		}
 	}
@@ -1027,10 +1055,12 @@ apply_full_kernel(const DevSim S, int32_t reward)
 		unsigned long long b = S.rcmPtr[tgt], e = S.rcmPtr[tgt + 1];
 		for(unsigned long long p = b + lane; p < e; p += 32) {
 			const int32_t acc = S.rcmAcc[p];
-			const uint32_t fwd = S.rcmFwd[p];
-			const int32_t w = (int32_t) S.syn[fwd].y;
+			const int32_t w = S.rcmW[p];
 			const int32_t nw = stdp_updated_weight(S.sp, w, fx_mul_dev(reward, acc));
-			if(nw != w) S.syn[fwd].y = (uint32_t) nw;
+			if(nw != w) {
+				S.rcmW[p] = nw;
+				S.syn[S.rcmFwd[p]].y = (uint32_t) nw;
+			}
 			if(acc) S.rcmAcc[p] = 0;
 		}
 	}
@@ -1584,6 +1614,7 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 		}
 		size_t P = rcmPtr[N];
 		hvector<uint32_t> rsrc(P), rfwd(P);
+		hvector<int32_t> rw(P);
 		std::vector<unsigned long long> fill(rcmPtr.begin(), rcmPtr.end() - 1);
 		for(size_t k = 0; k < Sn; ++k) {
 			if(!splastic[k]) continue;
@@ -1591,10 +1622,13 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 			rsrc[p] = lsrc[k] | ((sdelay[k] - 1) << 26);
 			if(pos[k] > 0xffffffffull) NB_THROW(NEMO_API_UNSUPPORTED, "too many synapses for STDP");
 			rfwd[p] = (uint32_t) pos[k];
+			rw[p] = fxw[k];
 		}
 		auto* dRsrc = dalloc<uint32_t>(P);
 		auto* dRfwd = dalloc<uint32_t>(P);
 		S.rcmAcc = dalloc<int32_t>(P);
+		S.rcmW = dalloc<int32_t>(P);
+		NB_CUDA(cudaMemcpyAsync(S.rcmW, rw.data(), P * 4, cudaMemcpyHostToDevice, m_stream));
 		NB_CUDA(cudaMemcpyAsync(dRsrc, rsrc.data(), P * 4, cudaMemcpyHostToDevice, m_stream));
 		NB_CUDA(cudaMemcpyAsync(dRfwd, rfwd.data(), P * 4, cudaMemcpyHostToDevice, m_stream));
 		S.rcmSrc = dRsrc;
@@ -1780,8 +1814,10 @@ unsigned Simulation::runGridFor(uint32_t T) const
 	// run_kernel and serve_kernel (the resident loop of nemo_step) share
 	// the launch shape
 	int perSm = 0, perSmServe = 0;
-	NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, run_kernel<false>, (int) T, m_dev.recentBytes));
-	NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmServe, serve_kernel, (int) T, m_dev.recentBytes));
+	NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, run_kernel_for(T, false), (int) T,
+			m_dev.recentBytes));
+	NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmServe, serve_kernel_for(T), (int) T,
+			m_dev.recentBytes));
 	perSm = std::min(perSm, perSmServe);
 	return perSm > 0 ? (unsigned) perSm * (unsigned) m_sms : 0u;
 }
@@ -1866,8 +1902,8 @@ void Simulation::launchRun(unsigned n, bool finalStdp, const uint32_t* stim, uin
 	int fin = finalStdp ? 1 : 0;
 	void* args[] = { &dev, &P, &steps, &c0, &gb, &base, &fin, &stim, &nf, &ni, &hostFired };
 	timedBegin(K_RUN);
-	const void* kernel = m_dev.trace ? (const void*) run_kernel<true> : (const void*) run_kernel<false>;
-	NB_CUDA(cudaLaunchCooperativeKernel(kernel, dim3(grid), dim3(m_runT), args, m_dev.recentBytes, m_stream));
+	NB_CUDA(cudaLaunchCooperativeKernel(run_kernel_for(m_runT, m_dev.trace != nullptr), dim3(grid), dim3(m_runT), args,
+			m_dev.recentBytes, m_stream));
 	timedEnd();
 	m_barrierBase += arrivals;
 	m_cycle += n;
@@ -1997,7 +2033,7 @@ void Simulation::launchServe()
 	unsigned long long idleNs = (unsigned long long) residentIdleUs * 1000ull;
 	const unsigned grid = (unsigned) std::min<uint64_t>(m_runGrid, std::max<uint64_t>(1, (m_N + P - 1) / P));
 	void* args[] = { &dev, &P, &c0, &gb, &ctl, &seq0, &stim, &hf, &idleNs };
-	NB_CUDA(cudaLaunchCooperativeKernel((const void*) serve_kernel, dim3(grid), dim3(m_runT), args, m_dev.recentBytes,
+	NB_CUDA(cudaLaunchCooperativeKernel(serve_kernel_for(m_runT), dim3(grid), dim3(m_runT), args, m_dev.recentBytes,
 			m_stream));
 	NB_CUDA(cudaEventRecord(m_serveEnd, m_stream));
 	m_serving = true;
@@ -2382,7 +2418,7 @@ float Simulation::autotune(unsigned trialSteps)
 	const bool pers = persistentActive();
 	if(pers) {
 		// persistent loop: 256 to RUN_THREADS threads per CTA, 1 to 4 partitions per CTA
-		for(uint32_t T : {256u, 384u, RUN_THREADS}) {
+		for(uint32_t T : {256u, 384u, RUN_THREADS_PAIR, RUN_THREADS}) {
 			const unsigned g = runGridFor(T);
 			if(!g) continue;
 			for(unsigned k : {1u, 2u, 4u}) {

@@ -129,6 +129,7 @@ struct DevSim {
 	const uint32_t* rcmSrc;   // source | (delay - 1) << 26
 	const uint32_t* rcmFwd;   // index into syn
 	int32_t* rcmAcc;          // STDP accumulator per incoming plastic synapse
+	int32_t* rcmW;            // the plastic synapse's weight (equal to its syn entry's), in reverse order
 	// work published by a step's update for the next pre-phase: the delay
 	// groups arriving next step (ranges of syn) and the incoming plastic
 	// synapses of its STDP targets (ranges of the reverse matrix)
