@@ -72,6 +72,13 @@ def _address(buf) -> int:
     return buf.buffer_info()[0] if isinstance(buf, array.array) else buf.ctypes.data
 
 
+def add_plugin_path(directory: str):
+    """nemo.add_plugin_path: a directory searched for neuron-type
+    descriptors (<type>.ini) before ~/.nemo/plugins and the library's own
+    plugins/ directory (src/nemo/NeuronType.cpp:45-70)."""
+    _check(lib().nemo_add_plugin_path(str(directory).encode()))
+
+
 def version() -> str:
     return lib().nemo_version().decode()
 
