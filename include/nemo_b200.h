@@ -14,9 +14,9 @@
  * reference signatures carry only C types are exported under their reference
  * names.  The two that take reference C++ objects
  * (cuda_simulation(const network::Generator*, const ConfigurationImpl*) and
- * cuda_set_configuration(ConfigurationImpl*, int)) are bound through a
- * small C++ adapter compiled on the reference side, which forwards to
- * Part 1.
+ * cuda_set_configuration(ConfigurationImpl*, int)) are provided by the
+ * C++ adapter nemosim_b200/adapter/b200_backend.cpp, compiled on the
+ * reference side against its headers, which forwards to Part 1.
  *
  * Part 3 is extensions with no counterpart in the reference: bulk
  * construction, device-resident multi-step runs and bulk read-back.
@@ -37,6 +37,11 @@ extern "C" {
 #define NEMO_B200_API
 #endif
 
+/* The status codes, backend ids and basic types of src/nemo/types.h.  A
+ * translation unit that includes the reference's <nemo/types.h> before this
+ * header (the backend adapter does) takes them from there: the values are
+ * the same. */
+#ifndef NEMO_TYPES_H
 /* src/nemo/types.h:31-61 */
 #define NEMO_OK 0
 #define NEMO_CUDA_INVOCATION_ERROR 1
@@ -58,6 +63,7 @@ extern "C" {
 enum { NEMO_BACKEND_CUDA = 0, NEMO_BACKEND_CPU = 1 };
 typedef unsigned backend_t;
 typedef uint64_t synapse_id;
+#endif
 
 /* src/nemo.h:42-52 */
 struct nemo_network_class;
