@@ -304,3 +304,237 @@ def zero_reward_clears(mod):
             s.step(list(range(GROUP)) if ms == 10 else list(range(GROUP, 2 * GROUP)) if ms == 20 else None)
         s.apply_stdp(0.8)
     return weights(cleared), weights(twin)
+
+
+FX = float(1 << 20)
+
+
+def fx_round_trip(w):
+    """fx_toFloat(fx_toFix(w)) (src/nemo/fixedpoint.cpp:17-36): truncation
+    to Q11.20 and back, in float32."""
+    return float(np.float32(int(np.float32(w) * np.float32(FX))) / np.float32(FX))
+
+
+def expected_synapses(src, tgt, dly, w, pl):
+    """The network's synapse ids (source << 32 | index by insertion order per
+    source, src/nemo/NetworkImpl.cpp:105-130) with their target, delay,
+    fixed-point rounded weight and plasticity."""
+    out, count = {}, {}
+    for s, t, d, x, p in zip(src.tolist(), tgt.tolist(), dly.tolist(), w.tolist(), pl.tolist()):
+        i = count.get(s, 0)
+        count[s] = i + 1
+        out.setdefault(s, []).append(((s << 32) | i, t, d, fx_round_trip(x), bool(p)))
+    return out
+
+
+def get_synapses(mod, stdp):
+    """testGetSynapses (src/test/test.cpp:562-603): the simulation holds the
+    network's synapses -- the same ids per source, targets, delays,
+    plasticity and (fixed-point rounded) weights -- on a random network and
+    on a ring whose indices start at 10^6.  Returns the simulation's
+    (id, target, delay, weight, plastic) tuples."""
+    import oracle as O
+    conf = nets.standard_stdp(mod) if stdp else mod.Configuration()
+    ring = np.arange(1000000, 1001500, dtype=np.uint32)
+    cases = [(mod.example_random(300, 50, 20, stdp), expected_synapses(*O.example_random(300, 50, 20, stdp).synapses())),
+             (nets.create_ring(mod, mod.Network(), 1500, 1000000),
+              expected_synapses(ring, np.roll(ring, -1), np.ones(1500, np.uint32), np.full(1500, 1000.0, f32),
+                                np.zeros(1500, np.uint8)))]
+    out = []
+    for net, expect in cases:
+        sim = mod.Simulation(net, conf)
+        sim.step()
+        for src, syn in sorted(expect.items())[::3]:
+            assert list(sim.get_synapses_from(src)) == [x[0] for x in syn], src
+            for i, t, d, w, p in syn:
+                got = (i, sim.get_synapse_target(i), sim.get_synapse_delay(i), sim.get_synapse_weight(i),
+                       bool(sim.get_synapse_plastic(i)))
+                assert got == (i, t, d, w, p), (got, (i, t, d, w, p))
+                out.append(got)
+    return out
+
+
+def write_only_synapses(mod):
+    """testWriteOnlySynapses (src/test/test.cpp:605-624)"""
+    conf = mod.Configuration()
+    conf.set_write_only_synapses()
+    sim = mod.Simulation(nets.create_ring(mod, mod.Network(), 10, 0, True), conf)
+    sim.step()
+    for query in (lambda: sim.get_synapses_from(0), lambda: sim.get_synapse_weight((1 << 32) | 0)):
+        try:
+            query()
+        except mod.NemoError:
+            pass
+        else:
+            raise AssertionError("write-only synapses were read")
+
+
+def synapses_from_unconnected_neuron(mod):
+    """testGetSynapsesFromUnconnectedNeuron (src/test/test.cpp:626-655)"""
+    net = mod.Network()
+    iz = net.add_neuron_type("Izhikevich")
+    for n in range(4):
+        net.add_neuron(iz, n, 0.1, 0.2, 0.3, 0.4, 0.7, 0.5, 0.6)
+    sim = mod.Simulation(net, mod.Configuration())
+    sim.step()
+    try:
+        sim.get_synapses_from(4)
+    except mod.NemoError:
+        pass
+    else:
+        raise AssertionError("synapses of a non-existing neuron")
+    assert list(sim.get_synapses_from(3)) == []
+
+
+def high_firing(mod, steps=1000):
+    """testHighFiring (src/test/test.cpp:697-736): every neuron stimulated
+    to fire every step (1024 neurons x 1000 synapses, delays 1-32): every
+    delivery group of every source is pending at once.  Returns the state."""
+    n = 1024
+    sim = mod.Simulation(mod.example_random(n, 1000, 32, False), mod.Configuration())
+    everyone = list(range(n))
+    for _ in range(steps):
+        assert sim.step(everyone) == everyone
+    return sim.type_state(0, 2, n)
+
+
+def vprobe(mod):
+    """testVProbe (src/test/test.cpp:738-753): the membrane potential of a
+    new simulation is the one it was given."""
+    net = mod.Network()
+    iz = net.add_neuron_type("Izhikevich")
+    v0 = -65.0
+    net.add_neuron(iz, 0, 0.02, 0.2, -65.0 + 15.0 * 0.25, 8.0 - 6.0 * 0.25, 5.0, 0.2 * -65.0, v0)
+    sim = mod.Simulation(net, mod.Configuration())
+    assert sim.get_membrane_potential(0) == v0
+
+
+def stdp_with_all_static(mod):
+    """testStdpWithAllStatic (src/test/test.cpp:666-680): STDP configured
+    but no plastic synapse; applyStdp is accepted and changes nothing."""
+    net = mod.example_random(1000, 1000, 1, False)
+    sim = mod.Simulation(net, nets.standard_stdp(mod))
+    stream = []
+    for _ in range(2):
+        for _ in range(300):
+            stream.append(sim.step())
+        sim.apply_stdp(1.0)
+    return stream
+
+
+def set_neuron_network(mod):
+    """testSetNeuron, the network half (src/test/test.cpp:769-835):
+    setters and getters of a neuron before a simulation exists, and their
+    index and variable errors.  Arguments in the Izhikevich plugin order
+    (a, b, c, d, sigma | u, v)."""
+    a, b, c, d = f32(0.02), f32(0.2), f32(-65.0 + 15.0 * 0.25), f32(8.0 - 6.0 * 0.25)
+    v = f32(-65.0)
+    u, sigma, e = f32(b * v), f32(5.0), f32(0.1)
+    net = mod.Network()
+    iz = net.add_neuron_type("Izhikevich")
+
+    def fails(f):
+        try:
+            f()
+        except mod.NemoError:
+            return True
+        return False
+    assert fails(lambda: net.set_neuron(0, a, b, c, d, sigma, u, v))
+    net.add_neuron(iz, 0, a, b, f32(c - f32(0.1)), d, sigma, u, f32(v - f32(1.0)))
+    assert fails(lambda: net.get_neuron_parameter(1, 0)) and fails(lambda: net.get_neuron_state(1, 0))
+    assert fails(lambda: net.get_neuron_parameter(0, 5)) and fails(lambda: net.get_neuron_state(0, 2))
+    args = [f32(x - e) for x in (a, b, c, d, sigma, u, v)]
+    net.set_neuron(0, *args)
+    assert [net.get_neuron_parameter(0, k) for k in range(5)] + [net.get_neuron_state(0, k) for k in range(2)] \
+        == [float(x) for x in args]
+    for k, x in enumerate((a, b, c, d, sigma)):
+        net.set_neuron_parameter(0, k, x)
+        assert net.get_neuron_parameter(0, k) == float(x)
+    for k, x in enumerate((u, v)):
+        net.set_neuron_state(0, k, x)
+        assert net.get_neuron_state(0, k) == float(x)
+    assert fails(lambda: net.set_neuron_parameter(1, 0, 0.0)) and fails(lambda: net.set_neuron_state(1, 0, 0.0))
+    assert fails(lambda: net.set_neuron_parameter(0, 5, 0.0)) and fails(lambda: net.set_neuron_state(0, 2, 0.0))
+    return net, (a, b, c, d, sigma, u, v, e)
+
+
+def set_neuron_simulation(mod):
+    """testSetNeuron, the simulation half (src/test/test.cpp:837-963):
+    setters during a run take effect without being overwritten, parameters
+    stay and state evolves, errors for invalid indices, a changed c that the
+    neuron does not use leaves the run unchanged, setting the state does
+    not copy it twice, and a potential set before the first step is the one
+    simulated.  Returns the membrane potentials it observed."""
+    a, b, c, d = f32(0.02), f32(0.2), f32(-65.0 + 15.0 * 0.25), f32(8.0 - 6.0 * 0.25)
+    v = f32(-65.0)
+    u, sigma, e = f32(b * v), f32(5.0), f32(0.1)
+    # the network the network half leaves (set_neuron_network)
+    net = mod.Network()
+    net.add_neuron(net.add_neuron_type("Izhikevich"), 0, a, b, c, d, sigma, u, v)
+    conf = mod.Configuration()
+
+    def fails(f):
+        try:
+            f()
+        except mod.NemoError:
+            return True
+        return False
+    seen = []
+    sim = mod.Simulation(net, conf)
+    sim.step()
+    sim.set_neuron_state(0, 0, f32(u - e))
+    assert sim.get_neuron_state(0, 0) == float(f32(u - e))
+    sim.set_neuron_state(0, 1, f32(v - e))
+    assert sim.get_neuron_state(0, 1) == float(f32(v - e))
+    u0, v0 = sim.get_neuron_state(0, 0), sim.get_neuron_state(0, 1)
+    for k, x in enumerate((a, b, c, d, sigma)):
+        sim.set_neuron_parameter(0, k, f32(x - e))
+        assert sim.get_neuron_parameter(0, k) == float(f32(x - e))
+    sim.step()
+    for k, x in enumerate((a, b, c, d, sigma)):
+        assert sim.get_neuron_parameter(0, k) == float(f32(x - e))
+    assert sim.get_neuron_state(0, 0) != u0 and sim.get_neuron_state(0, 1) != v0
+    seen += [sim.get_neuron_state(0, 0), sim.get_neuron_state(0, 1)]
+    for f in (lambda: sim.set_neuron_parameter(1, 0, 0.0), lambda: sim.set_neuron_state(1, 0, 0.0),
+              lambda: sim.get_neuron_parameter(1, 0), lambda: sim.get_neuron_state(1, 0),
+              lambda: sim.set_neuron_parameter(0, 5, 0.0), lambda: sim.set_neuron_state(0, 2, 0.0),
+              lambda: sim.get_neuron_parameter(0, 5), lambda: sim.get_neuron_state(0, 2)):
+        assert fails(f)
+    del sim
+
+    sim = mod.Simulation(net, conf)
+    sim.step()
+    v0 = sim.get_membrane_potential(0)
+    del sim
+    sim = mod.Simulation(net, conf)
+    assert sim.get_neuron_state(0, 0) == float(u) and sim.get_neuron_state(0, 1) == float(v)
+    sim.set_neuron(0, a, b, f32(c + f32(1.0)), d, sigma, u, v)
+    sim.step()
+    assert v0 == sim.get_membrane_potential(0)
+    assert [sim.get_neuron_parameter(0, k) for k in range(5)] == [float(x) for x in (a, b, f32(c + f32(1.0)), d, sigma)]
+    seen.append(v0)
+    del sim
+
+    net0 = mod.Network()
+    iz = net0.add_neuron_type("Izhikevich")
+    net0.add_neuron(iz, 0, a, b, c, d, 0.0, u, v)
+    sim0 = mod.Simulation(net0, conf)
+    sim0.step()
+    sim0.step()
+    sim1 = mod.Simulation(net0, conf)
+    sim1.step()
+    sim1.set_neuron(0, a, b, c, d, 0.0, u, v)
+    sim1.step()
+    sim1.step()
+    assert sim0.get_membrane_potential(0) == sim1.get_membrane_potential(0)
+    seen.append(sim1.get_membrane_potential(0))
+
+    net1 = mod.Network()
+    iz = net1.add_neuron_type("Izhikevich")
+    net1.add_neuron(iz, 0, a, b, c, d, sigma, u, f32(v - f32(1.0)))
+    sim = mod.Simulation(net1, conf)
+    sim.set_neuron(0, a, b, c, d, sigma, u, v)
+    assert sim.get_membrane_potential(0) == float(v)
+    sim.step()
+    assert sim.get_membrane_potential(0) == v0
+    return seen

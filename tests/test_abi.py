@@ -158,3 +158,10 @@ def test_example_generator_matches_oracle():
             assert np.float32(a.get_neuron_parameter(n, p)) == np.float32(ob.get_neuron_parameter(n, p))
         for v in range(2):
             assert np.float32(a.get_neuron_state(n, v)) == np.float32(ob.get_neuron_state(n, v))
+
+
+def test_set_neuron_on_the_network():
+    """testSetNeuron's network half (src/test/test.cpp:769-835) on the
+    product's host-side network"""
+    from tests import kat
+    kat.set_neuron_network(nb)

@@ -72,6 +72,35 @@ def test_zero_reward_clears_accumulators():
     kat.zero_reward_clears(O)
 
 
+@pytest.mark.parametrize("stdp", [False, True])
+def test_get_synapses(stdp):
+    kat.get_synapses(O, stdp)
+
+
+def test_write_only_synapses():
+    kat.write_only_synapses(O)
+
+
+def test_synapses_from_unconnected_neuron():
+    kat.synapses_from_unconnected_neuron(O)
+
+
+def test_high_firing():
+    kat.high_firing(O, steps=100)
+
+
+def test_vprobe():
+    kat.vprobe(O)
+
+
+def test_stdp_with_all_static():
+    kat.stdp_with_all_static(O)
+
+
+def test_set_neuron():
+    kat.set_neuron_simulation(O)
+
+
 def test_ring_delay_80_rejected():
     """The CPU backend rejects delays above 64 (src/nemo/cpu/Simulation.cpp:52-56)."""
     with pytest.raises(O.NemoError):

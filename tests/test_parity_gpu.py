@@ -109,6 +109,57 @@ def test_zero_reward_clears_accumulators():
     assert kat.zero_reward_clears(nb) == kat.zero_reward_clears(O)
 
 
+@pytest.mark.parametrize("stdp", [False, True])
+def test_get_synapses(stdp):
+    """testGetSynapses (src/test/test.cpp:562-603): the simulation's synapse
+    ids, targets, delays, weights and plasticity, equal to the network's and
+    to the oracle's"""
+    assert kat.get_synapses(nb, stdp) == kat.get_synapses(O, stdp)
+
+
+def test_get_synapses_after_stdp():
+    """Weights read back one by one after applyStdp equal the oracle's and
+    the bulk read-back"""
+    sims = [m.Simulation(m.example_random(1000, 100, 20, True), nets.standard_stdp(m)) for m in (nb, O)]
+    for s in sims:
+        s.run(300, 100, 1.0)
+    for src in range(0, 1000, 37):
+        ids = sims[0].get_synapses_from(src)
+        assert list(ids) == list(sims[1].get_synapses_from(src))
+        assert [sims[0].get_synapse_weight(i) for i in ids] == [sims[1].get_synapse_weight(i) for i in ids]
+    assert np.array_equal(sims[0].weights_fx(100000), sims[1].weights_fx(100000))
+
+
+def test_write_only_synapses():
+    kat.write_only_synapses(nb)
+
+
+def test_synapses_from_unconnected_neuron():
+    kat.synapses_from_unconnected_neuron(nb)
+
+
+def test_high_firing():
+    """testHighFiring (src/test/test.cpp:697-736): every neuron fires every
+    step, all delivery groups pending; state bit-exact with the oracle"""
+    assert same_bits(kat.high_firing(nb), kat.high_firing(O))
+
+
+def test_vprobe():
+    kat.vprobe(nb)
+
+
+def test_stdp_with_all_static():
+    """testStdpWithAllStatic (src/test/test.cpp:666-680), fire stream equal
+    to the oracle's"""
+    assert kat.stdp_with_all_static(nb) == kat.stdp_with_all_static(O)
+
+
+def test_set_neuron():
+    """testSetNeuron (src/test/test.cpp:769-963) during simulation; every
+    membrane potential it observes equal to the oracle's"""
+    assert kat.set_neuron_simulation(nb) == kat.set_neuron_simulation(O)
+
+
 # ---------------------------------------------------------------------------
 # bit-exact parity with the oracle on noisy networks
 
