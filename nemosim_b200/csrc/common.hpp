@@ -34,7 +34,8 @@ enum NeuronKind {
 	KIND_IF_CURR_EXP = 1,
 	KIND_POISSON = 2,
 	KIND_INPUT = 3,
-	KIND_COUNT = 4
+	KIND_IZHIKEVICH_RS = 4,
+	KIND_COUNT = 5
 };
 
 struct NeuronTypeDesc {

@@ -116,6 +116,10 @@ __device__ __forceinline__ void load_neuron(const DevSim& S, const TypeRange& T,
 			R.p[0] = P[nl];  // rate
 			load_rng(S, n, R);
 			break;
+		case KIND_IZHIKEVICH_RS:
+			R.x[0] = X[nl];       // u
+			R.x[1] = X[nn + nl];  // v
+			break;
 		default:
 			break;
 	}
@@ -193,6 +197,37 @@ __device__ __forceinline__ bool update_if_curr_exp(NeuronRegs& R, float cE, floa
 	return fired;
 }
 
+// IzhikevichRS, the reference's CUDA plugin (it has no CPU plugin),
+// src/nemo/cuda/plugins/IzhikevichRS.cu:76-116: the Izhikevich update in
+// float with a = 0.02, b = 0.2, c = -65, d = 8 built in and no input noise,
+// in source order without contraction.
+__device__ __forceinline__ bool update_izhikevich_rs(NeuronRegs& R, float cE, float cI, float ext, bool fs)
+{
+	const float a = 0.02f, b = 0.2f;
+	const float I = __fadd_rn(__fadd_rn(cE, cI), ext);
+	float u = R.x[0], v = R.x[1];
+	bool fired = false;
+#pragma unroll
+	for(int k = 0; k < 4; ++k) {
+		if(!fired) {
+			float t = __fadd_rn(__fmul_rn(0.04f, v), 5.0f);
+			t = __fadd_rn(__fmul_rn(t, v), 140.0f);
+			t = __fadd_rn(__fsub_rn(t, u), I);
+			v = __fadd_rn(v, __fmul_rn(0.25f, t));
+			u = __fadd_rn(u, __fmul_rn(0.25f, __fmul_rn(a, __fsub_rn(__fmul_rn(b, v), u))));
+			fired = v >= 30.0f;
+		}
+	}
+	fired = fired || fs;
+	if(fired) {
+		v = -65.0f;
+		u = __fadd_rn(u, 8.0f);
+	}
+	R.x[0] = u;
+	R.x[1] = v;
+	return fired;
+}
+
 // PoissonSource, src/nemo/cpu/plugins/PoissonSource.cpp:6-30
 __device__ __forceinline__ bool update_poisson(NeuronRegs& R, bool fs)
 {
@@ -209,6 +244,7 @@ __device__ __forceinline__ bool update_neuron(const DevSim& S, const TypeRange& 
 		case KIND_IZHIKEVICH: return update_izhikevich(S.calib, R, cE, cI, ext, fs);
 		case KIND_IF_CURR_EXP: return update_if_curr_exp(R, cE, cI, ext, fs);
 		case KIND_POISSON: return update_poisson(R, fs);
+		case KIND_IZHIKEVICH_RS: return update_izhikevich_rs(R, cE, cI, ext, fs);
 		default: return fs;  // Input, src/nemo/cpu/plugins/Input.cpp:17-22
 	}
 }
@@ -231,6 +267,10 @@ __device__ __forceinline__ void store_neuron(const DevSim& S, const TypeRange& T
 			break;
 		case KIND_POISSON:
 			store_rng(S, n, R);
+			break;
+		case KIND_IZHIKEVICH_RS:
+			X[nl] = R.x[0];
+			X[nn + nl] = R.x[1];
 			break;
 		default:
 			break;

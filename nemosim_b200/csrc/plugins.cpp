@@ -32,6 +32,7 @@ const KernelLayout KERNELS[KIND_COUNT] = {
 	{ "IF_curr_exp", 9, 4, false },
 	{ "PoissonSource", 1, 0, true },
 	{ "Input", 0, 0, false },
+	{ "IzhikevichRS", 0, 2, false },
 };
 
 namespace {

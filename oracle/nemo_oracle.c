@@ -221,7 +221,7 @@ static int hmap_insert(hmap* m, uint32_t k, uint64_t v, uint64_t** slot)
 /* Neuron types: .ini descriptors src/nemo/plugins/<Type>.ini and index   */
 /* headers src/nemo/plugins/Izhikevich.h, IF_curr_exp.h                   */
 
-enum { KIND_IZHIKEVICH, KIND_IF_CURR_EXP, KIND_POISSON, KIND_INPUT };
+enum { KIND_IZHIKEVICH, KIND_IF_CURR_EXP, KIND_POISSON, KIND_INPUT, KIND_IZHIKEVICH_RS };
 
 typedef struct { const char* name; int kind; unsigned nparam, nstate, mpot; } type_desc;
 
@@ -230,6 +230,7 @@ static const type_desc TYPES[] = {
 	{ "IF_curr_exp", KIND_IF_CURR_EXP, 9, 4, 0 },  /* IF_curr_exp.ini:14-24 */
 	{ "PoissonSource", KIND_POISSON, 1, 0, 0 },    /* PoissonSource.ini:1-3 */
 	{ "Input", KIND_INPUT, 0, 0, 0 },              /* Input.ini:1-3 */
+	{ "IzhikevichRS", KIND_IZHIKEVICH_RS, 0, 2, 1 },  /* IzhikevichRS.ini:3-5 */
 };
 #define NTYPES_KNOWN (sizeof TYPES / sizeof TYPES[0])
 
@@ -929,6 +930,46 @@ static inline int32_t weight_change(const nemo_oracle_simulation* s, uint64_t pr
 	return wrap_add32(update_region(s, pre & s->potBits), update_region(s, pre & s->depBits));
 }
 
+/* IzhikevichRS has no CPU plugin in the reference (IzhikevichRS.ini:
+ * backends cpu=false): this restates its CUDA plugin,
+ * cuda/plugins/IzhikevichRS.cu:76-116 -- the Izhikevich update in float with
+ * a = 0.02, b = 0.2, c = -65, d = 8 built in and no input noise, in source
+ * order with no contraction (the reference's own build may contract).  State
+ * u, v. */
+static void update_izhikevich_rs(nemo_oracle_simulation* s, sim_type* t)
+{
+	const unsigned n = t->n, start = t->base;
+	float* U = t->state + 0 * n;
+	float* V = t->state + 1 * n;
+	const float a = 0.02f, b = 0.2f;
+	int nn = (int) n;
+#pragma omp parallel for default(shared)
+	for(int nl = 0; nl < nn; nl++) {
+		unsigned ng = start + nl;
+		float I = s->curE[ng] + s->curI[ng] + s->curExt[ng];
+		s->curExt[ng] = 0.0f;
+		float u = U[nl];
+		float v = V[nl];
+		int fired = 0;
+		for(unsigned k = 0; k < 4; ++k) {
+			if(!fired) {
+				v += 0.25f * ((0.04f * v + 5.0f) * v + 140.0f - u + I);
+				u += 0.25f * (a * (b * v - u));
+				fired = v >= 30.0f;
+			}
+		}
+		s->fired[ng] = fired || s->fstim[ng];
+		s->fstim[ng] = 0;
+		s->recent[ng] = (s->recent[ng] << 1) | (uint64_t) s->fired[ng];
+		if(s->fired[ng]) {
+			v = -65.0f;
+			u += 8.0f;
+		}
+		U[nl] = u;
+		V[nl] = v;
+	}
+}
+
 /* ConnectivityMatrix::accumulateStdp, ConnectivityMatrix.cpp:193-227 */
 static void accumulate_stdp(nemo_oracle_simulation* s)
 {
@@ -953,6 +994,7 @@ static void fire(nemo_oracle_simulation* s)
 			case KIND_IF_CURR_EXP: update_if_curr_exp(s, st); break;
 			case KIND_POISSON: update_poisson(s, st); break;
 			case KIND_INPUT: update_input(s, st); break;
+			case KIND_IZHIKEVICH_RS: update_izhikevich_rs(s, st); break;
 		}
 	}
 	accumulate_stdp(s);

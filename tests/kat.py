@@ -538,3 +538,44 @@ def set_neuron_simulation(mod):
     sim.step()
     assert sim.get_membrane_potential(0) == v0
     return seen
+
+
+def izhikevich_rs_no_parameters(mod):
+    """testNoParamNeuronType (src/test/test.cpp:980-1000): IzhikevichRS
+    neurons take only their state (u, v); 100 steps keep it finite.
+    Returns (u, v) of every neuron."""
+    net = mod.Network()
+    rs = net.add_neuron_type("IzhikevichRS")
+    net.add_neuron(rs, np.arange(1000, dtype=np.uint32), -13.0, -65.0)
+    sim = mod.Simulation(net, mod.Configuration())
+    for _ in range(100):
+        sim.step()
+        u, v = sim.get_neuron_state(100, 0), sim.get_neuron_state(100, 1)
+        assert np.isfinite(u) and np.isfinite(v)
+    return sim.type_state(rs, 2, 1000)
+
+
+def izhikevich_rs_network(mod, steps=500, seed=11, resident=True):
+    """A connected IzhikevichRS network (1000 neurons, 50 random synapses
+    each, mixed signs, delays 1-10) driven by a firing stimulus every 5
+    steps and a current stimulus every 7.  Returns the fire stream and the
+    final state."""
+    rng = np.random.default_rng(seed)
+    n = 1000
+    net = mod.Network()
+    rs = net.add_neuron_type("IzhikevichRS")
+    net.add_neuron(rs, np.arange(n, dtype=np.uint32), -13.0, -65.0)
+    src = np.repeat(np.arange(n, dtype=np.uint32), 50)
+    tgt = rng.integers(0, n, len(src)).astype(np.uint32)
+    w = np.where(rng.random(len(src)) < 0.8, 6.0 * rng.random(len(src)), -8.0 * rng.random(len(src))).astype(f32)
+    dly = rng.integers(1, 11, len(src)).astype(np.uint32)
+    net.add_synapse(src, tgt, dly, w, np.zeros(len(src), np.uint8))
+    sim = mod.Simulation(net, mod.Configuration())
+    if not resident:
+        sim.set_resident_step(0)
+    stream = []
+    for t in range(steps):
+        fstim = rng.choice(n, 20, replace=False).tolist() if t % 5 == 0 else None
+        istim = [(int(i), 12.0) for i in rng.choice(n, 30, replace=False)] if t % 7 == 0 else None
+        stream.append(sim.step(fstim, istim))
+    return stream, sim.type_state(rs, 2, n)

@@ -101,6 +101,12 @@ def test_set_neuron():
     kat.set_neuron_simulation(O)
 
 
+def test_izhikevich_rs():
+    kat.izhikevich_rs_no_parameters(O)
+    stream, _ = kat.izhikevich_rs_network(O, steps=200)
+    assert sum(len(f) for f in stream) > 500
+
+
 def test_ring_delay_80_rejected():
     """The CPU backend rejects delays above 64 (src/nemo/cpu/Simulation.cpp:52-56)."""
     with pytest.raises(O.NemoError):

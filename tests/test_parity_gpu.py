@@ -160,6 +160,24 @@ def test_set_neuron():
     assert kat.set_neuron_simulation(nb) == kat.set_neuron_simulation(O)
 
 
+def test_izhikevich_rs_no_parameters():
+    """testNoParamNeuronType (src/test/test.cpp:980-1000), state bit-exact
+    with the oracle's restatement of the reference's IzhikevichRS plugin"""
+    assert same_bits(kat.izhikevich_rs_no_parameters(nb), kat.izhikevich_rs_no_parameters(O))
+
+
+@pytest.mark.parametrize("resident", [True, False])
+def test_izhikevich_rs_network(resident):
+    """A connected, stimulated IzhikevichRS network, stepped through the
+    resident loop or two launches per step: fire stream and state bit-exact
+    with the oracle"""
+    p = kat.izhikevich_rs_network(nb, resident=resident)
+    o = kat.izhikevich_rs_network(O)
+    assert sum(len(f) for f in p[0]) > 2000
+    assert p[0] == o[0]
+    assert same_bits(p[1], o[1])
+
+
 # ---------------------------------------------------------------------------
 # bit-exact parity with the oracle on noisy networks
 
