@@ -35,7 +35,8 @@ enum NeuronKind {
 	KIND_POISSON = 2,
 	KIND_INPUT = 3,
 	KIND_IZHIKEVICH_RS = 4,
-	KIND_COUNT = 5
+	KIND_KURAMOTO = 5,
+	KIND_COUNT = 6
 };
 
 struct NeuronTypeDesc {
@@ -58,6 +59,7 @@ struct KernelLayout {
 	const char* name;
 	unsigned nparam, nstate;
 	bool nrand;
+	unsigned history;  // state history the kernel keeps
 };
 extern const KernelLayout KERNELS[KIND_COUNT];
 // Q(31-f).f with f = 20 (src/nemo/ConfigurationImpl.cpp:22)

@@ -236,6 +236,49 @@ __device__ __forceinline__ bool update_poisson(NeuronRegs& R, bool fs)
 	return p1 < p0 || fs;
 }
 
+// Kuramoto oscillators, src/nemo/cpu/plugins/Kuramoto.cpp:78-124
+// (src/nemo/plugins/Kuramoto.h): parameter the frequency, state the phase,
+// kept for the last 32 cycles (T.state is [32][n]).  One fourth-order
+// Runge-Kutta step of the phase; each stage sums, over the target's
+// incoming synapses, weight x sin(source phase at emission - target phase),
+// the source phase being the one at cycle - (delay - 1).  The neuron never
+// fires and ignores stimulus and synaptic current.  sinf is CUDA's, which
+// is within an ulp or two of the host libm's but not equal to it, so the
+// phases agree with the CPU plugin to a tolerance, not bit for bit.
+// b, e: the neuron's range of the all-synapse reverse matrix (sources as
+// source | (delay - 1) << 26, weights); base, nn: the type's first local
+// index and size; cycle: this step's.
+__device__ __forceinline__ bool update_kuramoto(const float* param, float* state, uint32_t base, uint32_t nn,
+		uint32_t nl, const uint32_t* allSrc, const float* allW, unsigned long long b, unsigned long long e,
+		uint32_t cycle)
+{
+	constexpr uint32_t H = 32;
+	const float f = param[nl];
+	const float phase0 = state[(size_t) (cycle % H) * nn + nl];
+	auto coupling = [&](float targetPhase) {
+		float sum = 0.0f;
+		for(unsigned long long p = b; p < e; ++p) {
+			const uint32_t sd = allSrc[p];
+			const uint32_t delay = (sd >> 26) + 1;
+			const uint32_t src = (sd & (MAX_NEURONS - 1)) - base;
+			const float sp = state[(size_t) ((cycle - (delay - 1)) % H) * nn + src];
+			sum = __fadd_rn(sum, __fmul_rn(allW[p], sinf(__fsub_rn(sp, targetPhase))));
+		}
+		return sum;
+	};
+	const float k0 = __fadd_rn(f, coupling(phase0));
+	const float k1 = __fadd_rn(f, coupling(__fadd_rn(phase0, __fmul_rn(k0, 0.5f))));
+	const float k2 = __fadd_rn(f, coupling(__fadd_rn(phase0, __fmul_rn(k1, 0.5f))));
+	const float k3 = __fadd_rn(f, coupling(__fadd_rn(phase0, k2)));
+	const float sum = __fadd_rn(__fadd_rn(__fadd_rn(k0, __fmul_rn(2.0f, k1)), __fmul_rn(2.0f, k2)), k3);
+	const float phase = __fadd_rn(phase0, __fdiv_rn(sum, 6.0f));
+	// fmodf by 2 pi rounded to float, plus 2 pi in double for a negative
+	// phase, rounded once to float (the plugin's C expression)
+	const double wrapped = (double) fmodf(phase, 6.2831855f) + (phase < 0.0f ? 6.283185307179586 : 0.0);
+	state[(size_t) ((cycle + 1) % H) * nn + nl] = __double2float_rn(wrapped);
+	return false;
+}
+
 // One step of neuron nl (local index n) of type T; returns whether it fired.
 __device__ __forceinline__ bool update_neuron(const DevSim& S, const TypeRange& T, NeuronRegs& R, float cE, float cI,
 		float ext, bool fs)

@@ -28,11 +28,12 @@ namespace nemo_b200 {
 
 // the kernels of kernels.cuh, by kind
 const KernelLayout KERNELS[KIND_COUNT] = {
-	{ "Izhikevich", 5, 2, true },
-	{ "IF_curr_exp", 9, 4, false },
-	{ "PoissonSource", 1, 0, true },
-	{ "Input", 0, 0, false },
-	{ "IzhikevichRS", 0, 2, false },
+	{ "Izhikevich", 5, 2, true, 1 },
+	{ "IF_curr_exp", 9, 4, false, 1 },
+	{ "PoissonSource", 1, 0, true, 1 },
+	{ "Input", 0, 0, false, 1 },
+	{ "IzhikevichRS", 0, 2, false, 1 },
+	{ "Kuramoto", 1, 1, false, 32 },
 };
 
 namespace {
@@ -220,12 +221,12 @@ void checkKernelBinding(const NeuronTypeDesc& d)
 				d.name.c_str(), d.name.c_str());
 	}
 	const KernelLayout& k = KERNELS[d.kind];
-	if(d.nparam != k.nparam || d.nstate != k.nstate || d.nrand != k.nrand) {
+	if(d.nparam != k.nparam || d.nstate != k.nstate || d.nrand != k.nrand || d.history != k.history) {
 		NB_THROW(NEMO_DL_ERROR,
-				"Error when loading plugin %s: the descriptor in %s gives %u parameters, %u state variables and "
-				"normal RNG %s; the B200 kernel for %s expects %u, %u and %s",
-				d.name.c_str(), d.pluginDir.c_str(), d.nparam, d.nstate, d.nrand ? "on" : "off", k.name, k.nparam,
-				k.nstate, k.nrand ? "on" : "off");
+				"Error when loading plugin %s: the descriptor in %s gives %u parameters, %u state variables, "
+				"normal RNG %s and history %u; the B200 kernel for %s expects %u, %u, %s and %u",
+				d.name.c_str(), d.pluginDir.c_str(), d.nparam, d.nstate, d.nrand ? "on" : "off", d.history, k.name,
+				k.nparam, k.nstate, k.nrand ? "on" : "off", k.history);
 	}
 	if(d.mpot >= d.nstate && d.nstate > 0) {
 		NB_THROW(NEMO_DL_ERROR, "Error when loading plugin %s: membrane-potential index %u is not a state variable",

@@ -99,11 +99,13 @@ __device__ __forceinline__ void trace_mark(const DevSim& S, uint32_t row, uint32
 
 // Inside a CUDA graph the step's cycle comes from a device counter (the
 // graph is replayed at different cycles): cycle = *cycleDev + offset.
-__device__ __forceinline__ void step_indices(const DevSim& S, uint32_t offset, uint32_t& cur, uint32_t& ring)
+__device__ __forceinline__ void step_indices(const DevSim& S, uint32_t offset, uint32_t& cur, uint32_t& ring,
+		uint32_t& cycleLo)
 {
 	const unsigned long long c = *S.cycleDev + offset;
 	cur = (uint32_t) (c & 1);
 	ring = (uint32_t) (c % S.R);
+	cycleLo = (uint32_t) c;
 }
 
 __global__ void advance_cycle_kernel(unsigned long long* cycle, uint32_t by)
@@ -184,8 +186,9 @@ struct CtaCounters {
 // blockDim.x threads loop over them.  Every thread of the CTA calls it.
 // cur = t & 1.
 // hostFired: also write the fired bit-vector words there (host memory)
+// cycleLo: the low 32 bits of t (the state slot of a type with history)
 __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, uint32_t last, uint32_t cur,
-		uint32_t ring, CtaCounters& C, bool preNoise = false, uint32_t* hostFired = nullptr)
+		uint32_t ring, uint32_t cycleLo, CtaCounters& C, bool preNoise = false, uint32_t* hostFired = nullptr)
 {
 	const uint32_t tid = threadIdx.x, lane = tid & 31;
 	const uint64_t* histPrev = S.hist + (size_t) (cur ^ 1u) * S.N;
@@ -237,8 +240,12 @@ __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, ui
 			const float cE = wfx_to_float((long long) acc.x);
 			const float cI = wfx_to_float((long long) acc.y);
 			const bool fs = (fw >> lane) & 1u;
-			fired = update_neuron(S, T, R, cE, cI, ext, fs);
-			store_neuron(S, T, nl, n, R);
+			// a Kuramoto oscillator never fires; its phase is updated by the
+			// pass after this loop
+			if(T.kind != KIND_KURAMOTO) {
+				fired = update_neuron(S, T, R, cE, cI, ext, fs);
+				store_neuron(S, T, nl, n, R);
+			}
 			const uint64_t h = (hp << 1) | (uint64_t) fired;
 			histCur[n] = h;
 			hist_nonzero = h != 0;
@@ -328,6 +335,19 @@ __device__ __forceinline__ void update_range(const DevSim& S, uint32_t first, ui
 			if(lane == 0) atomicAdd(&C.stdp, se);
 		}
 	}
+	// the phases of the Kuramoto oscillators among [first, last), apart from
+	// the loop above so that no register of it stays live across the sums
+	if(S.allSrc) {
+		for(uint32_t n = first + tid; n < last; n += blockDim.x) {
+			uint32_t k = 0;
+			while(k + 1 < S.ntypes && n >= S.types[k + 1].base) ++k;
+			const TypeRange& T = S.types[k];
+			if(T.kind == KIND_KURAMOTO) {
+				update_kuramoto(T.param, T.state, T.base, T.n, n - T.base, S.allSrc, S.allW, S.allPtr[n], S.allPtr[n + 1],
+						cycleLo);
+			}
+		}
+	}
 }
 
 // Adds the CTA's counters to those of ring position `ring` and clears them
@@ -352,22 +372,22 @@ __device__ __forceinline__ void flush_counters(const DevSim& S, uint32_t ring, C
 // more of each neuron's chain of loads.
 template<unsigned MAXT, unsigned MINB>
 __global__ void __launch_bounds__(MAXT, MINB)
-update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t ring, uint32_t offset, int fromDev,
-		uint32_t* hostFired = nullptr)
+update_kernel(const DevSim S, uint32_t P, uint32_t cur, uint32_t ring, uint32_t cycleLo, uint32_t offset,
+		int fromDev, uint32_t* hostFired = nullptr)
 {
 	chain_wait_then_release();
-	if(fromDev) step_indices(S, offset, cur, ring);
+	if(fromDev) step_indices(S, offset, cur, ring, cycleLo);
 	__shared__ CtaCounters sC;
 	if(threadIdx.x == 0) sC = CtaCounters{ 0, 0, 0, 0, 0, 0, 0 };
 	__syncthreads();
 	const uint32_t first = blockIdx.x * P;
-	update_range(S, first, min(S.N, first + P), cur, ring, sC, false, hostFired);
+	update_range(S, first, min(S.N, first + P), cur, ring, cycleLo, sC, false, hostFired);
 	__syncthreads();
 	flush_counters(S, ring, sC);
 }
 
 // the update_kernel instance for the two-launch step's threads per CTA
-using UpdateKernel = void (*)(const DevSim, uint32_t, uint32_t, uint32_t, uint32_t, int, uint32_t*);
+using UpdateKernel = void (*)(const DevSim, uint32_t, uint32_t, uint32_t, uint32_t, uint32_t, int, uint32_t*);
 static UpdateKernel update_kernel_for(uint32_t threads)
 {
 	return threads <= 256 ? update_kernel<256, 5> : update_kernel<1024, 1>;
@@ -560,7 +580,8 @@ deliver_kernel(const DevSim S, uint32_t pub, uint32_t what, uint32_t offset, int
 	chain_wait_then_release();
 	if(fromDev) {
 		uint32_t cur, ring;
-		step_indices(S, offset, cur, ring);
+		uint32_t cycleLo;
+		step_indices(S, offset, cur, ring, cycleLo);
 		pub = cur ^ 1u;
 	}
 	if(stim) apply_stimulus(S, stim, nf, ni);
@@ -694,7 +715,7 @@ __device__ __forceinline__ bool persistent_step(const DevSim& S, uint32_t P, uns
 	if(!grid_wait(gb, sTarget, sOk, S.waitLimit)) return false;
 	trace_mark(S, row, 2);
 	for(uint32_t p = blockIdx.x; p < nparts; p += gridDim.x) {
-		update_range(S, p * P, min(S.N, p * P + P), cur, ring, sC, true, hostFired);
+		update_range(S, p * P, min(S.N, p * P + P), cur, ring, (uint32_t) c, sC, true, hostFired);
 	}
 	__syncthreads();
 	flush_counters(S, ring, sC);
@@ -1303,6 +1324,24 @@ static void seed_rng(std::vector<uint32_t>& planes, unsigned N)
 
 static inline uint64_t shl64(uint64_t x, unsigned s) { return x << (s & 63); }
 
+// cpu_init_neurons of the Kuramoto plugin (src/nemo/cpu/plugins/
+// Kuramoto.cpp:131-151): the 31 phases before cycle 0, run backwards without
+// coupling, into the slots (0 - k) % 32 of state [32][n] (frequency [n]);
+// the host's float arithmetic is the plugin's (no contraction).
+static void init_kuramoto_history(const float* frequency, float* state, unsigned n)
+{
+	const unsigned H = 32;
+	for(unsigned k = 0; k < H - 1; k++) {
+		const unsigned current = 0U - k, previous = 0U - (k + 1U);
+		const float* phase0 = state + (size_t) (current % H) * n;
+		float* phase1 = state + (size_t) (previous % H) * n;
+		for(unsigned i = 0; i < n; i++) {
+			const float phase = phase0[i] - frequency[i];
+			phase1[i] = (float) ((double) fmodf(phase, (float) (2.0f * M_PI)) + (phase < 0.0f ? 2.0f * M_PI : 0.0f));
+		}
+	}
+}
+
 Simulation::Simulation(const Network& net, const Configuration& conf) :
 	Simulation(std::vector<const Network*>{ &net }, conf)
 {
@@ -1422,7 +1461,8 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 			}
 		}
 		const unsigned np = ht.desc.nparam, ns = ht.desc.nstate, na = np + ns;
-		std::vector<float> param((size_t) np * ht.n), state((size_t) ns * ht.n);
+		// state [history][nstate][n]: the given state in slot 0, the slot of cycle 0
+		std::vector<float> param((size_t) np * ht.n), state((size_t) ht.desc.history * ns * ht.n);
 		unsigned i0 = 0;
 		for(size_t i = 0; i < nets.size(); ++i) {
 			for(size_t t = 0; t < nets[i]->types.size(); ++t) {
@@ -1446,6 +1486,7 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 				i0 += (unsigned) c.size();
 			}
 		}
+		if(kind == KIND_KURAMOTO) init_kuramoto_history(param.data(), state.data(), ht.n);
 		ht.dParam = dalloc<float>(param.size());
 		ht.dState = dalloc<float>(state.size());
 		NB_CUDA(cudaMemcpyAsync(ht.dParam, param.data(), param.size() * 4, cudaMemcpyHostToDevice, m_stream));
@@ -1457,6 +1498,7 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 		tr.n = ht.n;
 		tr.param = ht.dParam;
 		tr.state = ht.dState;
+		tr.history = ht.desc.history;
 		m_types.push_back(ht);
 		l += ht.n;
 		NB_CUDA(cudaStreamSynchronize(m_stream)); // host vectors go out of scope
@@ -1487,6 +1529,59 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 				splastic[k] = net.plastic[q];
 			}
 		}
+	}
+
+	// the reverse matrix of all synapses, for a type that reads its sources
+	// (construction/RCM.cpp:58-99 and 150-172 with STDP off); it cannot
+	// coexist with STDP's (:90-98)
+	{
+		bool needAll = false;
+		for(const HostType& t : m_types) {
+			needAll |= t.desc.rcmSources || t.desc.rcmDelays || t.desc.rcmForward || t.desc.rcmWeights;
+		}
+		if(needAll && conf.stdp) {
+			NB_THROW(NEMO_API_UNSUPPORTED, "The current version does not support a mix of STDP with neuron types "
+					"which require reverse connectivity for other purposes");
+		}
+		std::vector<unsigned long long> allPtr(N + 1, 0);
+		if(needAll) {
+			for(size_t k = 0; k < Sn; ++k) allPtr[ltgt[k] + 1]++;
+			for(unsigned t = 0; t < N; ++t) allPtr[t + 1] += allPtr[t];
+			hvector<uint32_t> asrc(Sn);
+			hvector<float> aw(Sn);
+			std::vector<unsigned long long> fill(allPtr.begin(), allPtr.end() - 1);
+			size_t k = 0;
+			for(const Network* np : nets) {
+				for(size_t q = 0; q < np->src.size(); ++q, ++k) {
+					// a Kuramoto neuron reads its sources' phases from its own
+					// type's history of 32 steps
+					const HostType& tt = m_types[m_ltype[ltgt[k]]];
+					if(tt.desc.kind == KIND_KURAMOTO) {
+						if(m_ltype[lsrc[k]] != m_ltype[ltgt[k]]) {
+							NB_THROW(NEMO_INVALID_INPUT, "Synapse %u -> %u: a Kuramoto oscillator's sources must be "
+									"Kuramoto oscillators", np->src[q], np->tgt[q]);
+						}
+						if(sdelay[k] > 31) {
+							NB_THROW(NEMO_INVALID_INPUT, "Synapse %u -> %u: delay %u beyond the 31 steps of phase "
+									"history a Kuramoto oscillator reads", np->src[q], np->tgt[q], sdelay[k]);
+						}
+					}
+					const unsigned long long p = fill[ltgt[k]]++;
+					asrc[p] = lsrc[k] | ((sdelay[k] - 1) << 26);
+					aw[p] = np->weight[q];
+				}
+			}
+			auto* dSrc = dalloc<uint32_t>(Sn);
+			auto* dW = dalloc<float>(Sn);
+			NB_CUDA(cudaMemcpyAsync(dSrc, asrc.data(), Sn * 4, cudaMemcpyHostToDevice, m_stream));
+			NB_CUDA(cudaMemcpyAsync(dW, aw.data(), Sn * 4, cudaMemcpyHostToDevice, m_stream));
+			S.allSrc = dSrc;
+			S.allW = dW;
+		}
+		auto* dPtr = dalloc<unsigned long long>(N + 1);
+		NB_CUDA(cudaMemcpyAsync(dPtr, allPtr.data(), (N + 1) * 8, cudaMemcpyHostToDevice, m_stream));
+		S.allPtr = dPtr;
+		NB_CUDA(cudaStreamSynchronize(m_stream));
 	}
 
 	// forward matrix (src/nemo/ConnectivityMatrix.cpp:65-162): outgoing
@@ -1855,7 +1950,8 @@ void Simulation::launchStep(bool /*fullRecord*/)
 			(uint32_t) (PHASE_DELIVER | PHASE_STDP | PHASE_RESET), 0u, 0, nullptr, 0u, 0u);
 	timedEnd();
 	timedBegin(K_STEP);
-	launch_chained(update_kernel_for(m_T), grid, m_T, 0, m_stream, m_dev, m_P, cur, ring, 0u, 0, nullptr);
+	launch_chained(update_kernel_for(m_T), grid, m_T, 0, m_stream, m_dev, m_P, cur, ring, (uint32_t) m_cycle, 0u, 0,
+			nullptr);
 	timedEnd();
 	m_cycle++;
 	m_timerSteps++;
@@ -1971,7 +2067,7 @@ void Simulation::buildGraph()
 	for(unsigned k = 0; k < GRAPH_STEPS; ++k) {
 		launch_chained(deliver_kernel, m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream, m_dev, 0u,
 				(uint32_t) (PHASE_DELIVER | PHASE_STDP | PHASE_RESET), k, 1, nullptr, 0u, 0u);
-		launch_chained(update_kernel_for(m_T), grid, m_T, 0, m_stream, m_dev, m_P, 0u, 0u, k, 1, nullptr);
+		launch_chained(update_kernel_for(m_T), grid, m_T, 0, m_stream, m_dev, m_P, 0u, 0u, 0u, k, 1, nullptr);
 	}
 	advance_cycle_kernel<<<1, 1, 0, m_stream>>>(m_dev.cycleDev, GRAPH_STEPS);
 	NB_CUDA(cudaStreamEndCapture(m_stream, &g));
@@ -2157,7 +2253,8 @@ const std::vector<unsigned>& Simulation::step(const unsigned* fstim, size_t nf,
 	launch_chained(deliver_kernel, m_deliverGrid, STEP_THREADS, m_dev.recentBytes, m_stream, m_dev, c ^ 1u,
 			(uint32_t) (PHASE_DELIVER | PHASE_STDP | PHASE_RESET), 0u, 0,
 			need ? (const uint32_t*) m_dStimMapped : nullptr, (uint32_t) nf, (uint32_t) cur.size());
-	launch_chained(update_kernel_for(m_T), (m_N + m_P - 1) / m_P, m_T, 0, m_stream, m_dev, m_P, c, ring, 0u, 0,
+	launch_chained(update_kernel_for(m_T), (m_N + m_P - 1) / m_P, m_T, 0, m_stream, m_dev, m_P, c, ring,
+			(uint32_t) m_cycle, 0u, 0,
 			m_dFiredMapped);
 	m_cycle++;
 	m_timerSteps++;
@@ -2366,7 +2463,7 @@ float Simulation::autotune(unsigned trialSteps)
 	trialSteps = std::max(1u, trialSteps);
 	// the state that trial steps modify
 	std::vector<std::pair<void*, size_t>> regions;
-	for(const HostType& t : m_types) regions.emplace_back(t.dState, (size_t) t.n * t.desc.nstate * 4);
+	for(const HostType& t : m_types) regions.emplace_back(t.dState, (size_t) t.n * t.desc.nstate * t.desc.history * 4);
 	regions.emplace_back(m_dev.rng, (size_t) 4 * m_N * 4);
 	regions.emplace_back(m_dev.hist, (size_t) 2 * m_N * 8);
 	regions.emplace_back(m_dev.recent, (size_t) 2 * m_dev.recentWords * 4);
@@ -2513,6 +2610,13 @@ unsigned Simulation::tracePhases(unsigned steps, uint64_t* out, size_t cap)
 	return grid;
 }
 
+// the state of the current cycle of a type (slot cycle % history;
+// src/nemo/cpu/Neurons.cpp:80-92, :123)
+float* Simulation::currentState(const HostType& t) const
+{
+	return t.dState + (size_t) (m_cycle % t.desc.history) * t.desc.nstate * t.n;
+}
+
 float Simulation::getNeuronState(unsigned g, unsigned var)
 {
 	const HostType* t; unsigned i;
@@ -2520,7 +2624,7 @@ float Simulation::getNeuronState(unsigned g, unsigned var)
 	if(var >= t->desc.nstate) NB_THROW(NEMO_INVALID_INPUT, "Invalid state variable index %u", var);
 	float v;
 	NB_CUDA(cudaSetDevice(m_device));
-	NB_CUDA(cudaMemcpyAsync(&v, t->dState + (size_t) var * t->n + i, 4, cudaMemcpyDeviceToHost, m_stream));
+	NB_CUDA(cudaMemcpyAsync(&v, currentState(*t) + (size_t) var * t->n + i, 4, cudaMemcpyDeviceToHost, m_stream));
 	sync();
 	return v;
 }
@@ -2558,7 +2662,8 @@ void Simulation::setNeuron(unsigned g, unsigned nargs, const float* args)
 		NB_CUDA(cudaMemcpyAsync(t->dParam + (size_t) p * t->n + i, args + p, 4, cudaMemcpyHostToDevice, m_stream));
 	}
 	for(unsigned v = 0; v < ns; ++v) {
-		NB_CUDA(cudaMemcpyAsync(t->dState + (size_t) v * t->n + i, args + np + v, 4, cudaMemcpyHostToDevice, m_stream));
+		NB_CUDA(cudaMemcpyAsync(currentState(*t) + (size_t) v * t->n + i, args + np + v, 4, cudaMemcpyHostToDevice,
+				m_stream));
 	}
 	sync();
 }
@@ -2569,7 +2674,7 @@ void Simulation::setNeuronState(unsigned g, unsigned var, float v)
 	locate(g, &t, &i);
 	if(var >= t->desc.nstate) NB_THROW(NEMO_INVALID_INPUT, "Invalid state variable index %u", var);
 	NB_CUDA(cudaSetDevice(m_device));
-	NB_CUDA(cudaMemcpyAsync(t->dState + (size_t) var * t->n + i, &v, 4, cudaMemcpyHostToDevice, m_stream));
+	NB_CUDA(cudaMemcpyAsync(currentState(*t) + (size_t) var * t->n + i, &v, 4, cudaMemcpyHostToDevice, m_stream));
 	sync();
 }
 
@@ -2662,7 +2767,7 @@ void Simulation::getNetTypeState(unsigned net, unsigned netType, float* out, siz
 	if(cap < n) NB_THROW(NEMO_BUFFER_OVERFLOW, "state buffer too small");
 	NB_CUDA(cudaSetDevice(m_device));
 	for(unsigned v = 0; v < t.desc.nstate; ++v) {
-		NB_CUDA(cudaMemcpyAsync(out + (size_t) v * r.count, t.dState + (size_t) v * t.n + r.offset,
+		NB_CUDA(cudaMemcpyAsync(out + (size_t) v * r.count, currentState(t) + (size_t) v * t.n + r.offset,
 				(size_t) r.count * 4, cudaMemcpyDeviceToHost, m_stream));
 	}
 	sync();

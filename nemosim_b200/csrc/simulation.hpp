@@ -66,7 +66,8 @@ struct TypeRange {
 	int kind;
 	uint32_t base, n;
 	const float* param;  // [nparam][n]
-	float* state;        // [nstate][n]
+	float* state;        // [history][nstate][n]; slot cycle % history is the current one
+	uint32_t history;
 };
 
 // STDP process in fixed point (src/nemo/StdpProcess.cpp:20-46)
@@ -130,6 +131,12 @@ struct DevSim {
 	const uint32_t* rcmFwd;   // index into syn
 	int32_t* rcmAcc;          // STDP accumulator per incoming plastic synapse
 	int32_t* rcmW;            // the plastic synapse's weight (equal to its syn entry's), in reverse order
+	// reverse matrix of all synapses into the targets of a type that reads
+	// its sources (Kuramoto): per target, source | (delay - 1) << 26 and the
+	// weight as given
+	const unsigned long long* allPtr;
+	const uint32_t* allSrc;
+	const float* allW;
 	// work published by a step's update for the next pre-phase: the delay
 	// groups arriving next step (ranges of syn) and the incoming plastic
 	// synapses of its STDP targets (ranges of the reverse matrix)
@@ -248,6 +255,7 @@ private:
 		float* dState = nullptr;
 	};
 
+	float* currentState(const HostType& t) const;
 	unsigned localIdx(unsigned g) const;
 	bool findLocal(unsigned g, unsigned* l) const;  // localIdx without throwing (one network)
 	void locate(unsigned g, const HostType** t, unsigned* i) const;

@@ -221,16 +221,19 @@ static int hmap_insert(hmap* m, uint32_t k, uint64_t v, uint64_t** slot)
 /* Neuron types: .ini descriptors src/nemo/plugins/<Type>.ini and index   */
 /* headers src/nemo/plugins/Izhikevich.h, IF_curr_exp.h                   */
 
-enum { KIND_IZHIKEVICH, KIND_IF_CURR_EXP, KIND_POISSON, KIND_INPUT, KIND_IZHIKEVICH_RS };
+enum { KIND_IZHIKEVICH, KIND_IF_CURR_EXP, KIND_POISSON, KIND_INPUT, KIND_IZHIKEVICH_RS, KIND_KURAMOTO };
 
-typedef struct { const char* name; int kind; unsigned nparam, nstate, mpot; } type_desc;
+/* history: state history length; rcm: needs the reverse matrix of all
+ * synapses (sources, delays, weights) */
+typedef struct { const char* name; int kind; unsigned nparam, nstate, mpot, history; int rcm; } type_desc;
 
 static const type_desc TYPES[] = {
-	{ "Izhikevich", KIND_IZHIKEVICH, 5, 2, 1 },    /* Izhikevich.ini:2-4 */
-	{ "IF_curr_exp", KIND_IF_CURR_EXP, 9, 4, 0 },  /* IF_curr_exp.ini:14-24 */
-	{ "PoissonSource", KIND_POISSON, 1, 0, 0 },    /* PoissonSource.ini:1-3 */
-	{ "Input", KIND_INPUT, 0, 0, 0 },              /* Input.ini:1-3 */
-	{ "IzhikevichRS", KIND_IZHIKEVICH_RS, 0, 2, 1 },  /* IzhikevichRS.ini:3-5 */
+	{ "Izhikevich", KIND_IZHIKEVICH, 5, 2, 1, 1, 0 },    /* Izhikevich.ini:2-4 */
+	{ "IF_curr_exp", KIND_IF_CURR_EXP, 9, 4, 0, 1, 0 },  /* IF_curr_exp.ini:14-24 */
+	{ "PoissonSource", KIND_POISSON, 1, 0, 0, 1, 0 },    /* PoissonSource.ini:1-3 */
+	{ "Input", KIND_INPUT, 0, 0, 0, 1, 0 },              /* Input.ini:1-3 */
+	{ "IzhikevichRS", KIND_IZHIKEVICH_RS, 0, 2, 1, 1, 0 },  /* IzhikevichRS.ini:3-5 */
+	{ "Kuramoto", KIND_KURAMOTO, 1, 1, 0, 32, 1 },       /* Kuramoto.ini:2-14 */
 };
 #define NTYPES_KNOWN (sizeof TYPES / sizeof TYPES[0])
 
@@ -450,7 +453,7 @@ typedef struct {
 	unsigned netType;   /* network type id; types without neurons are skipped */
 	unsigned base, n;
 	float* param;   /* [nparam][n] */
-	float* state;   /* [nstate][n] */
+	float* state;   /* [history][nstate][n]; slot cycle % history is the current one */
 	unsigned* rng;  /* [n][4] */
 } sim_type;
 
@@ -499,6 +502,14 @@ struct nemo_oracle_simulation {
 	uint64_t potBits, depBits, prePostBits, postPreBits, postFireMask;
 	int32_t minE, maxE, minI, maxI;
 
+	/* reverse matrix of all synapses, per target, for a type that reads
+	 * its sources (construction/RCM.cpp:58-99, 150-172 with STDP off):
+	 * source, delay, the weight as given */
+	size_t* allStart;   /* ncount + 1 */
+	uint32_t* allSource;
+	uint32_t* allDelay;
+	float* allWeight;
+
 	/* reverse matrix (plastic synapses only when STDP is on), per target */
 	size_t* rcmStart;   /* ncount + 1 */
 	uint32_t* rcmSource;
@@ -533,6 +544,7 @@ void nemo_oracle_delete_simulation(nemo_oracle_simulation* s)
 	hmap_free(&s->aux); free(s->auxFirst); free(s->auxCount); free(s->auxIdx); free(s->auxDelay); free(s->auxPlastic); free(s->queried);
 	free(s->fnPre); free(s->fnPost);
 	free(s->rcmStart); free(s->rcmSource); free(s->rcmDelay); free(s->rcmForward); free(s->rcmAcc);
+	free(s->allStart); free(s->allSource); free(s->allDelay); free(s->allWeight);
 	free(s->firedList);
 	free(s);
 }
@@ -562,6 +574,8 @@ static size_t* iteration_order(const nemo_oracle_network* net)
 	free(tmp); free(cnt);
 	return order;
 }
+
+static void init_kuramoto(sim_type* t);
 
 nemo_oracle_simulation* nemo_oracle_new_simulation(nemo_oracle_network* net, nemo_oracle_configuration* conf)
 {
@@ -617,7 +631,7 @@ nemo_oracle_simulation* nemo_oracle_new_simulation(nemo_oracle_network* net, nem
 		st->n = (unsigned) c->n;
 		unsigned np = c->desc->nparam, ns = c->desc->nstate, na = np + ns;
 		st->param = malloc((np * c->n + 1) * sizeof(float));
-		st->state = malloc((ns * c->n + 1) * sizeof(float));
+		st->state = calloc(c->desc->history * ns * c->n + 1, sizeof(float));
 		st->rng = malloc(4 * c->n * sizeof(unsigned));
 		for(size_t i = 0; i < c->n; ++i) {
 			for(unsigned p = 0; p < np; ++p) st->param[p * c->n + i] = c->args[i * na + p];
@@ -628,6 +642,7 @@ nemo_oracle_simulation* nemo_oracle_new_simulation(nemo_oracle_network* net, nem
 		}
 		/* RNG seeding by local index (cpu/Neurons.cpp:41, RNG.cpp:38-63) */
 		nemo_oracle_seed_states(st->base, st->n, st->rng);
+		if(c->desc->kind == KIND_KURAMOTO) init_kuramoto(st);
 		l += st->n;
 	}
 
@@ -653,6 +668,32 @@ nemo_oracle_simulation* nemo_oracle_new_simulation(nemo_oracle_network* net, nem
 		ltgt[k] = local_idx(s, sy->tgt[i], &ok);
 		if(!ok) { fail(NEMO_INVALID_INPUT, "Non-existing neuron index %u", sy->tgt[i]); goto bad; }
 		if(fx_toFix(sy->weight[i], &fxw[k]) != NEMO_OK) goto bad;
+	}
+
+	/* a type that reads its sources needs the reverse matrix of all synapses,
+	 * which cannot coexist with STDP's (construction/RCM.cpp:90-98) */
+	int needAll = 0;
+	for(unsigned t = 0; t < s->ntypes; ++t) needAll |= s->types[t].desc->rcm;
+	if(needAll && conf->stdp) {
+		fail(NEMO_API_UNSUPPORTED, "The current version does not support a mix of STDP with neuron types which require reverse connectivity for other purposes");
+		goto bad;
+	}
+	if(needAll) {
+		s->allStart = calloc(N + 1, sizeof(size_t));
+		for(size_t k = 0; k < S; ++k) s->allStart[ltgt[k] + 1]++;
+		for(size_t n = 0; n < N; ++n) s->allStart[n+1] += s->allStart[n];
+		s->allSource = malloc((S ? S : 1) * sizeof(uint32_t));
+		s->allDelay = malloc((S ? S : 1) * sizeof(uint32_t));
+		s->allWeight = malloc((S ? S : 1) * sizeof(float));
+		size_t* afill = malloc((N ? N : 1) * sizeof(size_t));
+		memcpy(afill, s->allStart, N * sizeof(size_t));
+		for(size_t k = 0; k < S; ++k) {
+			size_t p = afill[ltgt[k]]++;
+			s->allSource[p] = lsrc[k];
+			s->allDelay[p] = sy->delay[order[k]];
+			s->allWeight[p] = sy->weight[order[k]];
+		}
+		free(afill);
 	}
 
 	{
@@ -970,6 +1011,65 @@ static void update_izhikevich_rs(nemo_oracle_simulation* s, sim_type* t)
 	}
 }
 
+/* Kuramoto oscillators, cpu/plugins/Kuramoto.cpp (plugins/Kuramoto.h):
+ * parameter the frequency, state the phase, kept for the last 32 cycles.
+ * Each update integrates the phase with one fourth-order Runge-Kutta step
+ * whose coupling sums, over the incoming synapses in reverse-matrix order,
+ * weight x sinf(source phase at emission - target phase); the source phase
+ * is the one at cycle - (delay - 1).  The neuron never fires. */
+#define KURAMOTO_HISTORY 32
+
+static float* kuramoto_phase(sim_type* t, unsigned long cycle)
+{
+	return t->state + (size_t) (cycle % KURAMOTO_HISTORY) * t->n;
+}
+
+/* sumN (cpu/plugins/Kuramoto.cpp:17-30) */
+static float kuramoto_coupling(nemo_oracle_simulation* s, sim_type* t, unsigned ng, float targetPhase)
+{
+	float sum = 0.0f;
+	for(size_t k = s->allStart[ng]; k < s->allStart[ng + 1]; ++k) {
+		const float* src = kuramoto_phase(t, s->cycle - (s->allDelay[k] - 1));
+		sum += s->allWeight[k] * sinf(src[s->allSource[k] - t->base] - targetPhase);
+	}
+	return sum;
+}
+
+/* cpu_update_neurons (cpu/plugins/Kuramoto.cpp:78-124) */
+static void update_kuramoto(nemo_oracle_simulation* s, sim_type* t)
+{
+	const float* frequency = t->param;
+	const float* phase0 = kuramoto_phase(t, s->cycle);
+	float* phase1 = kuramoto_phase(t, s->cycle + 1);
+	for(unsigned nl = 0; nl < t->n; ++nl) {
+		const unsigned ng = t->base + nl;
+		const float f = frequency[nl];
+		float targetPhase = phase0[nl];
+		float k0 = f + kuramoto_coupling(s, t, ng, targetPhase);
+		float k1 = f + kuramoto_coupling(s, t, ng, targetPhase + k0 * 0.5f);
+		float k2 = f + kuramoto_coupling(s, t, ng, targetPhase + k1 * 0.5f);
+		float k3 = f + kuramoto_coupling(s, t, ng, targetPhase + k2);
+		targetPhase += (k0 + 2 * k1 + 2 * k2 + k3) / 6.0f;
+		phase1[nl] = fmodf(targetPhase, 2.0f * M_PI) + (targetPhase < 0.0f ? 2.0f * M_PI : 0.0f);
+	}
+}
+
+/* cpu_init_neurons (cpu/plugins/Kuramoto.cpp:131-151): the history before
+ * cycle 0, run backwards without coupling */
+static void init_kuramoto(sim_type* t)
+{
+	const float* frequency = t->param;
+	for(unsigned k = 0; k < KURAMOTO_HISTORY - 1; k++) {
+		const unsigned current = 0U - k, previous = 0U - (k + 1U);
+		const float* phase0 = t->state + (size_t) (current % KURAMOTO_HISTORY) * t->n;
+		float* phase1 = t->state + (size_t) (previous % KURAMOTO_HISTORY) * t->n;
+		for(unsigned nl = 0; nl < t->n; nl++) {
+			float phase = phase0[nl] - frequency[nl];
+			phase1[nl] = fmodf(phase, 2.0f * M_PI) + (phase < 0.0f ? 2.0f * M_PI : 0.0f);
+		}
+	}
+}
+
 /* ConnectivityMatrix::accumulateStdp, ConnectivityMatrix.cpp:193-227 */
 static void accumulate_stdp(nemo_oracle_simulation* s)
 {
@@ -995,6 +1095,7 @@ static void fire(nemo_oracle_simulation* s)
 			case KIND_POISSON: update_poisson(s, st); break;
 			case KIND_INPUT: update_input(s, st); break;
 			case KIND_IZHIKEVICH_RS: update_izhikevich_rs(s, st); break;
+			case KIND_KURAMOTO: update_kuramoto(s, st); break;
 		}
 	}
 	accumulate_stdp(s);
@@ -1101,12 +1202,18 @@ static int locate(nemo_oracle_simulation* s, unsigned g, sim_type** t, unsigned*
 	return NEMO_OK;
 }
 
+/* the state of the current cycle (cpu/Neurons.cpp:80-92, :123) */
+static float* current_state(nemo_oracle_simulation* s, sim_type* t)
+{
+	return t->state + (size_t) (s->cycle % t->desc->history) * t->desc->nstate * t->n;
+}
+
 int nemo_oracle_get_neuron_state(nemo_oracle_simulation* s, unsigned g, unsigned var, float* val)
 {
 	sim_type* t; unsigned i;
 	int r = locate(s, g, &t, &i); if(r) return r;
 	if(var >= t->desc->nstate) return fail(NEMO_INVALID_INPUT, "Invalid state variable index %u", var);
-	*val = t->state[var * t->n + i];
+	*val = current_state(s, t)[var * t->n + i];
 	return NEMO_OK;
 }
 
@@ -1131,7 +1238,7 @@ int nemo_oracle_set_neuron_state(nemo_oracle_simulation* s, unsigned g, unsigned
 	sim_type* t; unsigned i;
 	int r = locate(s, g, &t, &i); if(r) return r;
 	if(var >= t->desc->nstate) return fail(NEMO_INVALID_INPUT, "Invalid state variable index %u", var);
-	t->state[var * t->n + i] = val;
+	current_state(s, t)[var * t->n + i] = val;
 	return NEMO_OK;
 }
 
@@ -1155,7 +1262,7 @@ int nemo_oracle_set_neuron(nemo_oracle_simulation* s, unsigned g, unsigned nargs
 				"Unexpected number of parameters/state variables when modifying neuron. Expected %u, found %u", np + ns, nargs);
 	}
 	for(unsigned p = 0; p < np; ++p) t->param[p * t->n + i] = args[p];
-	for(unsigned v = 0; v < ns; ++v) t->state[v * t->n + i] = args[np + v];
+	for(unsigned v = 0; v < ns; ++v) current_state(s, t)[v * t->n + i] = args[np + v];
 	return NEMO_OK;
 }
 
@@ -1237,7 +1344,7 @@ int nemo_oracle_get_type_state(nemo_oracle_simulation* s, unsigned type, float* 
 		if(s->types[t].netType != type) continue;
 		size_t n = (size_t) s->types[t].n * s->types[t].desc->nstate;
 		if(cap < n) return fail(NEMO_BUFFER_OVERFLOW, "state buffer too small");
-		memcpy(out, s->types[t].state, n * sizeof(float));
+		memcpy(out, current_state(s, &s->types[t]), n * sizeof(float));
 		*len = n;
 		return NEMO_OK;
 	}

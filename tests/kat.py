@@ -579,3 +579,134 @@ def izhikevich_rs_network(mod, steps=500, seed=11, resident=True):
         istim = [(int(i), 12.0) for i in rng.choice(n, 30, replace=False)] if t % 7 == 0 else None
         stream.append(sim.step(fstim, istim))
     return stream, sim.type_state(rs, 2, n)
+
+
+def close(a, b, percent=0.001):
+    """BOOST_REQUIRE_CLOSE: |a - b| within `percent` % of both a and b"""
+    d = abs(float(a) - float(b))
+    return d <= percent / 100 * abs(float(a)) and d <= percent / 100 * abs(float(b))
+
+
+def oscillator_network(mod):
+    """OscillatorNetwork (src/test/Kuramoto.cpp:11-34)"""
+    net = mod.Network()
+    return net, net.add_neuron_type("Kuramoto")
+
+
+def kuramoto_init(mod):
+    """testInit (src/test/Kuramoto.cpp:42-61)"""
+    net, k = oscillator_network(mod)
+    net.add_neuron(k, 0, 0.1, 0.0)
+    sim = mod.Simulation(net, mod.Configuration())
+    assert sim.get_neuron_state(0, 0) == 0.0
+    sim.step()
+    assert close(sim.get_neuron_state(0, 0), f32(0.0) + f32(0.1))
+
+
+def kuramoto_uncoupled(mod):
+    """testUncoupled (src/test/Kuramoto.cpp:65-86)"""
+    net, k = oscillator_network(mod)
+    n, freq = 1200, f32(0.1)
+    net.add_neuron(k, np.arange(n, dtype=np.uint32), freq, 0.0)
+    sim = mod.Simulation(net, mod.Configuration())
+    phase = f32(0.0)
+    for _ in range(1000):
+        sim.step()
+        phase = np.fmod(f32(phase + freq), f32(2 * np.pi))
+        assert close(sim.get_neuron_state(n // 2, 0), phase)
+
+
+def kuramoto_simple_coupled(mod):
+    """testSimpleCoupled (src/test/Kuramoto.cpp:90-122).  Returns both
+    phases after every step."""
+    net, k = oscillator_network(mod)
+    freq, phase = [f32(0.1), f32(0.1)], [f32(0.0), f32(1.57)]
+    net.add_neuron(k, 0, freq[0], phase[0])
+    net.add_neuron(k, 1, freq[1], phase[1])
+    net.add_synapse(0, 1, 1, 1.0, False)
+    sim = mod.Simulation(net, mod.Configuration())
+    seen = []
+    for _ in range(100):
+        sim.step()
+        k1 = f32(freq[0] + np.sin(phase[0] - phase[1]))
+        k2 = f32(freq[0] + np.sin(phase[0] - f32(phase[1] + f32(0.5) * k1)))
+        k3 = f32(freq[0] + np.sin(phase[0] - f32(phase[1] + f32(0.5) * k2)))
+        k4 = f32(freq[0] + np.sin(phase[0] - f32(phase[1] + k3)))
+        phase[1] = f32(phase[1] + f32(f32(k1 + f32(2.0) * k2 + f32(2.0) * k3 + k4) / f32(6.0)))
+        phase[0] = f32(phase[0] + freq[0])
+        for i in range(2):
+            phase[i] = np.fmod(phase[i], f32(2 * np.pi))
+            assert close(sim.get_neuron_state(i, 0), phase[i]), (i, sim.get_neuron_state(i, 0), phase[i])
+        seen.append([sim.get_neuron_state(0, 0), sim.get_neuron_state(1, 0)])
+    return np.array(seen, np.float32)
+
+
+def kuramoto_n_to_1(mod, ncount, noise):
+    """testNto1 (src/test/Kuramoto.cpp:126-185): one oscillator driven by
+    ncount others of strength 1/ncount (with zero-strength couplings among
+    the others when `noise`).  Returns the driven phase after every step."""
+    net, k = oscillator_network(mod)
+    freq, strength = f32(0.1), f32(1.0 / ncount)
+    phase0 = phaseN = f32(0.0)
+    net.add_neuron(k, 0, freq, phase0)
+    for n in range(ncount):
+        net.add_neuron(k, n + 1, freq, phaseN)
+        net.add_synapse(n + 1, 0, 1, strength, False)
+        if noise:
+            tgts = [t for t in range(1, ncount) if t != n + 1]
+            if tgts:
+                net.add_synapse(np.full(len(tgts), n + 1, np.uint32), np.array(tgts, np.uint32),
+                                np.ones(len(tgts), np.uint32), np.zeros(len(tgts), f32), np.zeros(len(tgts), np.uint8))
+    sim = mod.Simulation(net, mod.Configuration())
+    seen = []
+    for _ in range(50):
+        sim.step()
+        w = f32(ncount) * strength
+        k1 = f32(freq + w * np.sin(f32(phaseN - phase0), dtype=f32))
+        k2 = f32(freq + w * np.sin(f32(phaseN - f32(phase0 + f32(0.5) * k1)), dtype=f32))
+        k3 = f32(freq + w * np.sin(f32(phaseN - f32(phase0 + f32(0.5) * k2)), dtype=f32))
+        k4 = f32(freq + w * np.sin(f32(phaseN - f32(phase0 + k3)), dtype=f32))
+        phase0 = f32(phase0 + f32(f32(k1 + f32(2.0) * k2 + f32(2.0) * k3 + k4) / f32(6.0)))
+        phase0 = np.fmod(phase0, f32(2 * np.pi))
+        phaseN = np.fmod(f32(phaseN + freq), f32(2 * np.pi))
+        assert close(sim.get_neuron_state(0, 0), phase0), (sim.get_neuron_state(0, 0), phase0)
+        for n in range(0, ncount, max(1, ncount // 7)):
+            assert close(sim.get_neuron_state(n + 1, 0), phaseN)
+        seen.append(sim.get_neuron_state(0, 0))
+    return np.array(seen, np.float32)
+
+
+def kuramoto_with_stdp_fails(mod):
+    """A type that reads its sources cannot coexist with STDP
+    (src/nemo/construction/RCM.cpp:90-98): NEMO_API_UNSUPPORTED"""
+    net, k = oscillator_network(mod)
+    net.add_neuron(k, 0, 0.1, 0.0)
+    net.add_neuron(k, 1, 0.1, 1.0)
+    net.add_synapse(0, 1, 1, 1.0, True)
+    try:
+        mod.Simulation(net, nets.standard_stdp(mod))
+    except mod.NemoError as e:
+        assert "does not support a mix of STDP" in str(e)
+        return e.code
+    raise AssertionError("STDP with a reverse-matrix type accepted")
+
+
+def kuramoto_random(mod, ncount=2048, scount=32, steps=1000, seed=5):
+    """The reference's example oscillator network (src/examples/
+    kuramoto.cpp:49-68): frequencies U(0, 0.2), phases U(0, 2 pi), scount
+    outgoing couplings of strength 0.001 and lag 1 to uniform targets; here
+    with lags 1-20 as well.  Seeded numpy draws stand in for the Boost
+    generator.  Returns the phases after `steps` steps."""
+    rng = np.random.default_rng(seed)
+    net, k = oscillator_network(mod)
+    freq = rng.uniform(0.0, 0.2, ncount).astype(f32)
+    phase = rng.uniform(0.0, 2 * np.pi, ncount).astype(f32)
+    net.add_neuron(k, np.arange(ncount, dtype=np.uint32), freq, phase)
+    src = np.repeat(np.arange(ncount, dtype=np.uint32), scount)
+    tgt = rng.integers(0, ncount, len(src)).astype(np.uint32)
+    lag = rng.integers(1, 21, len(src)).astype(np.uint32)
+    net.add_synapse(src, tgt, lag, np.full(len(src), 0.001, f32), np.zeros(len(src), np.uint8))
+    sim = mod.Simulation(net, mod.Configuration())
+    for _ in range(steps):
+        assert sim.step() == []
+    return sim.type_state(k, 1, ncount)[0]

@@ -107,6 +107,17 @@ def test_izhikevich_rs():
     assert sum(len(f) for f in stream) > 500
 
 
+def test_kuramoto():
+    """src/test/Kuramoto.cpp against the analytic phases (the reference's
+    0.001 % tolerance)"""
+    kat.kuramoto_init(O)
+    kat.kuramoto_uncoupled(O)
+    kat.kuramoto_simple_coupled(O)
+    for n, noise in [(2, False), (100, False), (100, True), (256, False)]:
+        kat.kuramoto_n_to_1(O, n, noise)
+    kat.kuramoto_with_stdp_fails(O)
+
+
 def test_ring_delay_80_rejected():
     """The CPU backend rejects delays above 64 (src/nemo/cpu/Simulation.cpp:52-56)."""
     with pytest.raises(O.NemoError):

@@ -178,6 +178,62 @@ def test_izhikevich_rs_network(resident):
     assert same_bits(p[1], o[1])
 
 
+def test_kuramoto_known_answers():
+    """src/test/Kuramoto.cpp on the device, against the analytic phases with
+    the reference's 0.001 % tolerance; STDP with a type that reads its
+    sources is refused with NEMO_API_UNSUPPORTED"""
+    kat.kuramoto_init(nb)
+    kat.kuramoto_uncoupled(nb)
+    kat.kuramoto_simple_coupled(nb)
+    for n, noise in [(2, False), (100, False), (100, True), (256, False)]:
+        kat.kuramoto_n_to_1(nb, n, noise)
+    assert kat.kuramoto_with_stdp_fails(nb) == 5
+
+
+@pytest.mark.parametrize("persistent", [True, False])
+def test_kuramoto_matches_oracle(persistent):
+    """A 2048-oscillator network with delayed couplings, 1000 steps: the
+    phases agree with the oracle's to 1e-4 radian.  Not bit for bit: the
+    device's sinf is CUDA's, the oracle's the host libm's."""
+    class Persistent:
+        def __init__(self, on):
+            self.on = on
+
+        def __getattr__(self, name):
+            return getattr(nb, name)
+
+        def Simulation(self, net, conf):
+            sim = nb.Simulation(net, conf)
+            sim.set_persistent(self.on)
+            return sim
+
+    mod = Persistent(persistent)
+    p = kat.kuramoto_random(mod, steps=300)
+    o = kat.kuramoto_random(O, steps=300)
+    d = np.abs(((p.astype(np.float64) - o + np.pi) % (2 * np.pi)) - np.pi)
+    assert d.max() < 1e-4, d.max()
+
+
+def test_kuramoto_source_and_delay_checks():
+    """A Kuramoto oscillator reads its sources' phases from its own type's
+    32-step history: other sources, or delays above 31, are refused"""
+    net, k = kat.oscillator_network(nb)
+    iz = net.add_neuron_type("Izhikevich")
+    net.add_neuron(k, 0, 0.1, 0.0)
+    net.add_neuron(iz, 1, *nets.exc_neuron_args())
+    net.add_synapse(1, 0, 1, 1.0, False)
+    with pytest.raises(nb.NemoError) as e:
+        nb.Simulation(net, nb.Configuration())
+    assert e.value.code == 6
+    net, k = kat.oscillator_network(nb)
+    net.add_neuron(k, 0, 0.1, 0.0)
+    net.add_neuron(k, 1, 0.1, 1.0)
+    net.add_synapse(1, 0, 32, 1.0, False)
+    with pytest.raises(nb.NemoError) as e:
+        nb.Simulation(net, nb.Configuration())
+    assert e.value.code == 6
+
+
 # ---------------------------------------------------------------------------
 # bit-exact parity with the oracle on noisy networks
 
