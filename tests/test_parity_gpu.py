@@ -366,7 +366,7 @@ def test_phase_trace_advances_like_run():
     a.run(100, 100, 1.0)
     b.run(100, 100, 1.0)
     tr = a.trace_phases(100)
-    b.run(100, 100, 1.0)
+    b.run(100)  # the traced launch is a run's launch without applyStdp
     assert tr.shape[0] == 100 and tr.shape[2] == 5
     assert np.all(np.diff(tr.astype(np.int64), axis=2) >= 0)
     ra = a.run(200, 100, 1.0)
