@@ -292,15 +292,19 @@ def run_b200(args, rank, world, local):
 
     t0 = time.perf_counter()
     net = nb.example_random(args.neurons, SYNAPSES, DMAX, True)
+    gen_s = time.perf_counter() - t0
     conf = stdp_conf(nb)
     conf.set_cuda_backend(local)
+    if args.host_construction:
+        conf.set_device_construction(False)
+    t0 = time.perf_counter()
     sim = nb.Simulation(net, conf)
+    build_s = time.perf_counter() - t0
     del net
     if args.no_graphs:
         sim.set_graphs(False)
     if args.no_persistent:
         sim.set_persistent(False)
-    build_s = time.perf_counter() - t0
     W = args.window
 
     # warm-up, then the launch-shape autotuner (its trial steps start from a
@@ -444,7 +448,11 @@ def run_b200(args, rank, world, local):
             # and apply kernels
             "gpu_launches": args.steps * ((1 if persistent else 2 * W + (W // 100)) + 2),
             "clocks": clk.summary(),
+            # network generation (the random example's own loop, on the host)
+            # and the simulation's construction from it, both untimed
+            "network_gen_s": gen_s,
             "build_s": build_s,
+            "built_on_device": sim.connectivity_digest()[1],
             "phases_us": phases,
             "launch": {"partition": launch[0], "threads": launch[1],
                        "autotuned_us_per_step": tuned_us,
@@ -589,13 +597,19 @@ def run_bptt(args, local):
     W, a, b = net.tensors(dev)
     c, d = net.constants(dev)
     st = baseline.Structure(net.source, net.target, net.delay, N, dev)
+    torch_reps = 2
+    for _ in range(max(1, min(args.warmup, 2))):  # warm-up: allocator, kernels' first launches
+        W.grad = a.grad = b.grad = None
+        baseline.loss(W, a, b, c, d, noise, target, st, R, False).backward()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     start.record()
-    baseline.loss(W, a, b, c, d, noise, target, st, R, False).backward()
+    for _ in range(torch_reps):
+        W.grad = a.grad = b.grad = None
+        baseline.loss(W, a, b, c, d, noise, target, st, R, False).backward()
     end.record()
     torch.cuda.synchronize()
-    torch_ms = start.elapsed_time(end)
+    torch_ms = start.elapsed_time(end) / torch_reps
     line = {
         "metric": "BPTT gradient step speedup vs PyTorch autograd (same GPU)", "value": torch_ms / ms32,
         "unit": "x", "n_gpus": 1, "higher_is_better": True, "dtype": "fp32", "data": "synthetic",
@@ -604,6 +618,7 @@ def run_bptt(args, local):
                    "delays_ms": [1, 10], "noise_sigma": 5.0},
         "adjoint_ms": ms32, "adjoint_fp64_state_ms": ms64, "torch_autograd_ms": torch_ms,
         "speedup_fp64_state": torch_ms / ms64, "steps": args.steps, "warmup": args.warmup,
+        "torch_autograd_reps": torch_reps,
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
@@ -626,6 +641,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--no-persistent", action="store_true")
+    ap.add_argument("--host-construction", action="store_true",
+                    help="build the connectivity on the host instead of the device")
     ap.add_argument("--workload", choices=["headline", "batch256", "bptt"], default="headline",
                     help="headline: the 100k x 1k STDP network (default); batch256: batched networks "
                          "against sequential runs; bptt: differentiable mode against PyTorch autograd")

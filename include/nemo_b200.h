@@ -326,6 +326,23 @@ NEMO_B200_API nemo_status_t nemo_b200_trace_phases(nemo_simulation_t, unsigned s
  * loop that is running keeps the limit it was launched with; this call
  * ends it first. */
 NEMO_B200_API nemo_status_t nemo_b200_set_wait_limit(nemo_simulation_t, unsigned polls);
+/* Where a simulation created with this configuration builds its
+ * connectivity (the forward matrix sorted by source and delay, its delay
+ * groups, the reverse matrix of plastic synapses): on = 1 (the default)
+ * builds it on the device when the network allows it -- one network, global
+ * neuron ids below 4 per neuron plus 2^20, fewer than 2^31 - 1 synapses
+ * and neurons x maximum delay, no neuron type that reads the reverse
+ * matrix of all synapses -- and on the host otherwise; on = 0 always builds
+ * it on the host.  Both builds give the same bytes, the same errors and the
+ * same results. */
+NEMO_B200_API nemo_status_t nemo_b200_set_device_construction(nemo_configuration_t, int on);
+/* Digests of the simulation's connectivity as it sits in device memory:
+ * out[0..7] hash the forward matrix, its row starts, the delay-group ends,
+ * the per-source delay masks, and the reverse matrix of plastic synapses
+ * (row starts, sources, forward indices, weights); out[8] is the number of
+ * delay groups and out[9] is 1 when the device built it.  Two simulations
+ * with equal out[0..8] hold the same bytes. */
+NEMO_B200_API nemo_status_t nemo_b200_connectivity_digest(nemo_simulation_t, uint64_t out[10]);
 /* Statistics of the last nemo_b200_run: its device time in ms (CUDA events
  * on the simulation's stream), and per kernel kind (0 = update kernel and
  * 1 = deliver kernel of the two-launch step, 2 = applyStdp, 3 = persistent

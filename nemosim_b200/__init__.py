@@ -127,6 +127,11 @@ class Configuration:
     def set_write_only_synapses(self):
         _check(lib().nemo_set_write_only_synapses(self._h))
 
+    def set_device_construction(self, on: bool = True):
+        """Build the connectivity on the device where the network allows it
+        (an extension; the default) or always on the host."""
+        _check(lib().nemo_b200_set_device_construction(self._h, int(bool(on))))
+
     def backend_description(self) -> str:
         d = C.c_char_p()
         _check(lib().nemo_backend_description(self._h, C.byref(d)))
@@ -414,6 +419,14 @@ class Simulation:
         ctas = C.c_uint()
         _check(lib().nemo_b200_trace_phases(self._h, steps, out, cap, C.byref(ctas)))
         return out[: steps * ctas.value * 5].reshape(steps, ctas.value, 5)
+
+    def connectivity_digest(self):
+        """(digests of the device connectivity and its delay-group count,
+        built on the device) -- an extension; equal digests mean equal
+        bytes."""
+        out = np.zeros(10, np.uint64)
+        _check(lib().nemo_b200_connectivity_digest(self._h, out))
+        return [int(v) for v in out[:9]], bool(out[9])
 
     def set_wait_limit(self, polls: int):
         """Polls of each grid-barrier or request wait before it gives up and

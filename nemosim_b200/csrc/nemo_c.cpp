@@ -643,6 +643,19 @@ nemo_status_t nemo_b200_set_wait_limit(nemo_simulation_t s, unsigned polls)
 	CALL(S(s).setWaitLimit(polls));
 }
 
+nemo_status_t nemo_b200_set_device_construction(nemo_configuration_t c, int on)
+{
+	NULLCHECK(c);
+	CALL(c->conf.deviceConstruction = on != 0);
+}
+
+nemo_status_t nemo_b200_connectivity_digest(nemo_simulation_t s, uint64_t out[10])
+{
+	NULLCHECK(s);
+	NULLCHECK(out);
+	CALL(S(s).connectivityDigest(out));
+}
+
 nemo_status_t nemo_b200_run_stats(nemo_simulation_t s, float* runMs, float kernelMs[4], unsigned launches[4],
 		uint64_t* fired, uint64_t* events, uint64_t* stdpEntries, uint64_t* plastic)
 {

@@ -72,6 +72,8 @@ struct Configuration {
 	std::vector<float> prefire, postfire;
 	float minE = 0, maxE = 0, minI = 0, maxI = 0;
 	bool writeOnlySynapses = false;
+	// build the connectivity on the device where the network allows it
+	bool deviceConstruction = true;
 	bool logging = false;
 	backend_t backend = NEMO_BACKEND_CUDA;
 	int device = -1;

@@ -10,6 +10,7 @@
 #include "kernels.cuh"
 #include "hugevec.hpp"
 #include "libm_calib.hpp"
+#include "construction.hpp"
 #include "plugins.hpp"
 
 namespace nemo_b200 {
@@ -1505,176 +1506,215 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	}
 	S.ntypes = (uint32_t) m_types.size();
 
-	// synapses of all networks, each mapped through its own network's ids
+	// synapses: the forward matrix, its delay groups and, with STDP, the
+	// reverse matrix of plastic synapses, built on the device where the
+	// network allows it and on the host otherwise (both give the same bytes)
 	size_t Sn = 0;
 	for(const Network* np : nets) Sn += np->src.size();
 	m_nsyn = Sn;
-	hvector<unsigned> lsrc(Sn), ltgt(Sn), sdelay(Sn);
-	hvector<int32_t> fxw(Sn);
-	hvector<uint8_t> splastic(Sn);
-	{
-		size_t k = 0;
-		for(size_t i = 0; i < nets.size(); ++i) {
-			const Network& net = *nets[i];
-			const auto& g2l = m_g2l[i];
-			for(size_t q = 0; q < net.src.size(); ++q, ++k) {
-				auto is = g2l.find(net.src[q]);
-				if(is == g2l.end()) NB_THROW(NEMO_INVALID_INPUT, "Non-existing neuron index %u", net.src[q]);
-				auto it = g2l.find(net.tgt[q]);
-				if(it == g2l.end()) NB_THROW(NEMO_INVALID_INPUT, "Non-existing neuron index %u", net.tgt[q]);
-				lsrc[k] = is->second;
-				ltgt[k] = it->second;
-				fxw[k] = fx_toFix(net.weight[q]);
-				sdelay[k] = net.delay[q];
-				splastic[k] = net.plastic[q];
-			}
-		}
-	}
-
-	// the reverse matrix of all synapses, for a type that reads its sources
-	// (construction/RCM.cpp:58-99 and 150-172 with STDP off); it cannot
-	// coexist with STDP's (:90-98)
-	{
-		bool needAll = false;
-		for(const HostType& t : m_types) {
-			needAll |= t.desc.rcmSources || t.desc.rcmDelays || t.desc.rcmForward || t.desc.rcmWeights;
-		}
-		if(needAll && conf.stdp) {
-			NB_THROW(NEMO_API_UNSUPPORTED, "The current version does not support a mix of STDP with neuron types "
-					"which require reverse connectivity for other purposes");
-		}
-		std::vector<unsigned long long> allPtr(N + 1, 0);
-		if(needAll) {
-			for(size_t k = 0; k < Sn; ++k) allPtr[ltgt[k] + 1]++;
-			for(unsigned t = 0; t < N; ++t) allPtr[t + 1] += allPtr[t];
-			hvector<uint32_t> asrc(Sn);
-			hvector<float> aw(Sn);
-			std::vector<unsigned long long> fill(allPtr.begin(), allPtr.end() - 1);
-			size_t k = 0;
-			for(const Network* np : nets) {
-				for(size_t q = 0; q < np->src.size(); ++q, ++k) {
-					// a Kuramoto neuron reads its sources' phases from its own
-					// type's history of 32 steps
-					const HostType& tt = m_types[m_ltype[ltgt[k]]];
-					if(tt.desc.kind == KIND_KURAMOTO) {
-						if(m_ltype[lsrc[k]] != m_ltype[ltgt[k]]) {
-							NB_THROW(NEMO_INVALID_INPUT, "Synapse %u -> %u: a Kuramoto oscillator's sources must be "
-									"Kuramoto oscillators", np->src[q], np->tgt[q]);
-						}
-						if(sdelay[k] > 31) {
-							NB_THROW(NEMO_INVALID_INPUT, "Synapse %u -> %u: delay %u beyond the 31 steps of phase "
-									"history a Kuramoto oscillator reads", np->src[q], np->tgt[q], sdelay[k]);
-						}
-					}
-					const unsigned long long p = fill[ltgt[k]]++;
-					asrc[p] = lsrc[k] | ((sdelay[k] - 1) << 26);
-					aw[p] = np->weight[q];
-				}
-			}
-			auto* dSrc = dalloc<uint32_t>(Sn);
-			auto* dW = dalloc<float>(Sn);
-			NB_CUDA(cudaMemcpyAsync(dSrc, asrc.data(), Sn * 4, cudaMemcpyHostToDevice, m_stream));
-			NB_CUDA(cudaMemcpyAsync(dW, aw.data(), Sn * 4, cudaMemcpyHostToDevice, m_stream));
-			S.allSrc = dSrc;
-			S.allW = dW;
-		}
-		auto* dPtr = dalloc<unsigned long long>(N + 1);
-		NB_CUDA(cudaMemcpyAsync(dPtr, allPtr.data(), (N + 1) * 8, cudaMemcpyHostToDevice, m_stream));
-		S.allPtr = dPtr;
-		NB_CUDA(cudaStreamSynchronize(m_stream));
-	}
-
-	// forward matrix (src/nemo/ConnectivityMatrix.cpp:65-162): outgoing
-	// synapses per local source, sorted by delay, insertion order within a
-	// delay -- the reference's row order
 	const unsigned D = std::max(1u, m_maxDelay);
-	std::vector<unsigned long long> outPtr(N + 1);
-	hvector<uint64_t> pos(Sn);
+	S.dStride = D;
 	// deliverSpikes' validSpikes = ~(~0 << maxDelay) with x86 shift
 	// semantics (src/nemo/cpu/Simulation.cpp:263): nothing is delivered when
 	// the maximum delay is 0 or 64
 	const bool deliver = m_maxDelay >= 1 && m_maxDelay <= 63;
-	std::vector<uint64_t> delayMask(N, 0);
+	std::vector<unsigned long long> outPtr(N + 1), rcmPtr(N + 1, 0);
 	uint64_t dlvGroups = 0;  // delay groups of all sources (all pending at once, at most)
-	{
-		hvector<uint64_t> rowStart((size_t) N * D + 1, 0);
-		for(size_t k = 0; k < Sn; ++k) rowStart[(size_t) lsrc[k] * D + sdelay[k]]++;
-		for(size_t r = 0; r < (size_t) N * D; ++r) rowStart[r + 1] += rowStart[r];
-		for(unsigned s = 0; s <= N; ++s) outPtr[s] = rowStart[(size_t) s * D];
-		m_outDegree.resize(N);
-		for(unsigned s = 0; s < N; ++s) {
-			m_outDegree[s] = (uint32_t) (outPtr[s + 1] - outPtr[s]);
-			m_maxOutDeg = std::max(m_maxOutDeg, m_outDegree[s]);
-		}
-		// delay groups: the end of each source's delay-d group within its row
-		const bool narrow = m_maxOutDeg < 65536;
-		hvector<uint16_t> end16(narrow ? (size_t) N * D : 0);
-		hvector<uint32_t> end32(narrow ? 0 : (size_t) N * D);
-		for(unsigned s = 0; s < N; ++s) {
-			const uint64_t base = rowStart[(size_t) s * D];
-			uint64_t prev = 0;
-			for(unsigned d = 1; d <= D; ++d) {
-				const uint64_t e = rowStart[(size_t) s * D + d] - base;
-				if(narrow) end16[(size_t) s * D + d - 1] = (uint16_t) e;
-				else end32[(size_t) s * D + d - 1] = (uint32_t) e;
-				if(deliver && e > prev) {
-					delayMask[s] |= 1ull << (d - 1);
-					++dlvGroups;
+	bool needAll = false;  // a type reads the reverse matrix of all synapses
+	for(const HostType& t : m_types) {
+		needAll |= t.desc.rcmSources || t.desc.rcmDelays || t.desc.rcmForward || t.desc.rcmWeights;
+	}
+	S.stdp = conf.stdp ? 1 : 0;
+
+	std::vector<uint32_t> g2lDense;
+	if(conf.deviceConstruction && !batch && !needAll && Sn < (1ull << 31) - 1 && (uint64_t) N * D < (1ull << 31) - 1 &&
+			denseIds(g2lDense)) {
+		buildOnDevice(*nets[0], g2lDense, deliver, outPtr, rcmPtr, dlvGroups);
+	} else {
+		// synapses of all networks, each mapped through its own network's ids
+		hvector<unsigned> lsrc(Sn), ltgt(Sn), sdelay(Sn);
+		hvector<int32_t> fxw(Sn);
+		hvector<uint8_t> splastic(Sn);
+		{
+			size_t k = 0;
+			for(size_t i = 0; i < nets.size(); ++i) {
+				const Network& net = *nets[i];
+				const auto& g2l = m_g2l[i];
+				for(size_t q = 0; q < net.src.size(); ++q, ++k) {
+					auto is = g2l.find(net.src[q]);
+					if(is == g2l.end()) NB_THROW(NEMO_INVALID_INPUT, "Non-existing neuron index %u", net.src[q]);
+					auto it = g2l.find(net.tgt[q]);
+					if(it == g2l.end()) NB_THROW(NEMO_INVALID_INPUT, "Non-existing neuron index %u", net.tgt[q]);
+					lsrc[k] = is->second;
+					ltgt[k] = it->second;
+					fxw[k] = fx_toFix(net.weight[q]);
+					sdelay[k] = net.delay[q];
+					splastic[k] = net.plastic[q];
 				}
-				prev = e;
 			}
 		}
-		S.dStride = D;
-		if(narrow) {
-			auto* p = dalloc<uint16_t>(end16.size());
-			NB_CUDA(cudaMemcpyAsync(p, end16.data(), end16.size() * 2, cudaMemcpyHostToDevice, m_stream));
-			S.dEnd16 = p;
-			S.dEnd32 = nullptr;
-		} else {
-			auto* p = dalloc<uint32_t>(end32.size());
-			NB_CUDA(cudaMemcpyAsync(p, end32.data(), end32.size() * 4, cudaMemcpyHostToDevice, m_stream));
-			S.dEnd16 = nullptr;
-			S.dEnd32 = p;
-		}
-		auto* dm = dalloc<uint64_t>(N);
-		NB_CUDA(cudaMemcpyAsync(dm, delayMask.data(), (size_t) N * 8, cudaMemcpyHostToDevice, m_stream));
-		S.delayMask = dm;
-		NB_CUDA(cudaStreamSynchronize(m_stream)); // the host tables go out of scope
-		for(size_t k = 0; k < Sn; ++k) pos[k] = rowStart[(size_t) lsrc[k] * D + sdelay[k] - 1]++;
-	}
-	{
-		hvector<uint2> syn(Sn);
-		for(size_t k = 0; k < Sn; ++k) {
-			syn[pos[k]] = make_uint2(ltgt[k] | ((sdelay[k] - 1) << 26), (uint32_t) fxw[k]);
-		}
-		auto* dOut = dalloc<unsigned long long>(N + 1);
-		auto* dSyn = dalloc<uint2>(Sn);
-		NB_CUDA(cudaMemcpyAsync(dOut, outPtr.data(), (N + 1) * 8, cudaMemcpyHostToDevice, m_stream));
-		NB_CUDA(cudaMemcpyAsync(dSyn, syn.data(), Sn * 8, cudaMemcpyHostToDevice, m_stream));
-		S.outPtr = dOut;
-		S.syn = dSyn;
-		NB_CUDA(cudaStreamSynchronize(m_stream));
-	}
 
-	// query tables of one network: per local source, its synapses by
-	// per-source index
-	if(!m_writeOnly) {
-		const Network& net = *nets[0];
-		m_srcStart.assign(N + 1, 0);
-		for(size_t k = 0; k < Sn; ++k) m_srcStart[lsrc[k] + 1]++;
-		for(unsigned s = 0; s < N; ++s) m_srcStart[s + 1] += m_srcStart[s];
-		m_srcOrder.resize(Sn);
-		for(size_t k = 0; k < Sn; ++k) m_srcOrder[m_srcStart[lsrc[k]] + net.sid[k]] = k;
-		m_pos.assign(pos.begin(), pos.end());
-		m_synDelay.assign(net.delay.begin(), net.delay.end());
-		m_synPlastic.assign(net.plastic.begin(), net.plastic.end());
-		m_synTarget.assign(net.tgt.begin(), net.tgt.end());
-	}
+		// the reverse matrix of all synapses, for a type that reads its sources
+		// (construction/RCM.cpp:58-99 and 150-172 with STDP off); it cannot
+		// coexist with STDP's (:90-98)
+		{
+			if(needAll && conf.stdp) {
+				NB_THROW(NEMO_API_UNSUPPORTED, "The current version does not support a mix of STDP with neuron types "
+						"which require reverse connectivity for other purposes");
+			}
+			std::vector<unsigned long long> allPtr(N + 1, 0);
+			if(needAll) {
+				for(size_t k = 0; k < Sn; ++k) allPtr[ltgt[k] + 1]++;
+				for(unsigned t = 0; t < N; ++t) allPtr[t + 1] += allPtr[t];
+				hvector<uint32_t> asrc(Sn);
+				hvector<float> aw(Sn);
+				std::vector<unsigned long long> fill(allPtr.begin(), allPtr.end() - 1);
+				size_t k = 0;
+				for(const Network* np : nets) {
+					for(size_t q = 0; q < np->src.size(); ++q, ++k) {
+						// a Kuramoto neuron reads its sources' phases from its own
+						// type's history of 32 steps
+						const HostType& tt = m_types[m_ltype[ltgt[k]]];
+						if(tt.desc.kind == KIND_KURAMOTO) {
+							if(m_ltype[lsrc[k]] != m_ltype[ltgt[k]]) {
+								NB_THROW(NEMO_INVALID_INPUT, "Synapse %u -> %u: a Kuramoto oscillator's sources must be "
+										"Kuramoto oscillators", np->src[q], np->tgt[q]);
+							}
+							if(sdelay[k] > 31) {
+								NB_THROW(NEMO_INVALID_INPUT, "Synapse %u -> %u: delay %u beyond the 31 steps of phase "
+										"history a Kuramoto oscillator reads", np->src[q], np->tgt[q], sdelay[k]);
+							}
+						}
+						const unsigned long long p = fill[ltgt[k]]++;
+						asrc[p] = lsrc[k] | ((sdelay[k] - 1) << 26);
+						aw[p] = np->weight[q];
+					}
+				}
+				auto* dSrc = dalloc<uint32_t>(Sn);
+				auto* dW = dalloc<float>(Sn);
+				NB_CUDA(cudaMemcpyAsync(dSrc, asrc.data(), Sn * 4, cudaMemcpyHostToDevice, m_stream));
+				NB_CUDA(cudaMemcpyAsync(dW, aw.data(), Sn * 4, cudaMemcpyHostToDevice, m_stream));
+				S.allSrc = dSrc;
+				S.allW = dW;
+			}
+			auto* dPtr = dalloc<unsigned long long>(N + 1);
+			NB_CUDA(cudaMemcpyAsync(dPtr, allPtr.data(), (N + 1) * 8, cudaMemcpyHostToDevice, m_stream));
+			S.allPtr = dPtr;
+			NB_CUDA(cudaStreamSynchronize(m_stream));
+		}
 
-	// STDP (src/nemo/StdpProcess.cpp:20-46) and the reverse matrix of plastic
-	// synapses (src/nemo/construction/RCM.cpp:150-172)
-	S.stdp = conf.stdp ? 1 : 0;
-	std::vector<unsigned long long> rcmPtr(N + 1, 0);
+		// forward matrix (src/nemo/ConnectivityMatrix.cpp:65-162): outgoing
+		// synapses per local source, sorted by delay, insertion order within a
+		// delay -- the reference's row order
+		hvector<uint64_t> pos(Sn);
+		std::vector<uint64_t> delayMask(N, 0);
+		{
+			hvector<uint64_t> rowStart((size_t) N * D + 1, 0);
+			for(size_t k = 0; k < Sn; ++k) rowStart[(size_t) lsrc[k] * D + sdelay[k]]++;
+			for(size_t r = 0; r < (size_t) N * D; ++r) rowStart[r + 1] += rowStart[r];
+			for(unsigned s = 0; s <= N; ++s) outPtr[s] = rowStart[(size_t) s * D];
+			m_outDegree.resize(N);
+			for(unsigned s = 0; s < N; ++s) {
+				m_outDegree[s] = (uint32_t) (outPtr[s + 1] - outPtr[s]);
+				m_maxOutDeg = std::max(m_maxOutDeg, m_outDegree[s]);
+			}
+			// delay groups: the end of each source's delay-d group within its row
+			const bool narrow = m_maxOutDeg < 65536;
+			hvector<uint16_t> end16(narrow ? (size_t) N * D : 0);
+			hvector<uint32_t> end32(narrow ? 0 : (size_t) N * D);
+			for(unsigned s = 0; s < N; ++s) {
+				const uint64_t base = rowStart[(size_t) s * D];
+				uint64_t prev = 0;
+				for(unsigned d = 1; d <= D; ++d) {
+					const uint64_t e = rowStart[(size_t) s * D + d] - base;
+					if(narrow) end16[(size_t) s * D + d - 1] = (uint16_t) e;
+					else end32[(size_t) s * D + d - 1] = (uint32_t) e;
+					if(deliver && e > prev) {
+						delayMask[s] |= 1ull << (d - 1);
+						++dlvGroups;
+					}
+					prev = e;
+				}
+			}
+			if(narrow) {
+				auto* p = dalloc<uint16_t>(end16.size());
+				NB_CUDA(cudaMemcpyAsync(p, end16.data(), end16.size() * 2, cudaMemcpyHostToDevice, m_stream));
+				S.dEnd16 = p;
+				S.dEnd32 = nullptr;
+			} else {
+				auto* p = dalloc<uint32_t>(end32.size());
+				NB_CUDA(cudaMemcpyAsync(p, end32.data(), end32.size() * 4, cudaMemcpyHostToDevice, m_stream));
+				S.dEnd16 = nullptr;
+				S.dEnd32 = p;
+			}
+			auto* dm = dalloc<uint64_t>(N);
+			NB_CUDA(cudaMemcpyAsync(dm, delayMask.data(), (size_t) N * 8, cudaMemcpyHostToDevice, m_stream));
+			S.delayMask = dm;
+			NB_CUDA(cudaStreamSynchronize(m_stream)); // the host tables go out of scope
+			for(size_t k = 0; k < Sn; ++k) pos[k] = rowStart[(size_t) lsrc[k] * D + sdelay[k] - 1]++;
+		}
+		{
+			hvector<uint2> syn(Sn);
+			for(size_t k = 0; k < Sn; ++k) {
+				syn[pos[k]] = make_uint2(ltgt[k] | ((sdelay[k] - 1) << 26), (uint32_t) fxw[k]);
+			}
+			auto* dOut = dalloc<unsigned long long>(N + 1);
+			auto* dSyn = dalloc<uint2>(Sn);
+			NB_CUDA(cudaMemcpyAsync(dOut, outPtr.data(), (N + 1) * 8, cudaMemcpyHostToDevice, m_stream));
+			NB_CUDA(cudaMemcpyAsync(dSyn, syn.data(), Sn * 8, cudaMemcpyHostToDevice, m_stream));
+			S.outPtr = dOut;
+			S.syn = dSyn;
+			NB_CUDA(cudaStreamSynchronize(m_stream));
+		}
+
+		// query tables of one network: per local source, its synapses by
+		// per-source index
+		if(!m_writeOnly) {
+			const Network& net = *nets[0];
+			m_srcStart.assign(N + 1, 0);
+			for(size_t k = 0; k < Sn; ++k) m_srcStart[lsrc[k] + 1]++;
+			for(unsigned s = 0; s < N; ++s) m_srcStart[s + 1] += m_srcStart[s];
+			m_srcOrder.resize(Sn);
+			for(size_t k = 0; k < Sn; ++k) m_srcOrder[m_srcStart[lsrc[k]] + net.sid[k]] = k;
+			m_pos.assign(pos.begin(), pos.end());
+			m_synDelay.assign(net.delay.begin(), net.delay.end());
+			m_synPlastic.assign(net.plastic.begin(), net.plastic.end());
+			m_synTarget.assign(net.tgt.begin(), net.tgt.end());
+		}
+
+		// the reverse matrix of plastic synapses (src/nemo/construction/RCM.cpp:150-172)
+		if(conf.stdp) {
+			for(size_t k = 0; k < Sn; ++k) if(splastic[k]) rcmPtr[ltgt[k] + 1]++;
+			for(unsigned t = 0; t < N; ++t) {
+				m_maxPlasticInDeg = std::max(m_maxPlasticInDeg, (uint32_t) rcmPtr[t + 1]);
+				rcmPtr[t + 1] += rcmPtr[t];
+			}
+			size_t P = rcmPtr[N];
+			hvector<uint32_t> rsrc(P), rfwd(P);
+			hvector<int32_t> rw(P);
+			std::vector<unsigned long long> fill(rcmPtr.begin(), rcmPtr.end() - 1);
+			for(size_t k = 0; k < Sn; ++k) {
+				if(!splastic[k]) continue;
+				size_t p = fill[ltgt[k]]++;
+				rsrc[p] = lsrc[k] | ((sdelay[k] - 1) << 26);
+				if(pos[k] > 0xffffffffull) NB_THROW(NEMO_API_UNSUPPORTED, "too many synapses for STDP");
+				rfwd[p] = (uint32_t) pos[k];
+				rw[p] = fxw[k];
+			}
+			auto* dRsrc = dalloc<uint32_t>(P);
+			auto* dRfwd = dalloc<uint32_t>(P);
+			S.rcmAcc = dalloc<int32_t>(P);
+			S.rcmW = dalloc<int32_t>(P);
+			NB_CUDA(cudaMemcpyAsync(S.rcmW, rw.data(), P * 4, cudaMemcpyHostToDevice, m_stream));
+			NB_CUDA(cudaMemcpyAsync(dRsrc, rsrc.data(), P * 4, cudaMemcpyHostToDevice, m_stream));
+			NB_CUDA(cudaMemcpyAsync(dRfwd, rfwd.data(), P * 4, cudaMemcpyHostToDevice, m_stream));
+			S.rcmSrc = dRsrc;
+			S.rcmFwd = dRfwd;
+			lastPlastic = P;
+			NB_CUDA(cudaStreamSynchronize(m_stream));
+		}
+	}
+	// the STDP function (src/nemo/StdpProcess.cpp:20-46)
 	if(conf.stdp) {
 		StdpParams& sp = S.sp;
 		sp.npre = (uint32_t) conf.prefire.size();
@@ -1701,36 +1741,8 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 		sp.prePostBits = shl64(~shl64(~0ull, sp.npre), sp.npost);
 		sp.postPreBits = ~shl64(~0ull, sp.npost);
 		sp.postFireMask = shl64(1ull, sp.npost);
-
-		for(size_t k = 0; k < Sn; ++k) if(splastic[k]) rcmPtr[ltgt[k] + 1]++;
-		for(unsigned t = 0; t < N; ++t) {
-			m_maxPlasticInDeg = std::max(m_maxPlasticInDeg, (uint32_t) rcmPtr[t + 1]);
-			rcmPtr[t + 1] += rcmPtr[t];
-		}
-		size_t P = rcmPtr[N];
-		hvector<uint32_t> rsrc(P), rfwd(P);
-		hvector<int32_t> rw(P);
-		std::vector<unsigned long long> fill(rcmPtr.begin(), rcmPtr.end() - 1);
-		for(size_t k = 0; k < Sn; ++k) {
-			if(!splastic[k]) continue;
-			size_t p = fill[ltgt[k]]++;
-			rsrc[p] = lsrc[k] | ((sdelay[k] - 1) << 26);
-			if(pos[k] > 0xffffffffull) NB_THROW(NEMO_API_UNSUPPORTED, "too many synapses for STDP");
-			rfwd[p] = (uint32_t) pos[k];
-			rw[p] = fxw[k];
-		}
-		auto* dRsrc = dalloc<uint32_t>(P);
-		auto* dRfwd = dalloc<uint32_t>(P);
-		S.rcmAcc = dalloc<int32_t>(P);
-		S.rcmW = dalloc<int32_t>(P);
-		NB_CUDA(cudaMemcpyAsync(S.rcmW, rw.data(), P * 4, cudaMemcpyHostToDevice, m_stream));
-		NB_CUDA(cudaMemcpyAsync(dRsrc, rsrc.data(), P * 4, cudaMemcpyHostToDevice, m_stream));
-		NB_CUDA(cudaMemcpyAsync(dRfwd, rfwd.data(), P * 4, cudaMemcpyHostToDevice, m_stream));
-		S.rcmSrc = dRsrc;
-		S.rcmFwd = dRfwd;
-		lastPlastic = P;
-		NB_CUDA(cudaStreamSynchronize(m_stream));
 	}
+
 	auto* dRcmPtr = dalloc<unsigned long long>(N + 1);
 	NB_CUDA(cudaMemcpyAsync(dRcmPtr, rcmPtr.data(), (N + 1) * 8, cudaMemcpyHostToDevice, m_stream));
 	S.rcmPtr = dRcmPtr;
@@ -1748,6 +1760,7 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 			L.bucket = dalloc<uint32_t>(entries / BUCKET + 1);
 		};
 		makeList(S.dlvWork, dlvGroups, Sn);
+		m_dlvGroups = dlvGroups;
 		makeList(S.stdpWork, N, plastic);
 		uint64_t capA = 0;
 		for(unsigned n = 0; n < N; ++n) capA += (rcmPtr[n + 1] - rcmPtr[n] + CHUNK - 1) / CHUNK;
@@ -1847,6 +1860,7 @@ Simulation::~Simulation()
 {
 	cudaSetDevice(m_device);
 	stopServe();
+	freeKept();
 	if(m_stream) cudaStreamSynchronize(m_stream);
 	for(void* p : m_allocs) cudaFree(p);
 	if(m_graph) cudaGraphExecDestroy(m_graph);
@@ -2688,12 +2702,140 @@ void Simulation::setNeuronParameter(unsigned g, unsigned p, float v)
 	sync();
 }
 
+bool Simulation::denseIds(std::vector<uint32_t>& g2l) const
+{
+	uint32_t maxGid = 0;
+	for(unsigned g : m_l2g) maxGid = std::max(maxGid, g);
+	if((uint64_t) maxGid + 1 > 4ull * m_N + (1u << 20)) return false;
+	g2l.assign((size_t) maxGid + 1, ~0u);
+	for(unsigned l = 0; l < m_N; ++l) g2l[m_l2g[l]] = l;
+	return true;
+}
+
+// The device build of one network's connectivity (construction.cu): the
+// same forward matrix, delay groups and reverse matrix as the host build,
+// and the same errors, in the same order, for synapses between
+// non-existing neurons and weights outside the fixed-point range.
+void Simulation::buildOnDevice(const Network& net, const std::vector<uint32_t>& g2l, bool deliver,
+		std::vector<unsigned long long>& outPtr, std::vector<unsigned long long>& rcmPtr, uint64_t& dlvGroups)
+{
+	DevSim& S = m_dev;
+	const unsigned N = m_N;
+	DeviceConstruction c;
+	c.S = m_nsyn;
+	c.src = net.src.data();
+	c.tgt = net.tgt.data();
+	c.delay = net.delay.data();
+	c.weight = net.weight.data();
+	c.plastic = net.plastic.data();
+	c.g2l = g2l.data();
+	c.maxGid = (uint32_t) (g2l.size() - 1);
+	c.N = N;
+	c.D = S.dStride;
+	c.deliver = deliver;
+	c.stdp = S.stdp != 0;
+	c.keepQueries = !m_writeOnly;
+	try {
+		construct_on_device(c, m_stream, [this](size_t bytes) { return (void*) dalloc<uint8_t>(bytes); });
+	} catch(...) {
+		m_kept = KeptSynapses{ c.keptSrc, c.keptPos, c.keptTgt, c.keptDelay, c.keptPlastic };
+		freeKept();
+		throw;
+	}
+	m_kept = KeptSynapses{ c.keptSrc, c.keptPos, c.keptTgt, c.keptDelay, c.keptPlastic };
+	S.syn = c.syn;
+	S.outPtr = c.outPtr;
+	S.dEnd16 = c.dEnd16;
+	S.dEnd32 = c.dEnd32;
+	S.delayMask = c.delayMask;
+	S.allPtr = dalloc<unsigned long long>(N + 1);  // no reverse matrix of all synapses
+	outPtr = c.hostOutPtr;
+	m_outDegree.resize(N);
+	for(unsigned s = 0; s < N; ++s) {
+		m_outDegree[s] = (uint32_t) (outPtr[s + 1] - outPtr[s]);
+		m_maxOutDeg = std::max(m_maxOutDeg, m_outDegree[s]);
+	}
+	dlvGroups = c.dlvGroups;
+	if(c.stdp) {
+		rcmPtr = c.hostRcmPtr;
+		for(unsigned t = 0; t < N; ++t) {
+			m_maxPlasticInDeg = std::max(m_maxPlasticInDeg, (uint32_t) (rcmPtr[t + 1] - rcmPtr[t]));
+		}
+		S.rcmSrc = c.rcmSrc;
+		S.rcmFwd = c.rcmFwd;
+		S.rcmW = c.rcmW;
+		S.rcmAcc = dalloc<int32_t>(c.plastic_count);
+		lastPlastic = c.plastic_count;
+	}
+	m_builtOnDevice = true;
+	NB_CUDA(cudaStreamSynchronize(m_stream));
+}
+
+void Simulation::freeKept() noexcept
+{
+	cudaFree(m_kept.src);
+	cudaFree(m_kept.pos);
+	cudaFree(m_kept.tgt);
+	cudaFree(m_kept.delay);
+	cudaFree(m_kept.plastic);
+	m_kept = KeptSynapses{};
+}
+
+// The query tables of a device-built network, from the arrays it kept: a
+// synapse's per-source index is its rank among its source's synapses in
+// insertion order (Network::addSynapses), so a stable counting sort by
+// source gives each source's synapses in per-source-index order.
+void Simulation::ensureQueryTables()
+{
+	if(!m_kept.src) return;
+	const size_t Sn = m_nsyn;
+	NB_CUDA(cudaSetDevice(m_device));
+	hvector<uint32_t> src(Sn), pos(Sn), tgt(Sn);
+	hvector<uint8_t> delay(Sn), plastic(Sn);
+	NB_CUDA(cudaMemcpyAsync(src.data(), m_kept.src, Sn * 4, cudaMemcpyDeviceToHost, m_stream));
+	NB_CUDA(cudaMemcpyAsync(pos.data(), m_kept.pos, Sn * 4, cudaMemcpyDeviceToHost, m_stream));
+	NB_CUDA(cudaMemcpyAsync(tgt.data(), m_kept.tgt, Sn * 4, cudaMemcpyDeviceToHost, m_stream));
+	NB_CUDA(cudaMemcpyAsync(delay.data(), m_kept.delay, Sn, cudaMemcpyDeviceToHost, m_stream));
+	NB_CUDA(cudaMemcpyAsync(plastic.data(), m_kept.plastic, Sn, cudaMemcpyDeviceToHost, m_stream));
+	sync();
+	m_srcStart.assign(m_N + 1, 0);
+	for(size_t k = 0; k < Sn; ++k) m_srcStart[src[k] + 1]++;
+	for(unsigned s = 0; s < m_N; ++s) m_srcStart[s + 1] += m_srcStart[s];
+	std::vector<uint64_t> fill(m_srcStart.begin(), m_srcStart.end() - 1);
+	m_srcOrder.resize(Sn);
+	for(size_t k = 0; k < Sn; ++k) m_srcOrder[fill[src[k]]++] = k;
+	m_pos.assign(pos.begin(), pos.end());
+	m_synDelay.assign(delay.begin(), delay.end());
+	m_synPlastic.assign(plastic.begin(), plastic.end());
+	m_synTarget.assign(tgt.begin(), tgt.end());
+	freeKept();
+}
+
+void Simulation::connectivityDigest(uint64_t out[DIGESTS])
+{
+	NB_CUDA(cudaSetDevice(m_device));
+	const DevSim& S = m_dev;
+	const size_t N = m_N, P = lastPlastic;
+	const size_t rows = N * S.dStride;
+	out[0] = device_digest(S.syn, m_nsyn * 8, m_stream);
+	out[1] = device_digest(S.outPtr, (N + 1) * 8, m_stream);
+	out[2] = S.dEnd16 ? device_digest(S.dEnd16, rows * 2, m_stream) : device_digest(S.dEnd32, rows * 4, m_stream) ^ 1;
+	out[3] = device_digest(S.delayMask, N * 8, m_stream);
+	out[4] = device_digest(S.rcmPtr, (N + 1) * 8, m_stream);
+	out[5] = S.stdp ? device_digest(S.rcmSrc, P * 4, m_stream) : 0;
+	out[6] = S.stdp ? device_digest(S.rcmFwd, P * 4, m_stream) : 0;
+	out[7] = S.stdp ? device_digest(S.rcmW, P * 4, m_stream) : 0;
+	out[8] = m_dlvGroups;
+	out[9] = m_builtOnDevice ? 1 : 0;
+}
+
 /* src/nemo/ConnectivityMatrix.cpp:298-331 */
 const std::vector<uint64_t>& Simulation::getSynapsesFrom(unsigned source)
 {
 	if(m_writeOnly) NB_THROW(NEMO_INVALID_INPUT, "Cannot read synapse state if simulation configured with write-only synapses");
 	auto it = m_g2l[0].find(source);
 	if(it == m_g2l[0].end()) NB_THROW(NEMO_INVALID_INPUT, "Non-existing source neuron id (%u) in synapse id query", source);
+	ensureQueryTables();
 	uint64_t n = m_srcStart[it->second + 1] - m_srcStart[it->second];
 	m_queried.resize(n);
 	for(uint64_t i = 0; i < n; ++i) m_queried[i] = ((uint64_t) source << 32) | i;
@@ -2701,9 +2843,10 @@ const std::vector<uint64_t>& Simulation::getSynapsesFrom(unsigned source)
 }
 
 /* ConnectivityMatrix::axonTerminalAux (src/nemo/ConnectivityMatrix.cpp:343-360) */
-size_t Simulation::synapseKey(uint64_t id) const
+size_t Simulation::synapseKey(uint64_t id)
 {
 	if(m_writeOnly) NB_THROW(NEMO_INVALID_INPUT, "Cannot read synapse state if simulation configured with write-only synapses");
+	ensureQueryTables();
 	unsigned source = (unsigned) (id >> 32);
 	uint32_t s = (uint32_t) (id & 0xffffffffu);
 	auto it = m_g2l[0].find(source);
@@ -2733,6 +2876,7 @@ void Simulation::getWeightsFx(int32_t* out, size_t cap, size_t* len)
 {
 	if(m_writeOnly) NB_THROW(NEMO_INVALID_INPUT, "Cannot read synapse state if simulation configured with write-only synapses");
 	if(cap < m_nsyn) NB_THROW(NEMO_BUFFER_OVERFLOW, "weight buffer too small");
+	ensureQueryTables();
 	std::vector<uint2> syn(m_nsyn);
 	NB_CUDA(cudaSetDevice(m_device));
 	NB_CUDA(cudaMemcpyAsync(syn.data(), m_dev.syn, m_nsyn * 8, cudaMemcpyDeviceToHost, m_stream));

@@ -244,6 +244,11 @@ public:
 	// accumulation, as in run()) with the phase trace on: out receives
 	// steps x CTAs x TRACE_MARKS %globaltimer values (ns); returns the CTAs
 	unsigned tracePhases(unsigned steps, uint64_t* out, size_t cap);
+	// digests of the device connectivity (forward matrix, delay-group ends,
+	// delay masks, reverse matrix of plastic synapses), its delay-group
+	// count, and whether it was built on the device
+	enum { DIGESTS = 10 };
+	void connectivityDigest(uint64_t out[DIGESTS]);
 	uint64_t stepEvents = 0;  // synaptic events of all step() calls so far
 
 private:
@@ -259,7 +264,29 @@ private:
 	unsigned localIdx(unsigned g) const;
 	bool findLocal(unsigned g, unsigned* l) const;  // localIdx without throwing (one network)
 	void locate(unsigned g, const HostType** t, unsigned* i) const;
-	size_t synapseKey(uint64_t id) const;
+	size_t synapseKey(uint64_t id);
+	// the connectivity built on the device (one network whose global ids
+	// fit a dense table of at most 4 entries per neuron plus 2^20, fewer
+	// than 2^31 - 1 synapses and delay-group rows, no reverse matrix of all
+	// synapses)
+	bool denseIds(std::vector<uint32_t>& g2l) const;
+	void buildOnDevice(const Network& net, const std::vector<uint32_t>& g2l, bool deliver,
+			std::vector<unsigned long long>& outPtr, std::vector<unsigned long long>& rcmPtr, uint64_t& dlvGroups);
+	bool m_builtOnDevice = false;
+	uint64_t m_dlvGroups = 0;
+	// the device build keeps, per synapse in insertion order, its local
+	// source, position in the forward matrix, global target, delay and
+	// plasticity on the device until the first synapse query builds the
+	// host query tables from them
+	struct KeptSynapses {
+		uint32_t* src = nullptr;
+		uint32_t* pos = nullptr;
+		uint32_t* tgt = nullptr;
+		uint8_t* delay = nullptr;
+		uint8_t* plastic = nullptr;
+	} m_kept;
+	void ensureQueryTables();
+	void freeKept() noexcept;
 	void launchStep(bool fullRecord);
 	void launchSteps(unsigned n);
 	void launchRun(unsigned n, bool finalStdp = true, const uint32_t* stim = nullptr, uint32_t nf = 0, uint32_t ni = 0,
