@@ -101,7 +101,7 @@ def test_sparse_ids_fall_back_to_the_host_build():
 
 
 def test_mixed_types_interleaved_ids():
-    sd, sh = both(lambda: nets.mixed_network(nb), lambda: nets.standard_stdp(nb))
+    sd, sh = both(lambda: nets.mixed_network(nb)[0], lambda: nets.standard_stdp(nb))
     same_run(sd, sh, 300, 100)
 
 
