@@ -3,8 +3,9 @@
 // are mapped to local indices through a dense table; a stable radix sort by
 // (local source, delay) gives every synapse its place in the forward matrix
 // -- the host build's counting sort, which keeps insertion order within a
-// row -- and a stable radix sort of the plastic synapses by target gives
-// the reverse matrix in insertion order within a target.  The sorts are
+// row -- and a stable radix sort of the plastic synapses, taken in forward
+// order, by target gives the reverse matrix in forward order within a
+// target.  The sorts are
 // CUB's (construction is not the step loop).
 #include "construction.hpp"
 
@@ -46,6 +47,7 @@ struct Scratch {
 };
 
 constexpr unsigned THREADS = 256;
+constexpr uint32_t TARGET_MASK = (1u << 26) - 1;  // a forward entry's target bits
 
 unsigned blocks(size_t n)
 {
@@ -131,40 +133,40 @@ __global__ void groups_kernel(uint32_t N, uint32_t D, bool deliver, const uint32
 	}
 }
 
-__global__ void flag_kernel(size_t S, const uint8_t* plastic, uint32_t* flag)
+// flag[p]: forward entry p is plastic (sortedIdx[p] is its insertion index)
+__global__ void flag_kernel(size_t S, const uint32_t* sortedIdx, const uint8_t* plastic, uint32_t* flag)
 {
-	for(size_t k = blockIdx.x * (size_t) blockDim.x + threadIdx.x; k <= S; k += (size_t) gridDim.x * blockDim.x) {
-		flag[k] = k < S && plastic[k] ? 1u : 0u;
+	for(size_t p = blockIdx.x * (size_t) blockDim.x + threadIdx.x; p <= S; p += (size_t) gridDim.x * blockDim.x) {
+		flag[p] = p < S && plastic[sortedIdx[p]] ? 1u : 0u;
 	}
 }
 
-// the plastic synapses' indices in insertion order (at their exclusive-scan
+// the plastic forward entries in forward order (at their exclusive-scan
 // positions)
-__global__ void compact_kernel(size_t S, const uint8_t* plastic, const uint32_t* at, uint32_t* plk)
+__global__ void compact_kernel(size_t S, const uint32_t* flag, const uint32_t* at, uint32_t* plf)
 {
-	for(size_t k = blockIdx.x * (size_t) blockDim.x + threadIdx.x; k < S; k += (size_t) gridDim.x * blockDim.x) {
-		if(plastic[k]) plk[at[k]] = (uint32_t) k;
+	for(size_t p = blockIdx.x * (size_t) blockDim.x + threadIdx.x; p < S; p += (size_t) gridDim.x * blockDim.x) {
+		if(flag[p]) plf[at[p]] = (uint32_t) p;
 	}
 }
 
-__global__ void plastic_keys_kernel(size_t P, const uint32_t* plk, const uint32_t* lt, uint32_t* key2,
+__global__ void plastic_keys_kernel(size_t P, const uint32_t* plf, const uint2* syn, uint32_t* key2,
 		uint32_t* tgtCount)
 {
 	for(size_t q = blockIdx.x * (size_t) blockDim.x + threadIdx.x; q < P; q += (size_t) gridDim.x * blockDim.x) {
-		const uint32_t t = lt[plk[q]];
+		const uint32_t t = syn[plf[q]].x & TARGET_MASK;
 		key2[q] = t;
 		atomicAdd(tgtCount + t, 1u);
 	}
 }
 
-__global__ void fill_reverse_kernel(size_t P, const uint32_t* sortedPlk, const uint32_t* ls, const unsigned* delay,
-		const uint32_t* pos, const int32_t* fx, uint32_t* rsrc, uint32_t* rfwd, int32_t* rw)
+__global__ void fill_reverse_kernel(size_t P, const uint32_t* sortedPlf, const uint32_t* sortedIdx,
+		const uint32_t* ls, const uint2* syn, uint32_t* rsrc, uint32_t* rfwd)
 {
-	for(size_t p = blockIdx.x * (size_t) blockDim.x + threadIdx.x; p < P; p += (size_t) gridDim.x * blockDim.x) {
-		const uint32_t k = sortedPlk[p];
-		rsrc[p] = ls[k] | ((delay[k] - 1) << 26);
-		rfwd[p] = pos[k];
-		rw[p] = fx[k];
+	for(size_t q = blockIdx.x * (size_t) blockDim.x + threadIdx.x; q < P; q += (size_t) gridDim.x * blockDim.x) {
+		const uint32_t p = sortedPlf[q];
+		rsrc[q] = ls[sortedIdx[p]] | (syn[p].x & ~TARGET_MASK);
+		rfwd[q] = p;
 	}
 }
 
@@ -301,7 +303,7 @@ void construct_on_device(DeviceConstruction& c, cudaStream_t st, const std::func
 	if(c.stdp) {
 		uint32_t* flag = scratch.get<uint32_t>(S + 1);
 		uint32_t* at = scratch.get<uint32_t>(S + 1);
-		flag_kernel<<<blocks(S + 1), THREADS, 0, st>>>(S, pl, flag);
+		flag_kernel<<<blocks(S + 1), THREADS, 0, st>>>(S, idxSorted, pl, flag);
 		CC_CUDA(cudaGetLastError());
 		tmpBytes = 0;
 		CC_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmpBytes, flag, at, (int) (S + 1), st));
@@ -312,13 +314,13 @@ void construct_on_device(DeviceConstruction& c, cudaStream_t st, const std::func
 		CC_CUDA(cudaStreamSynchronize(st));
 		const size_t P = hsel;
 		uint32_t* plk = scratch.get<uint32_t>(P);
-		compact_kernel<<<blocks(S), THREADS, 0, st>>>(S, pl, at, plk);
+		compact_kernel<<<blocks(S), THREADS, 0, st>>>(S, flag, at, plk);
 		CC_CUDA(cudaGetLastError());
 		uint32_t* key2 = scratch.get<uint32_t>(P);
 		uint32_t* tgtCount = scratch.get<uint32_t>((size_t) N + 1);
 		uint32_t* tgtStart = scratch.get<uint32_t>((size_t) N + 1);
 		CC_CUDA(cudaMemsetAsync(tgtCount, 0, ((size_t) N + 1) * 4, st));
-		plastic_keys_kernel<<<blocks(P), THREADS, 0, st>>>(P, plk, lt, key2, tgtCount);
+		plastic_keys_kernel<<<blocks(P), THREADS, 0, st>>>(P, plk, c.syn, key2, tgtCount);
 		CC_CUDA(cudaGetLastError());
 		tmpBytes = 0;
 		CC_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmpBytes, tgtCount, tgtStart, (int) N + 1, st));
@@ -336,8 +338,7 @@ void construct_on_device(DeviceConstruction& c, cudaStream_t st, const std::func
 				st));
 		c.rcmSrc = static_cast<uint32_t*>(alloc(P * 4));
 		c.rcmFwd = static_cast<uint32_t*>(alloc(P * 4));
-		c.rcmW = static_cast<int32_t*>(alloc(P * 4));
-		fill_reverse_kernel<<<blocks(P), THREADS, 0, st>>>(P, plkSorted, ls, dly, pos, fx, c.rcmSrc, c.rcmFwd, c.rcmW);
+		fill_reverse_kernel<<<blocks(P), THREADS, 0, st>>>(P, plkSorted, idxSorted, ls, c.syn, c.rcmSrc, c.rcmFwd);
 		CC_CUDA(cudaGetLastError());
 		std::vector<uint32_t> hs((size_t) N + 1);
 		CC_CUDA(cudaMemcpyAsync(hs.data(), tgtStart, ((size_t) N + 1) * 4, cudaMemcpyDeviceToHost, st));

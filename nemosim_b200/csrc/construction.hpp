@@ -4,7 +4,7 @@
 // src/nemo/ConnectivityMatrix.cpp:65-162, and construction/RCM.cpp:109-172).
 // The result is byte for byte the host build's: rows keep the reference's
 // order (sources, then delays, insertion order within a delay), and the
-// reverse matrix keeps insertion order within a target.
+// reverse matrix holds each target's synapses in forward-matrix order.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -41,7 +41,6 @@ struct DeviceConstruction {
 	uint64_t* delayMask = nullptr;         // [N]
 	uint32_t* rcmSrc = nullptr;            // [P] source | (delay - 1) << 26
 	uint32_t* rcmFwd = nullptr;            // [P] index into syn
-	int32_t* rcmW = nullptr;               // [P] weight
 	// host copies of the row starts of both matrices ([N + 1] each)
 	std::vector<unsigned long long> hostOutPtr, hostRcmPtr;
 	uint64_t dlvGroups = 0;

@@ -45,11 +45,20 @@ namespace nemo_b200 {
 // loop (run_kernel), one cooperative launch for many steps.  The STDP
 // accumulation of the last step runs before applyStdp (flushStdp);
 // deliveries stay pending until the next step, so they read the weights
-// applyStdp leaves.  applyStdp itself works on chunks of at most CHUNK
-// synapses of the targets touched since its last call.
+// applyStdp leaves.  applyStdp itself walks the forward matrix one slice
+// at a time (below).
 
-constexpr uint32_t CHUNK = 128;  // entries per chunk: 4 per lane of a warp
-constexpr uint32_t ILP = CHUNK / 32;
+// applyStdp writes each changed weight into the forward matrix, at an index
+// scattered over all of it.  To keep those writes in L2, it processes the
+// forward matrix in slices of APPLY_SLICE_ENTRIES entries (16 MB): item
+// (slice k, 32 targets) covers the targets' incoming plastic synapses whose
+// forward index lies in slice k.  Each target's reverse-matrix entries are
+// sorted by forward index, so they form one run per slice, found in a
+// table built with the matrix; the items run slice-major, so the warps in
+// flight write into about three slices at a time.
+constexpr uint32_t APPLY_SLICE_ENTRIES = 2u << 20;
+constexpr uint32_t APPLY_MAX_SLICES = 64;
+constexpr uint32_t APPLY_ILP = 4;  // entries per lane per round
 
 // Chained launches (programmatic dependent launch): deliver_kernel and
 // update_kernel alternate on one stream, each launched while its
@@ -130,27 +139,6 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long x)
 #pragma unroll
 	for(int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
 	return x;
-}
-
-// Reserve nch chunk slots per lane in a global list (one atomic per warp);
-// returns this lane's first slot.
-__device__ __forceinline__ uint32_t reserve_chunks(uint32_t* counter, uint32_t nch)
-{
-	const uint32_t incl = warp_inclusive_scan(nch);
-	const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-	uint32_t base = 0;
-	if(total && (threadIdx.x & 31) == 31) base = atomicAdd(counter, total);
-	base = __shfl_sync(0xffffffffu, base, 31);
-	return base + incl - nch;
-}
-
-__device__ __forceinline__ void write_chunks(uint4* list, uint32_t pos, unsigned long long start,
-		uint32_t count, uint32_t nch, uint32_t tag)
-{
-	for(uint32_t j = 0; j < nch; ++j) {
-		const unsigned long long s = start + (unsigned long long) j * CHUNK;
-		list[pos + j] = make_uint4((uint32_t) s, (uint32_t) (s >> 32), min(CHUNK, count - j * CHUNK), tag);
-	}
 }
 
 constexpr uint32_t BUCKET = 32;  // entries per bucket of a work list
@@ -997,93 +985,122 @@ static const void* serve_kernel_for(uint32_t threads)
 			: (const void*) serve_kernel<RUN_THREADS, 1>;
 }
 
-// Turns the targets touched since the last applyStdp (a bit-vector) into
-// chunks of their incoming plastic synapses, and clears the bit-vector: one
-// thread per neuron, one reservation per warp.
+// Compacts the targets touched since the last applyStdp (a bit-vector) into
+// a list and clears the bit-vector: one warp per word, one atomic per warp.
 __global__ void __launch_bounds__(STEP_THREADS)
 collect_touched_kernel(const DevSim S)
 {
 	const uint32_t stride = gridDim.x * blockDim.x;
 	const uint32_t lane = threadIdx.x & 31;
-	const uint32_t end = S.W * 32;  // whole warps, so that all lanes take part in the reservation
+	const uint32_t end = S.W * 32;  // whole warps: n >> 5 is the warp's word
 	for(uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < end; n += stride) {
 		const uint32_t word = S.touchedBits[n >> 5];
-		const bool touched = n < S.N && ((word >> lane) & 1u);
-		unsigned long long rb = 0;
-		uint32_t len = 0;
-		if(touched) {
-			rb = S.rcmPtr[n];
-			len = (uint32_t) (S.rcmPtr[n + 1] - rb);
+		if(!word) continue;
+		uint32_t base = 0;
+		if(lane == 0) {
+			base = atomicAdd(S.touchedCount, (uint32_t) __popc(word));
+			S.touchedBits[n >> 5] = 0u;
 		}
-		const uint32_t nch = (len + CHUNK - 1) / CHUNK;
-		if(__any_sync(0xffffffffu, nch != 0)) {
-			const uint32_t pos = reserve_chunks(S.applyChunkCount, nch);
-			write_chunks(S.applyChunks, pos, rb, len, nch, n);
-		}
-		if(lane == 0 && word) S.touchedBits[n >> 5] = 0u;
+		base = __shfl_sync(0xffffffffu, base, 0);
+		if((word >> lane) & 1u) S.touchedList[base + __popc(word & ((1u << lane) - 1u))] = n;
 	}
 }
 
-// applyStdp (src/nemo/ConnectivityMatrix.cpp:241-294) over the targets
-// touched since the last call (their incoming plastic synapses are the only
-// ones with a nonzero accumulator).  One warp per chunk; d.w of an apply
-// chunk is its target.
-__global__ void __launch_bounds__(STEP_THREADS)
-apply_touched_kernel(const DevSim S, int32_t reward)
+// applyStdp (src/nemo/ConnectivityMatrix.cpp:241-294): w' =
+// updatedWeight(w, reward x acc) for every incoming plastic synapse of the
+// touched targets (the only ones whose accumulator can be nonzero), written
+// back to the forward matrix when it changed, and the accumulator cleared.
+// ALL: every target, whatever its accumulator -- the first call, which also
+// clamps weights that start outside their range.  Work items are (slice,
+// 32 targets), slice-major; a warp flattens its 32 runs with a scan and
+// finds each entry's run with a 5-step shuffle search.
+template<bool ALL>
+__global__ void __launch_bounds__(STEP_THREADS, 6)
+apply_kernel(const DevSim S, int32_t reward)
 {
-	const uint32_t nch = *S.applyChunkCount;
+	const uint32_t FULL = 0xffffffffu;
 	const uint32_t lane = threadIdx.x & 31;
+	const uint32_t nT = ALL ? S.N : *S.touchedCount;
+	const uint32_t batches = (nT + 31) >> 5;
+	const unsigned long long items = (unsigned long long) batches * S.applySlices;
 	const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-	for(uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nch; c += nw) {
-		const uint4 d = S.applyChunks[c];
-		const unsigned long long start = (unsigned long long) d.x | ((unsigned long long) d.y << 32);
-		const uint32_t len = d.z;
-		int32_t acc[ILP];
-		uint32_t fwd[ILP];
-		int32_t w[ILP];
-#pragma unroll
-		for(uint32_t j = 0; j < ILP; ++j) acc[j] = lane + 32 * j < len ? __ldcs(S.rcmAcc + start + lane + 32 * j) : 0;
-		// the old weight from the reverse-ordered copy (coalesced); only a
-		// changed weight is written to the forward matrix (scattered)
-#pragma unroll
-		for(uint32_t j = 0; j < ILP; ++j) {
-			if(acc[j]) {
-				fwd[j] = __ldcs(S.rcmFwd + start + lane + 32 * j);
-				w[j] = __ldcs(S.rcmW + start + lane + 32 * j);
-			}
+	for(unsigned long long i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < items; i += nw) {
+		const uint32_t k = (uint32_t) (i / batches);
+		const uint32_t j = (uint32_t) (i - (unsigned long long) k * batches) * 32 + lane;
+		unsigned long long lo = 0;
+		uint32_t len = 0;
+		if(j < nT) {
+			const uint32_t t = ALL ? j : S.touchedList[j];
+			const uint32_t* run = S.rcmSlice + (size_t) k * S.N + t;
+			const uint32_t a = run[0];
+			lo = S.rcmPtr[t] + a;
+			len = run[S.N] - a;
 		}
+		const uint32_t incl = warp_inclusive_scan(len);
+		const uint32_t total = __shfl_sync(FULL, incl, 31);
+		for(uint32_t off = 0; off < total; off += 32 * APPLY_ILP) {
+			unsigned long long e[APPLY_ILP];
+			int32_t acc[APPLY_ILP];
+			uint32_t fwd[APPLY_ILP];
+			bool live[APPLY_ILP];
 #pragma unroll
-		for(uint32_t j = 0; j < ILP; ++j) {
-			if(!acc[j]) continue;
-			const int32_t nw2 = stdp_updated_weight(S.sp, w[j], fx_mul_dev(reward, acc[j]));
-			if(nw2 != w[j]) {
-				S.rcmW[start + lane + 32 * j] = nw2;
-				S.syn[fwd[j]].y = (uint32_t) nw2;
+			for(uint32_t q = 0; q < APPLY_ILP; ++q) {
+				const uint32_t x = off + lane + 32 * q;
+				// the run holding flattened entry x: the first lane whose
+				// inclusive sum exceeds x
+				uint32_t r = 0;
+#pragma unroll
+				for(uint32_t step = 16; step; step >>= 1) {
+					if(__shfl_sync(FULL, incl, r + step - 1) <= x) r += step;
+				}
+				const uint32_t before = __shfl_sync(FULL, incl - len, r);
+				const unsigned long long rlo = __shfl_sync(FULL, lo, r);
+				e[q] = rlo + (x - before);
+				// the accumulator and the forward index load together
+				acc[q] = x < total ? __ldcs(S.rcmAcc + e[q]) : 0;
+				fwd[q] = x < total ? __ldcs(S.rcmFwd + e[q]) : 0u;
 			}
-			S.rcmAcc[start + lane + 32 * j] = 0;
+#pragma unroll
+			for(uint32_t q = 0; q < APPLY_ILP; ++q) live[q] = off + lane + 32 * q < total && (ALL || acc[q] != 0);
+			int32_t w[APPLY_ILP];
+#pragma unroll
+			for(uint32_t q = 0; q < APPLY_ILP; ++q) w[q] = live[q] ? (int32_t) S.syn[fwd[q]].y : 0;
+#pragma unroll
+			for(uint32_t q = 0; q < APPLY_ILP; ++q) {
+				if(!live[q]) continue;
+				const int32_t nw2 = stdp_updated_weight(S.sp, w[q], fx_mul_dev(reward, acc[q]));
+				if(nw2 != w[q]) S.syn[fwd[q]].y = (uint32_t) nw2;
+				if(acc[q]) S.rcmAcc[e[q]] = 0;
+			}
 		}
 	}
 }
 
-// applyStdp, first call: one warp per target over every incoming plastic
-// synapse, so that weights that start outside their clamp range are clamped
-// as in the reference.  Later calls use apply_touched_kernel.
-__global__ void __launch_bounds__(STEP_THREADS)
-apply_full_kernel(const DevSim S, int32_t reward)
+// The run table of applyStdp: rcmSlice[k][t] is the offset, within target
+// t's incoming plastic synapses (sorted by forward index), of the first one
+// whose forward index is at least k x sliceLen; row K is t's in-degree.
+// One warp per target, one lane per slice boundary (a binary search).
+__global__ void slice_table_kernel(uint32_t N, const unsigned long long* rcmPtr, const uint32_t* rcmFwd, uint32_t K,
+		uint32_t sliceLen, uint32_t* table)
 {
 	const uint32_t lane = threadIdx.x & 31;
-	const uint32_t warpsTotal = gridDim.x * (STEP_THREADS / 32);
-	for(uint32_t tgt = blockIdx.x * (STEP_THREADS / 32) + (threadIdx.x >> 5); tgt < S.N; tgt += warpsTotal) {
-		unsigned long long b = S.rcmPtr[tgt], e = S.rcmPtr[tgt + 1];
-		for(unsigned long long p = b + lane; p < e; p += 32) {
-			const int32_t acc = S.rcmAcc[p];
-			const int32_t w = S.rcmW[p];
-			const int32_t nw = stdp_updated_weight(S.sp, w, fx_mul_dev(reward, acc));
-			if(nw != w) {
-				S.rcmW[p] = nw;
-				S.syn[S.rcmFwd[p]].y = (uint32_t) nw;
+	const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+	for(uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < N; t += warps) {
+		const unsigned long long b = rcmPtr[t];
+		const uint32_t n = (uint32_t) (rcmPtr[t + 1] - b);
+		for(uint32_t k = lane; k <= K; k += 32) {
+			uint32_t v = n;
+			if(k < K) {
+				const unsigned long long bound = (unsigned long long) k * sliceLen;
+				uint32_t l = 0, h = n;
+				while(l < h) {
+					const uint32_t m = (l + h) >> 1;
+					if(rcmFwd[b + m] < bound) l = m + 1;
+					else h = m;
+				}
+				v = l;
 			}
-			if(acc) S.rcmAcc[p] = 0;
+			table[(size_t) k * N + t] = v;
 		}
 	}
 }
@@ -1682,30 +1699,29 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 			m_synTarget.assign(net.tgt.begin(), net.tgt.end());
 		}
 
-		// the reverse matrix of plastic synapses (src/nemo/construction/RCM.cpp:150-172)
+		// the reverse matrix of plastic synapses (src/nemo/construction/RCM.cpp:150-172),
+		// each target's synapses in forward-matrix order
 		if(conf.stdp) {
+			if(Sn > 0xffffffffull) NB_THROW(NEMO_API_UNSUPPORTED, "too many synapses for STDP");
 			for(size_t k = 0; k < Sn; ++k) if(splastic[k]) rcmPtr[ltgt[k] + 1]++;
 			for(unsigned t = 0; t < N; ++t) {
 				m_maxPlasticInDeg = std::max(m_maxPlasticInDeg, (uint32_t) rcmPtr[t + 1]);
 				rcmPtr[t + 1] += rcmPtr[t];
 			}
 			size_t P = rcmPtr[N];
-			hvector<uint32_t> rsrc(P), rfwd(P);
-			hvector<int32_t> rw(P);
+			hvector<uint32_t> rsrc(P), rfwd(P), kAt(Sn);
+			for(size_t k = 0; k < Sn; ++k) kAt[pos[k]] = (uint32_t) k;
 			std::vector<unsigned long long> fill(rcmPtr.begin(), rcmPtr.end() - 1);
-			for(size_t k = 0; k < Sn; ++k) {
+			for(size_t p = 0; p < Sn; ++p) {
+				const uint32_t k = kAt[p];
 				if(!splastic[k]) continue;
-				size_t p = fill[ltgt[k]]++;
-				rsrc[p] = lsrc[k] | ((sdelay[k] - 1) << 26);
-				if(pos[k] > 0xffffffffull) NB_THROW(NEMO_API_UNSUPPORTED, "too many synapses for STDP");
-				rfwd[p] = (uint32_t) pos[k];
-				rw[p] = fxw[k];
+				const size_t q = fill[ltgt[k]]++;
+				rsrc[q] = lsrc[k] | ((sdelay[k] - 1) << 26);
+				rfwd[q] = (uint32_t) p;
 			}
 			auto* dRsrc = dalloc<uint32_t>(P);
 			auto* dRfwd = dalloc<uint32_t>(P);
 			S.rcmAcc = dalloc<int32_t>(P);
-			S.rcmW = dalloc<int32_t>(P);
-			NB_CUDA(cudaMemcpyAsync(S.rcmW, rw.data(), P * 4, cudaMemcpyHostToDevice, m_stream));
 			NB_CUDA(cudaMemcpyAsync(dRsrc, rsrc.data(), P * 4, cudaMemcpyHostToDevice, m_stream));
 			NB_CUDA(cudaMemcpyAsync(dRfwd, rfwd.data(), P * 4, cudaMemcpyHostToDevice, m_stream));
 			S.rcmSrc = dRsrc;
@@ -1762,10 +1778,21 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 		makeList(S.dlvWork, dlvGroups, Sn);
 		m_dlvGroups = dlvGroups;
 		makeList(S.stdpWork, N, plastic);
-		uint64_t capA = 0;
-		for(unsigned n = 0; n < N; ++n) capA += (rcmPtr[n + 1] - rcmPtr[n] + CHUNK - 1) / CHUNK;
-		S.applyChunks = dalloc<uint4>(capA);
-		S.applyChunkCount = dalloc<uint32_t>(1);
+		S.touchedList = dalloc<uint32_t>(N);
+		S.touchedCount = dalloc<uint32_t>(1);
+	}
+	// applyStdp's slices of the forward matrix and each target's run in each
+	if(conf.stdp) {
+		const uint32_t K = (uint32_t) std::min<uint64_t>(APPLY_MAX_SLICES,
+				std::max<uint64_t>(1, (Sn + APPLY_SLICE_ENTRIES - 1) / APPLY_SLICE_ENTRIES));
+		S.applySlices = K;
+		S.sliceLen = (uint32_t) std::max<uint64_t>(1, (Sn + K - 1) / K);
+		auto* table = dalloc<uint32_t>((size_t) (K + 1) * N);
+		const unsigned grid = std::max(1u, std::min<unsigned>((N + 7) / 8, 148u * 16u));
+		slice_table_kernel<<<grid, 256, 0, m_stream>>>(N, S.rcmPtr, S.rcmFwd, K, S.sliceLen, table);
+		NB_CUDA(cudaGetLastError());
+		S.rcmSlice = table;
+		NB_CUDA(cudaStreamSynchronize(m_stream));
 	}
 
 	// per-neuron RNG, keyed by the network-local index
@@ -1826,7 +1853,13 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 		NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, deliver_kernel, STEP_THREADS, S.recentBytes));
 		m_deliverGrid = (unsigned) std::max(1, perSm) * (unsigned) m_sms;
 	}
-	m_applyGrid = (unsigned) m_sms * 8;
+	// applyStdp: as many CTAs as fit at once, so that the slice-major work
+	// order holds across the whole grid
+	{
+		int perSm = 0;
+		NB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, apply_kernel<false>, STEP_THREADS, 0));
+		m_applyGrid = (unsigned) std::max(1, perSm) * (unsigned) m_sms;
+	}
 	// default shape of the two-launch step (set while the persistent loop is
 	// not yet configured): two partitions per SM
 	{
@@ -2303,20 +2336,19 @@ void Simulation::applyStdpDevice(int32_t R)
 	const bool fullPassDone = m_weightsClamped;
 	timedBegin(K_APPLY);
 	if(!m_weightsClamped) {
-		unsigned grid = std::min<unsigned>((m_N + 7) / 8, (unsigned) m_sms * 8);
-		apply_full_kernel<<<grid, STEP_THREADS, 0, m_stream>>>(m_dev, R);
+		apply_kernel<true><<<m_applyGrid, STEP_THREADS, 0, m_stream>>>(m_dev, R);
 	} else {
 		const unsigned cgrid = std::max(1u, std::min<unsigned>((m_dev.W * 32 + STEP_THREADS - 1) / STEP_THREADS,
 				(unsigned) m_sms * 8));
 		collect_touched_kernel<<<cgrid, STEP_THREADS, 0, m_stream>>>(m_dev);
-		apply_touched_kernel<<<m_applyGrid, STEP_THREADS, 0, m_stream>>>(m_dev, R);
+		apply_kernel<false><<<m_applyGrid, STEP_THREADS, 0, m_stream>>>(m_dev, R);
 	}
 	timedEnd();
 	// updatedWeight's result always lies within the clamp range of its sign
 	// class, so after one full pass every plastic weight does, and only the
 	// synapses of touched targets can change
 	m_weightsClamped = true;
-	NB_CUDA(cudaMemsetAsync(m_dev.applyChunkCount, 0, 4, m_stream));
+	NB_CUDA(cudaMemsetAsync(m_dev.touchedCount, 0, 4, m_stream));
 	if(!fullPassDone) NB_CUDA(cudaMemsetAsync(m_dev.touchedBits, 0, (size_t) m_dev.W * 4, m_stream));
 }
 
@@ -2495,7 +2527,7 @@ float Simulation::autotune(unsigned trialSteps)
 		regions.emplace_back(L->count, 16);
 	}
 	if(m_dev.stdp) regions.emplace_back(m_dev.rcmAcc, (size_t) lastPlastic * 4);
-	regions.emplace_back(m_dev.applyChunkCount, 4);
+	regions.emplace_back(m_dev.touchedCount, 4);
 	regions.emplace_back(m_dev.touchedBits, (size_t) m_dev.W * 4);
 	std::vector<void*> backup;
 	for(auto& r : regions) {
@@ -2763,7 +2795,6 @@ void Simulation::buildOnDevice(const Network& net, const std::vector<uint32_t>& 
 		}
 		S.rcmSrc = c.rcmSrc;
 		S.rcmFwd = c.rcmFwd;
-		S.rcmW = c.rcmW;
 		S.rcmAcc = dalloc<int32_t>(c.plastic_count);
 		lastPlastic = c.plastic_count;
 	}
@@ -2824,7 +2855,7 @@ void Simulation::connectivityDigest(uint64_t out[DIGESTS])
 	out[4] = device_digest(S.rcmPtr, (N + 1) * 8, m_stream);
 	out[5] = S.stdp ? device_digest(S.rcmSrc, P * 4, m_stream) : 0;
 	out[6] = S.stdp ? device_digest(S.rcmFwd, P * 4, m_stream) : 0;
-	out[7] = S.stdp ? device_digest(S.rcmW, P * 4, m_stream) : 0;
+	out[7] = S.stdp ? device_digest(S.rcmSlice, (size_t) (S.applySlices + 1) * N * 4, m_stream) : 0;
 	out[8] = m_dlvGroups;
 	out[9] = m_builtOnDevice ? 1 : 0;
 }

@@ -126,11 +126,16 @@ struct DevSim {
 	unsigned long long* eventCount; // [R] synaptic events (out-degree of fired neurons)
 	unsigned long long* stdpCount;  // [R] incoming plastic synapses walked by STDP
 	int stdp;
+	// reverse matrix of plastic synapses: per target, sorted by forward index
 	const unsigned long long* rcmPtr; // [N+1] incoming plastic synapses per target
 	const uint32_t* rcmSrc;   // source | (delay - 1) << 26
 	const uint32_t* rcmFwd;   // index into syn
 	int32_t* rcmAcc;          // STDP accumulator per incoming plastic synapse
-	int32_t* rcmW;            // the plastic synapse's weight (equal to its syn entry's), in reverse order
+	// applyStdp's slices of the forward matrix: rcmSlice[k][t] is the offset
+	// within target t's entries of the first one whose forward index is at
+	// least k x sliceLen ([applySlices + 1][N]; the last row is the in-degree)
+	const uint32_t* rcmSlice;
+	uint32_t applySlices, sliceLen;
 	// reverse matrix of all synapses into the targets of a type that reads
 	// its sources (Kuramoto): per target, source | (delay - 1) << 26 and the
 	// weight as given
@@ -141,11 +146,9 @@ struct DevSim {
 	// groups arriving next step (ranges of syn) and the incoming plastic
 	// synapses of its STDP targets (ranges of the reverse matrix)
 	WorkList dlvWork, stdpWork;
-	// incoming plastic synapses of the targets touched since the last
-	// applyStdp: {start lo, start hi, length, target}
-	uint4* applyChunks;
-	uint32_t* applyChunkCount;
-	uint32_t* touchedBits;    // [W]
+	uint32_t* touchedBits;    // [W] STDP targets since the last applyStdp
+	uint32_t* touchedList;    // [N] applyStdp's compacted touched targets
+	uint32_t* touchedCount;
 	unsigned long long* cycleDev; // step counter read by kernels replayed from a CUDA graph
 	StdpParams sp;
 	LibmCalib calib;
@@ -321,7 +324,7 @@ private:
 	size_t decodeBatchStep(uint32_t r, unsigned step, unsigned* counts, unsigned* ids, size_t pos, size_t cap);
 	std::vector<std::vector<uint32_t>> m_batchScratch;
 	unsigned m_deliverGrid = 1184;  // CTAs of deliver_kernel
-	unsigned m_applyGrid = 1184;    // CTAs of apply_touched_kernel
+	unsigned m_applyGrid = 1184;    // CTAs of apply_kernel
 	uint32_t m_P = 256, m_T = 256;
 	uint32_t m_maxOutDeg = 0, m_maxPlasticInDeg = 0;
 	int m_sms = 148;
