@@ -136,6 +136,10 @@ class ClockSampler:
 
     def __exit__(self, *exc):
         self.t1 = time.monotonic()
+        # a region shorter than the sampling interval: wait for the next row
+        deadline = self.t1 + 4 * self.INTERVAL_MS / 1e3
+        while self.proc and not any(self.t0 <= t for t, _ in self.rows) and time.monotonic() < deadline:
+            time.sleep(0.005)
         if self.proc:
             self.proc.terminate()
             try:
@@ -146,8 +150,14 @@ class ClockSampler:
 
     def summary(self) -> dict:
         inside = [r for t, r in self.rows if self.t0 <= t <= self.t1]
+        extra = {}
         if not inside:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["not sampled"], "samples": 0}
+            # the region was shorter than the interval: the first row after it
+            after = [(t, r) for t, r in self.rows if t > self.t1]
+            if not after:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["not sampled"], "samples": 0}
+            inside = [after[0][1]]
+            extra = {"row_after_region_ms": round((after[0][0] - self.t1) * 1e3, 1)}
         sm = [float(r[1]) for r in inside if len(r) > 2 and r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in inside if len(r) > 2 and r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -157,7 +167,7 @@ class ClockSampler:
                 if len(r) > 5 + k and r[5 + k].lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(inside), "interval_ms": self.INTERVAL_MS}
+                "reasons": sorted(reasons), "samples": len(inside), "interval_ms": self.INTERVAL_MS, **extra}
 
 
 def dist_setup(args):
@@ -557,6 +567,34 @@ def run_batch(args, local):
     print(json.dumps(line), flush=True)
 
 
+def run_floor(args, local):
+    """The scattered-update floor under the step's delivery: the step at
+    100k neurons issues about 660k reductions into 100k 16-byte accumulator
+    slots.  The same count at pseudo-random indices, as 64-bit reductions,
+    32-bit reductions and 8-byte loads, from 1 to 16 CTAs of 256 threads
+    per SM, timed with CUDA events (mean of `--steps` launches)."""
+    import nemosim_b200 as nb
+    ops, slots = 660_000, NEURONS
+    sms = torch_sms(local)
+    rows = []
+    for kind, name in ((0, "red.add.u64"), (1, "red.add.u32"), (2, "ld.u64")):
+        for per_sm in (1, 2, 4, 8, 16):
+            us = nb.scatter_probe(ops, slots, kind, per_sm * sms, local, max(1, min(args.steps, 1000)))
+            rows.append({"op": name, "ctas": per_sm * sms, "us": us, "gops_per_s": ops / us / 1e3})
+    best = max(r["gops_per_s"] for r in rows if r["op"] == "red.add.u64")
+    line = {"metric": "scattered 64-bit reductions per second (delivery floor)", "value": best * 1e9,
+            "unit": "ops/s", "n_gpus": 1, "higher_is_better": True, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": "scatter-floor", "ops": ops, "slots": slots, "slot_bytes": 16},
+            "steps": args.steps, "sweep": rows,
+            "step_floor_us": ops / (best * 1e3)}
+    print(json.dumps(line), flush=True)
+
+
+def torch_sms(local):
+    import torch
+    return torch.cuda.get_device_properties(local).multi_processor_count
+
+
 def run_bptt(args, local):
     """The differentiable configuration at full size: one gradient step
     (forward + hand-written adjoint) against PyTorch float32 autograd of
@@ -644,9 +682,10 @@ def main():
     ap.add_argument("--no-persistent", action="store_true")
     ap.add_argument("--host-construction", action="store_true",
                     help="build the connectivity on the host instead of the device")
-    ap.add_argument("--workload", choices=["headline", "batch256", "bptt"], default="headline",
+    ap.add_argument("--workload", choices=["headline", "batch256", "bptt", "floor"], default="headline",
                     help="headline: the 100k x 1k STDP network (default); batch256: batched networks "
-                         "against sequential runs; bptt: differentiable mode against PyTorch autograd")
+                         "against sequential runs; bptt: differentiable mode against PyTorch autograd; "
+                         "floor: the scattered-reduction floor under delivery")
     ap.add_argument("--batch-networks", type=int, default=256)
     ap.add_argument("--batch-min-neurons", type=int, default=1000)
     ap.add_argument("--batch-max-neurons", type=int, default=32000)
@@ -669,7 +708,7 @@ def main():
         local = int(os.environ.get("LOCAL_RANK", 0))
         if int(os.environ.get("RANK", 0)) != 0:
             return  # these comparisons run on one GPU
-        (run_batch if args.workload == "batch256" else run_bptt)(args, local)
+        {"batch256": run_batch, "bptt": run_bptt, "floor": run_floor}[args.workload](args, local)
         return
     rank, world, local = dist_setup(args)
     args.gpus = world if world > 1 else args.gpus

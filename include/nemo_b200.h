@@ -387,6 +387,15 @@ NEMO_B200_API nemo_status_t nemo_b200_libm_verify(uint64_t* mismatches);
  * (nemo_new_simulation and the like) that report failure only by returning
  * NULL. */
 NEMO_B200_API nemo_status_t nemo_b200_last_status(void);
+/* Measures the scattered-update floor of the step's pre-phase: `ops`
+ * operations at pseudo-random indices into `elements` 16-byte slots --
+ * kind 0: 64-bit reductions (as delivery issues them), 1: 32-bit
+ * reductions, 2: 8-byte loads -- from `ctas` CTAs of 256 threads (0: 8
+ * per SM) on `device`.  *us receives the mean CUDA-event time of `reps`
+ * launches (1..1000) after one warm-up launch, in microseconds.  ops is at
+ * most 2^30.  Allocates and frees its own device memory. */
+NEMO_B200_API nemo_status_t nemo_b200_scatter_probe(unsigned ops, unsigned elements, int kind, unsigned ctas,
+		int device, unsigned reps, float* us);
 /* Differentiable float32 mode.  A network of `neurons` Izhikevich neurons
  * with `synapses` delayed synapses (source[], target[], delay[] in 1..;
  * ordered by source; synapse e has weight w[e]) run for `ms` milliseconds of

@@ -235,6 +235,15 @@ class Network:
         return bool(v.value)
 
 
+def scatter_probe(ops: int, elements: int, kind: int = 0, ctas: int = 0, device: int = 0, reps: int = 20) -> float:
+    """Microseconds per launch of `ops` scattered operations into `elements`
+    16-byte slots (kind 0: 64-bit reductions, 1: 32-bit reductions, 2:
+    8-byte loads) -- the floor under the step's delivery (an extension)."""
+    us = C.c_float()
+    _check(lib().nemo_b200_scatter_probe(ops, elements, kind, ctas, device, reps, C.byref(us)))
+    return us.value
+
+
 def example_random(ncount: int, scount: int, dmax: int, stdp: bool, seed: int | None = None,
                    sigma_exc: float = 5.0, sigma_inh: float = 2.0) -> Network:
     """The reference's example network random::construct

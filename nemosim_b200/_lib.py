@@ -103,6 +103,8 @@ SIGNATURES = {
     "nemo_b200_set_resident_step": (st, [vp, C.c_uint]),
     "nemo_b200_set_wait_limit": (st, [vp, C.c_uint]),
     "nemo_b200_set_device_construction": (st, [vp, C.c_int]),
+    "nemo_b200_scatter_probe": (st, [C.c_uint, C.c_uint, C.c_int, C.c_uint, C.c_int, C.c_uint,
+                                     C.POINTER(C.c_float)]),
     "nemo_b200_connectivity_digest": (st, [vp, u64p]),
     "nemo_b200_trace_phases": (st, [vp, C.c_uint, u64p, sz, PU]),
 

@@ -18,6 +18,7 @@
 #include "handles.hpp"
 #include "network.hpp"
 #include "plugins.hpp"
+#include "probe.hpp"
 #include "simulation.hpp"
 
 using namespace nemo_b200;
@@ -726,6 +727,13 @@ nemo_status_t nemo_b200_libm_verify(uint64_t* mismatches)
 }
 
 nemo_status_t nemo_b200_last_status(void) { return g_lastStatus; }
+
+nemo_status_t nemo_b200_scatter_probe(unsigned ops, unsigned elements, int kind, unsigned ctas, int device,
+		unsigned reps, float* us)
+{
+	NULLCHECK(us);
+	CALL(*us = scatter_probe(ops, elements, kind, ctas, device, reps));
+}
 
 nemo_b200_bptt_t nemo_b200_bptt_new(unsigned neurons, unsigned trials, unsigned ms, unsigned readout,
 		unsigned checkpoint_ms, size_t synapses, const unsigned source[], const unsigned target[],

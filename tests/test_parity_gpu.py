@@ -192,7 +192,7 @@ def test_kuramoto_known_answers():
 
 @pytest.mark.parametrize("persistent", [True, False])
 def test_kuramoto_matches_oracle(persistent):
-    """A 2048-oscillator network with delayed couplings, 1000 steps: the
+    """A 2048-oscillator network with delayed couplings, 300 steps: the
     phases agree with the oracle's to 1e-4 radian.  Not bit for bit: the
     device's sinf is CUDA's, the oracle's the host libm's."""
     class Persistent:
