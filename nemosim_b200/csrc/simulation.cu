@@ -601,6 +601,15 @@ __device__ __forceinline__ void red_release_add(uint32_t* p, uint32_t v)
 	asm volatile("red.release.gpu.global.add.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
 
+// Whether a wait gives up: after `limit` unsuccessful polls, or once another
+// CTA has given up (the error word, read at every 32nd poll only, so that a
+// poll costs one round trip to L2)
+__device__ __forceinline__ bool give_up(GridBarrier* gb, uint32_t& polls, uint32_t limit)
+{
+	++polls;
+	return polls > limit || ((polls & 31u) == 0 && ld_acquire(&gb->error));
+}
+
 // The barrier in two halves: grid_arrive, then work that needs nothing from
 // the other CTAs, then grid_wait.  target: this CTA's count of completed
 // barriers x gridDim.x (shared).
@@ -623,7 +632,7 @@ __device__ __forceinline__ bool grid_wait(GridBarrier* gb, uint32_t& target, uin
 	if(threadIdx.x == 0) {
 		uint32_t polls = 0;
 		while(!reached(ld_acquire(&gb->count), target)) {
-			if(++polls > limit || ld_acquire(&gb->error)) {
+			if(give_up(gb, polls, limit)) {
 				atomicExch(&gb->error, 1u);
 				ok = 0;
 				break;
@@ -643,7 +652,7 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier* gb, uint32_t& target, 
 		red_release_add(&gb->count, 1u);
 		uint32_t polls = 0;
 		while(!reached(ld_acquire(&gb->count), target)) {
-			if(++polls > limit || ld_acquire(&gb->error)) {
+			if(give_up(gb, polls, limit)) {
 				atomicExch(&gb->error, 1u);
 				ok = 0;
 				break;
@@ -887,7 +896,7 @@ __device__ __forceinline__ uint32_t wait_request(GridBarrier* gb, uint32_t want,
 				break;
 			}
 			if(v == (want | SERVE_STOP)) break;
-			if(++polls > limit || ld_acquire(&gb->error)) {
+			if(give_up(gb, polls, limit)) {
 				atomicExch(&gb->error, 1u);
 				ok = 0;
 				break;
@@ -1013,9 +1022,12 @@ collect_touched_kernel(const DevSim S)
 // ALL: every target, whatever its accumulator -- the first call, which also
 // clamps weights that start outside their range.  Work items are (slice,
 // 32 targets), slice-major; a warp flattens its 32 runs with a scan and
-// finds each entry's run with a 5-step shuffle search.
+// finds each entry's run with a 5-step shuffle search.  The targets of the
+// warp's item after next and the runs of its next item are loaded while an
+// item is processed (at 5 CTAs of 256 threads per SM: 48 registers, no
+// spills), so an item's two dependent prologue loads are off its path.
 template<bool ALL>
-__global__ void __launch_bounds__(STEP_THREADS, 6)
+__global__ void __launch_bounds__(STEP_THREADS, 5)
 apply_kernel(const DevSim S, int32_t reward)
 {
 	const uint32_t FULL = 0xffffffffu;
@@ -1024,20 +1036,39 @@ apply_kernel(const DevSim S, int32_t reward)
 	const uint32_t batches = (nT + 31) >> 5;
 	const unsigned long long items = (unsigned long long) batches * S.applySlices;
 	const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-	for(unsigned long long i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < items; i += nw) {
-		const uint32_t k = (uint32_t) (i / batches);
-		const uint32_t j = (uint32_t) (i - (unsigned long long) k * batches) * 32 + lane;
-		unsigned long long lo = 0;
-		uint32_t len = 0;
-		if(j < nT) {
-			const uint32_t t = ALL ? j : S.touchedList[j];
-			const uint32_t* run = S.rcmSlice + (size_t) k * S.N + t;
+	// lane's target of item ii (N: none)
+	auto target_of = [&](unsigned long long ii) -> uint32_t {
+		if(ii >= items) return S.N;
+		const uint32_t kk = (uint32_t) (ii / batches);
+		const uint32_t jj = (uint32_t) (ii - (unsigned long long) kk * batches) * 32 + lane;
+		return jj < nT ? (ALL ? jj : S.touchedList[jj]) : S.N;
+	};
+	// lane's run of item ii for target t
+	auto run_of = [&](unsigned long long ii, uint32_t t, unsigned long long& lo, uint32_t& len) {
+		lo = 0;
+		len = 0;
+		if(ii < items && t < S.N) {
+			const uint32_t kk = (uint32_t) (ii / batches);
+			const uint32_t* run = S.rcmSlice + (size_t) kk * S.N + t;
 			const uint32_t a = run[0];
 			lo = S.rcmPtr[t] + a;
 			len = run[S.N] - a;
 		}
+	};
+	unsigned long long i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	unsigned long long nlo;
+	uint32_t nlen;
+	run_of(i, target_of(i), nlo, nlen);
+	uint32_t tn = target_of(i + nw);
+	for(; i < items; i += nw) {
+		const unsigned long long lo = nlo;
+		const uint32_t len = nlen;
 		const uint32_t incl = warp_inclusive_scan(len);
 		const uint32_t total = __shfl_sync(FULL, incl, 31);
+		// the next items' targets and runs, loaded while this one is processed
+		const uint32_t tnn = target_of(i + 2ull * nw);
+		run_of(i + nw, tn, nlo, nlen);
+		tn = tnn;
 		for(uint32_t off = 0; off < total; off += 32 * APPLY_ILP) {
 			unsigned long long e[APPLY_ILP];
 			int32_t acc[APPLY_ILP];
