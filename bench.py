@@ -377,11 +377,12 @@ def run_b200(args, rank, world, local):
     if persistent:
         phases = phase_summary(sim.trace_phases(W))
 
-    # e2e through the C ABI with host buffers, the calls a C caller makes:
+    # e2e through the C ABI with host buffers, the calls a C program makes:
     # nemo_step once per ms (a one-neuron firing stimulus from host memory,
     # the fired ids returned in host memory) and nemo_apply_stdp once per
-    # period
-    # (bound here with plain pointer arguments, as C passes them)
+    # period, the loop itself in C (nemo_b200_bench_step_loop, the
+    # reference's benchmark() loop); then the same calls from a Python loop
+    # through ctypes
     import ctypes as C
     L = nb.lib()
     c_step = C.CDLL(nb.library_path()).nemo_step
@@ -390,17 +391,25 @@ def run_b200(args, rank, world, local):
                        C.c_void_p]
     rng = np.random.default_rng(rank)
     ke = max(1, min(args.steps, args.e2e_steps))
-    ev0 = sim.step_events()
-    stim = rng.integers(0, args.neurons, size=ke * W).astype(np.uint32)
-    no_u32, no_f32 = np.zeros(1, np.uint32), np.zeros(1, np.float32)
-    fired, nfired = C.POINTER(C.c_uint)(), C.c_size_t()
-    h, pf, pn = sim._h, C.addressof(fired), C.addressof(nfired)
-    p_stim, p_i, p_v = stim.ctypes.data, no_u32.ctypes.data, no_f32.ctypes.data
-    fired_total = 0
+    stim = rng.integers(0, args.neurons, size=2 * ke * W).astype(np.uint32)
     resident = persistent and not args.no_resident
     if not resident:
         sim.set_resident_step(0)
+    ev0 = sim.step_events()
+    fired_c, secs = C.c_uint64(), C.c_double()
     barrier(world)
+    nb._check(L.nemo_b200_bench_step_loop(sim._h, stim[: ke * W], 1, ke * W, W, 1.0, C.byref(fired_c),
+                                          C.byref(secs)))
+    barrier(world)
+    e2e_s = dist_max(secs.value, world)
+    e2e_events = dist_sum(float(sim.step_events() - ev0), world)
+    fired_total = fired_c.value
+    # the Python loop over the same C calls
+    no_u32, no_f32 = np.zeros(1, np.uint32), np.zeros(1, np.float32)
+    fired, nfired = C.POINTER(C.c_uint)(), C.c_size_t()
+    h, pf, pn = sim._h, C.addressof(fired), C.addressof(nfired)
+    p_stim, p_i, p_v = stim.ctypes.data + 4 * ke * W, no_u32.ctypes.data, no_f32.ctypes.data
+    ev1 = sim.step_events()
     t0 = time.perf_counter()
     k = 0
     for _ in range(ke):
@@ -408,13 +417,10 @@ def run_b200(args, rank, world, local):
             rc = c_step(h, p_stim + 4 * k, 1, p_i, p_v, 0, pf, pn)
             if rc:
                 nb._check(rc)
-            fired_total += nfired.value
             k += 1
         nb._check(L.nemo_apply_stdp(sim._h, 1.0))
-    e2e_s = time.perf_counter() - t0
-    barrier(world)
-    e2e_s = dist_max(e2e_s, world)
-    e2e_events = dist_sum(float(sim.step_events() - ev0), world)
+    py_loop_s = time.perf_counter() - t0
+    py_loop_events = float(sim.step_events() - ev1)
     # the same loop through the Python wrapper (fired ids as a list)
     t0 = time.perf_counter()
     for k in range(W):
@@ -449,7 +455,8 @@ def run_b200(args, rank, world, local):
             # launches: the fired bit-vector out instead)
             "e2e": {"value": e2e_events / e2e_s, "unit": UNIT, "h2d_bytes_per_step": (4 + 16) * W,
                     "d2h_bytes_per_step": (round(4 * fired_total / ke) + 16 * W) if resident else 4 * words * W,
-                    "api": "nemo_step + nemo_apply_stdp (C ABI)",
+                    "api": "nemo_step + nemo_apply_stdp (C ABI), loop in C (nemo_b200_bench_step_loop)",
+                    "python_loop_value": py_loop_events / py_loop_s,
                     "step_path": "resident step loop" if resident else "two launches per nemo_step",
                     "sim_ms_per_s": ke * W / e2e_s, "fired_per_ms": fired_total / (ke * W),
                     "python_step_us": py_step_us},

@@ -394,6 +394,16 @@ NEMO_B200_API nemo_status_t nemo_b200_last_status(void);
  * per SM) on `device`.  *us receives the mean CUDA-event time of `reps`
  * launches (1..1000) after one warm-up launch, in microseconds.  ops is at
  * most 2^30.  Allocates and frees its own device memory. */
+/* The end-to-end benchmark loop of a C program (the role of the
+ * reference's benchmark(), src/examples/common.cpp:13-122): `steps` calls
+ * of nemo_step, each with fstim_per_step firing-stimulus indices from
+ * fstim (host memory, consecutive per step) and the fired ids returned in
+ * host memory, and nemo_apply_stdp(reward) after every `period` steps (0:
+ * never).  It uses the public calls above only.  *fired_total receives the
+ * number of fired ids returned, *seconds the loop's host wall time. */
+NEMO_B200_API nemo_status_t nemo_b200_bench_step_loop(nemo_simulation_t, const unsigned* fstim,
+		size_t fstim_per_step, unsigned steps, unsigned period, float reward, uint64_t* fired_total,
+		double* seconds);
 NEMO_B200_API nemo_status_t nemo_b200_scatter_probe(unsigned ops, unsigned elements, int kind, unsigned ctas,
 		int device, unsigned reps, float* us);
 /* Differentiable float32 mode.  A network of `neurons` Izhikevich neurons

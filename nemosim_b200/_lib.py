@@ -103,6 +103,8 @@ SIGNATURES = {
     "nemo_b200_set_resident_step": (st, [vp, C.c_uint]),
     "nemo_b200_set_wait_limit": (st, [vp, C.c_uint]),
     "nemo_b200_set_device_construction": (st, [vp, C.c_int]),
+    "nemo_b200_bench_step_loop": (st, [vp, u32p, sz, C.c_uint, C.c_uint, C.c_float, C.POINTER(C.c_uint64),
+                                       C.POINTER(C.c_double)]),
     "nemo_b200_scatter_probe": (st, [C.c_uint, C.c_uint, C.c_int, C.c_uint, C.c_int, C.c_uint,
                                      C.POINTER(C.c_float)]),
     "nemo_b200_connectivity_digest": (st, [vp, u64p]),
