@@ -6,7 +6,8 @@
 // does: step() (prefire / stimulus / fire / postfire / readFiring),
 // applyStdp and the queries.  The checks are the reference's own
 // known-answer tests (src/test/test.cpp ring and current stimulus,
-// src/test/stdp.cpp testStdp).
+// src/test/stdp.cpp testStdp) and the comparison of the C++ and C paths
+// (src/test/c_api.cpp compareWithCpp).
 //
 //   driver nodevice   without a GPU: configuration and creation fail with
 //                     the reference's status codes
@@ -25,7 +26,9 @@
 #include <string.h>
 
 #include <memory>
+#include <random>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 extern "C" nemo::SimulationBackend* cuda_simulation(const nemo::network::Generator*, const nemo::ConfigurationImpl*);
@@ -77,8 +80,7 @@ public:
 	}
 	void addSynapse(unsigned src, unsigned tgt, unsigned delay, float w, bool plastic)
 	{
-		unsigned id = 0;
-		for(const nemo::Synapse& s : m_synapses) if(s.source == src) ++id;
+		const unsigned id = m_outCount[src]++;  // the per-source synapse index
 		m_synapses.emplace_back(src, delay, nemo::AxonTerminal(id, tgt, w, plastic));
 		if(delay > m_maxDelay) m_maxDelay = delay;
 	}
@@ -116,6 +118,7 @@ private:
 	std::vector<nemo::NeuronType> m_types;
 	std::vector<std::vector<neuron>> m_neurons;
 	std::vector<nemo::Synapse> m_synapses;
+	std::unordered_map<unsigned, unsigned> m_outCount;
 	unsigned m_maxDelay = 0;
 };
 
@@ -251,6 +254,108 @@ void testStdp()
 	}
 }
 
+// compareWithCpp (src/test/c_api.cpp:236-330): the same partially random
+// network of 1000 Izhikevich neurons x 1000 synapses (80% excitatory,
+// sigma 5 and 2), built once through the reference's C++ network
+// interface and run through the adapter's backend, and once through the C
+// API, for 2000 steps with an optional firing and current stimulus at
+// cycle 0: the fire streams are identical.  The C run reads a synapse back
+// every 100 steps, as the reference's does.
+void testCompareWithC(bool useFstim, bool useIstim)
+{
+	const unsigned ncount = 1000, scount = 1000, steps = 2000;
+	std::mt19937 rng(5489u);
+	auto param = [&]() { return (float) ((double) rng() / 4294967296.0); };
+	auto target = [&]() { return (unsigned) (rng() % ncount); };
+	VectorGenerator net;
+	const unsigned iz = net.addType("Izhikevich", 5, 2);
+	nemo_network_t cnet = nemo_new_network();
+	REQUIRE(cnet);
+	unsigned ciz = 0;
+	REQUIRE(nemo_add_neuron_type(cnet, "Izhikevich", &ciz) == NEMO_OK);
+	for(unsigned n = 0; n < ncount; ++n) {
+		const bool exc = n < ncount * 4 / 5;
+		const float v = -65.0f;
+		float a, b, c, d, sigma;
+		if(exc) {
+			const float r1 = param(), r2 = param();
+			a = 0.02f;
+			b = 0.2f;
+			c = v + 15.0f * r1 * r1;
+			d = 8.0f - 6.0f * r2 * r2;
+			sigma = 5.0f;
+		} else {
+			const float r1 = param();
+			a = 0.02f + 0.08f * r1;
+			const float r2 = param();
+			b = 0.25f - 0.05f * r2;
+			c = v;
+			d = 2.0f;
+			sigma = 2.0f;
+		}
+		const float u = b * v;
+		net.addNeuron(iz, n, { a, b, c, d, sigma }, { u, v });
+		float args[7] = { a, b, c, d, sigma, u, v };
+		REQUIRE(nemo_add_neuron(cnet, ciz, n, 7, args) == NEMO_OK);
+		for(unsigned k = 0; k < scount; ++k) {
+			const unsigned t = target();
+			const float w = exc ? 0.5f * param() : -param();
+			net.addSynapse(n, t, 1, w, false);
+			REQUIRE(nemo_add_synapse(cnet, n, t, 1, w, 0, nullptr) == NEMO_OK);
+		}
+	}
+	std::vector<unsigned> fstim;
+	if(useFstim) fstim.push_back(100);
+	nemo::Simulation::current_stimulus istim;
+	std::vector<unsigned> inidx;
+	std::vector<float> icur;
+	if(useIstim) {
+		for(unsigned i : { 20u, 40u, 60u }) {
+			istim.push_back(std::make_pair(i, 20.0f));
+			inidx.push_back(i);
+			icur.push_back(20.0f);
+		}
+	}
+	std::vector<std::pair<unsigned, unsigned>> cpp, c;
+	{
+		nemo::ConfigurationImpl conf;
+		std::unique_ptr<nemo::SimulationBackend> sim(cuda_simulation(&net, &conf));
+		for(unsigned ms = 0; ms < steps; ++ms) {
+			const std::vector<unsigned>& f = ms == 0 ? sim->step(fstim, istim) : sim->step();
+			for(unsigned id : f) cpp.emplace_back(ms, id);
+		}
+	}
+	{
+		nemo_configuration_t conf = nemo_new_configuration();
+		nemo_simulation_t sim = nemo_new_simulation(cnet, conf);
+		REQUIRE(sim);
+		for(unsigned ms = 0; ms < steps; ++ms) {
+			unsigned* fired = nullptr;
+			size_t nfired = 0;
+			if(ms == 0) {
+				REQUIRE(nemo_step(sim, fstim.empty() ? nullptr : fstim.data(), fstim.size(),
+						inidx.empty() ? nullptr : inidx.data(), icur.empty() ? nullptr : icur.data(), inidx.size(),
+						&fired, &nfired) == NEMO_OK);
+			} else {
+				REQUIRE(nemo_step(sim, nullptr, 0, nullptr, nullptr, 0, &fired, &nfired) == NEMO_OK);
+			}
+			for(size_t i = 0; i < nfired; ++i) c.emplace_back(ms, fired[i]);
+			if(ms % 100 == 0) {
+				synapse_id* ids = nullptr;
+				size_t len = 0;
+				REQUIRE(nemo_get_synapses_from_s(sim, 1, &ids, &len) == NEMO_OK && len == scount);
+				float w = 0;
+				REQUIRE(nemo_get_synapse_weight_s(sim, ids[0], &w) == NEMO_OK && w >= 0.0f && w <= 0.5f);
+			}
+		}
+		nemo_delete_simulation(sim);
+		nemo_delete_configuration(conf);
+	}
+	nemo_delete_network(cnet);
+	REQUIRE(!cpp.empty());
+	REQUIRE(cpp == c);
+}
+
 // without a device: the configuration fails as DeviceMap::setConfiguration
 // does, and creating the backend fails with a status, not a crash
 void testNoDevice()
@@ -297,6 +402,7 @@ int main(int argc, char** argv)
 			testRing();
 			testCurrentStimulus();
 			testStdp();
+			for(int k = 0; k < 4; ++k) testCompareWithC(k & 1, k & 2);
 		} else {
 			fprintf(stderr, "usage: driver nodevice|gpu\n");
 			return 2;
