@@ -12,6 +12,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <stdexcept>
 
 #include "common.hpp"
 
@@ -74,8 +75,8 @@ __device__ __forceinline__ bool fx_to_fix(float f, int32_t& out)
 }
 
 __global__ void map_kernel(size_t S, const unsigned* src, const unsigned* tgt, const unsigned* delay,
-		const float* weight, const uint32_t* g2l, uint32_t maxGid, uint32_t D, uint32_t* ls, uint32_t* lt,
-		int32_t* fx, uint32_t* key, uint32_t* idx, uint32_t* rowCount, unsigned long long* err)
+		const float* weight, const uint32_t* g2l, uint32_t maxGid, uint32_t srcBase, uint32_t D, uint32_t* ls,
+		uint32_t* lt, int32_t* fx, uint32_t* key, uint32_t* idx, uint32_t* rowCount, unsigned long long* err)
 {
 	for(size_t k = blockIdx.x * (size_t) blockDim.x + threadIdx.x; k < S; k += (size_t) gridDim.x * blockDim.x) {
 		const unsigned s = src[k], t = tgt[k];
@@ -86,7 +87,7 @@ __global__ void map_kernel(size_t S, const unsigned* src, const unsigned* tgt, c
 		if(b == ~0u) report(err, 2, k);
 		if(!fx_to_fix(weight[k], w)) report(err, 3, k);
 		if(a == ~0u || b == ~0u) continue;
-		const uint32_t r = a * D + (delay[k] - 1);
+		const uint32_t r = (a - srcBase) * D + (delay[k] - 1);
 		ls[k] = a;
 		lt[k] = b;
 		fx[k] = w;
@@ -96,6 +97,8 @@ __global__ void map_kernel(size_t S, const unsigned* src, const unsigned* tgt, c
 	}
 }
 
+// syn: the network's part of the union forward matrix; pos: each synapse's
+// place in it
 __global__ void fill_forward_kernel(size_t S, const uint32_t* sortedIdx, const uint32_t* lt, const unsigned* delay,
 		const int32_t* fx, uint2* syn, uint32_t* pos)
 {
@@ -106,29 +109,31 @@ __global__ void fill_forward_kernel(size_t S, const uint32_t* sortedIdx, const u
 	}
 }
 
-// per source: its row start, the end of each delay's group within the row,
-// and the delays deliverSpikes delivers (OutgoingDelays.cpp:70-80)
-__global__ void groups_kernel(uint32_t N, uint32_t D, bool deliver, const uint32_t* rowStart,
-		unsigned long long* outPtr, uint16_t* end16, uint32_t* end32, uint64_t* delayMask,
+// per source s of the network (union index srcBase + s): its row start, the
+// end of each delay's group within the row, and the delays deliverSpikes
+// delivers (OutgoingDelays.cpp:70-80)
+__global__ void groups_kernel(uint32_t n, uint32_t srcBase, uint64_t synOff, uint32_t D, bool deliver,
+		const uint32_t* rowStart, unsigned long long* outPtr, uint16_t* end16, uint32_t* end32, uint64_t* delayMask,
 		unsigned long long* groups)
 {
-	for(uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < N; s += gridDim.x * blockDim.x) {
+	for(uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
 		const uint32_t base = rowStart[(size_t) s * D];
+		const size_t u = (size_t) srcBase + s;
 		uint32_t prev = 0;
 		uint64_t mask = 0;
 		unsigned long long g = 0;
 		for(uint32_t d = 1; d <= D; ++d) {
 			const uint32_t e = rowStart[(size_t) s * D + d] - base;
-			if(end16) end16[(size_t) s * D + d - 1] = (uint16_t) e;
-			else end32[(size_t) s * D + d - 1] = e;
+			if(end16) end16[u * D + d - 1] = (uint16_t) e;
+			else end32[u * D + d - 1] = e;
 			if(deliver && e > prev) {
 				mask |= 1ull << (d - 1);
 				++g;
 			}
 			prev = e;
 		}
-		outPtr[s] = base;
-		delayMask[s] = mask;
+		outPtr[u] = synOff + base;
+		delayMask[u] = mask;
 		if(g) atomicAdd(groups, g);
 	}
 }
@@ -150,23 +155,25 @@ __global__ void compact_kernel(size_t S, const uint32_t* flag, const uint32_t* a
 	}
 }
 
-__global__ void plastic_keys_kernel(size_t P, const uint32_t* plf, const uint2* syn, uint32_t* key2,
-		uint32_t* tgtCount)
+// key2: the plastic entry's target relative to the network's first neuron
+__global__ void plastic_keys_kernel(size_t P, const uint32_t* plf, const uint2* syn, uint32_t srcBase,
+		uint32_t* key2, uint32_t* tgtCount)
 {
 	for(size_t q = blockIdx.x * (size_t) blockDim.x + threadIdx.x; q < P; q += (size_t) gridDim.x * blockDim.x) {
-		const uint32_t t = syn[plf[q]].x & TARGET_MASK;
+		const uint32_t t = (syn[plf[q]].x & TARGET_MASK) - srcBase;
 		key2[q] = t;
 		atomicAdd(tgtCount + t, 1u);
 	}
 }
 
+// rsrc, rfwd: the network's part of the union reverse matrix
 __global__ void fill_reverse_kernel(size_t P, const uint32_t* sortedPlf, const uint32_t* sortedIdx,
-		const uint32_t* ls, const uint2* syn, uint32_t* rsrc, uint32_t* rfwd)
+		const uint32_t* ls, const uint2* syn, uint64_t synOff, uint32_t* rsrc, uint32_t* rfwd)
 {
 	for(size_t q = blockIdx.x * (size_t) blockDim.x + threadIdx.x; q < P; q += (size_t) gridDim.x * blockDim.x) {
 		const uint32_t p = sortedPlf[q];
 		rsrc[q] = ls[sortedIdx[p]] | (syn[p].x & ~TARGET_MASK);
-		rfwd[q] = p;
+		rfwd[q] = (uint32_t) (synOff + p);
 	}
 }
 
@@ -210,11 +217,11 @@ T* upload(Scratch& scratch, const T* host, size_t n, cudaStream_t st)
 
 } // namespace
 
-void construct_on_device(DeviceConstruction& c, cudaStream_t st, const std::function<void*(size_t)>& alloc)
+void construct_on_device(DeviceConstruction& c, cudaStream_t st)
 {
 	Scratch scratch;
 	const size_t S = c.S;
-	const uint32_t N = c.N, D = c.D;
+	const uint32_t N = c.nLocal, D = c.D;
 	const size_t rows = (size_t) N * D;
 	if(S >= (1ull << 31) - 1 || rows >= (1ull << 31) - 1) {
 		NB_THROW(NEMO_API_UNSUPPORTED, "network too large for the device build");
@@ -237,8 +244,8 @@ void construct_on_device(DeviceConstruction& c, cudaStream_t st, const std::func
 	CC_CUDA(cudaMemsetAsync(rowCount, 0, (rows + 1) * 4, st));
 	CC_CUDA(cudaMemsetAsync(err, 0xff, 8, st));
 	CC_CUDA(cudaMemsetAsync(err + 1, 0, 8, st));
-	map_kernel<<<blocks(S), THREADS, 0, st>>>(S, src, tgt, dly, wgt, g2l, c.maxGid, D, ls, lt, fx, key, idx,
-			rowCount, err);
+	map_kernel<<<blocks(S), THREADS, 0, st>>>(S, src, tgt, dly, wgt, g2l, c.maxGid, c.srcBase, D, ls, lt, fx, key,
+			idx, rowCount, err);
 	CC_CUDA(cudaGetLastError());
 	unsigned long long herr = 0;
 	CC_CUDA(cudaMemcpyAsync(&herr, err, 8, cudaMemcpyDeviceToHost, st));
@@ -269,37 +276,28 @@ void construct_on_device(DeviceConstruction& c, cudaStream_t st, const std::func
 	tmp = scratch.get<uint8_t>(tmpBytes);
 	CC_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmpBytes, key, keySorted, idx, idxSorted, (int) S, 0, keyBits, st));
 
-	c.syn = static_cast<uint2*>(alloc(S * sizeof(uint2)));
+	uint2* syn = c.syn + c.synOff;
 	uint32_t* pos = scratch.get<uint32_t>(S);
-	fill_forward_kernel<<<blocks(S), THREADS, 0, st>>>(S, idxSorted, lt, dly, fx, c.syn, pos);
+	fill_forward_kernel<<<blocks(S), THREADS, 0, st>>>(S, idxSorted, lt, dly, fx, syn, pos);
 	CC_CUDA(cudaGetLastError());
 
-	// delay groups; the narrow table when every row is shorter than 65536
+	// delay groups
+	unsigned long long* groups = err + 1;
+	groups_kernel<<<blocks(N), THREADS, 0, st>>>(N, c.srcBase, c.synOff, D, c.deliver, rowStart, c.outPtr, c.dEnd16,
+			c.dEnd32, c.delayMask, groups);
+	CC_CUDA(cudaGetLastError());
 	std::vector<uint32_t> hostRowStart(rows + 1);
 	CC_CUDA(cudaMemcpyAsync(hostRowStart.data(), rowStart, (rows + 1) * 4, cudaMemcpyDeviceToHost, st));
-	CC_CUDA(cudaStreamSynchronize(st));
-	c.hostOutPtr.resize((size_t) N + 1);
-	uint32_t maxOut = 0;
-	for(uint32_t s = 0; s < N; ++s) {
-		c.hostOutPtr[s] = hostRowStart[(size_t) s * D];
-		maxOut = std::max(maxOut, hostRowStart[(size_t) (s + 1) * D] - hostRowStart[(size_t) s * D]);
-	}
-	c.hostOutPtr[N] = S;
-	const bool narrow = maxOut < 65536;
-	if(narrow) c.dEnd16 = static_cast<uint16_t*>(alloc(rows * 2));
-	else c.dEnd32 = static_cast<uint32_t*>(alloc(rows * 4));
-	c.outPtr = static_cast<unsigned long long*>(alloc(((size_t) N + 1) * 8));
-	c.delayMask = static_cast<uint64_t*>(alloc((size_t) N * 8));
-	unsigned long long* groups = err + 1;
-	groups_kernel<<<blocks(N), THREADS, 0, st>>>(N, D, c.deliver, rowStart, c.outPtr, c.dEnd16, c.dEnd32,
-			c.delayMask, groups);
-	CC_CUDA(cudaGetLastError());
-	CC_CUDA(cudaMemcpyAsync(c.outPtr + N, &c.hostOutPtr[N], 8, cudaMemcpyHostToDevice, st));
 	unsigned long long hg = 0;
 	CC_CUDA(cudaMemcpyAsync(&hg, groups, 8, cudaMemcpyDeviceToHost, st));
+	CC_CUDA(cudaStreamSynchronize(st));
+	c.hostOutPtr.resize(N);
+	for(uint32_t s = 0; s < N; ++s) c.hostOutPtr[s] = c.synOff + hostRowStart[(size_t) s * D];
 
-	// the reverse matrix of plastic synapses, insertion order within a target
-	c.hostRcmPtr.assign((size_t) N + 1, 0);
+	// the reverse matrix of plastic synapses, in forward order within a
+	// target
+	c.hostRcmPtr.assign(N, c.plOff);
+	c.plastic_count = 0;
 	if(c.stdp) {
 		uint32_t* flag = scratch.get<uint32_t>(S + 1);
 		uint32_t* at = scratch.get<uint32_t>(S + 1);
@@ -320,7 +318,7 @@ void construct_on_device(DeviceConstruction& c, cudaStream_t st, const std::func
 		uint32_t* tgtCount = scratch.get<uint32_t>((size_t) N + 1);
 		uint32_t* tgtStart = scratch.get<uint32_t>((size_t) N + 1);
 		CC_CUDA(cudaMemsetAsync(tgtCount, 0, ((size_t) N + 1) * 4, st));
-		plastic_keys_kernel<<<blocks(P), THREADS, 0, st>>>(P, plk, c.syn, key2, tgtCount);
+		plastic_keys_kernel<<<blocks(P), THREADS, 0, st>>>(P, plk, syn, c.srcBase, key2, tgtCount);
 		CC_CUDA(cudaGetLastError());
 		tmpBytes = 0;
 		CC_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmpBytes, tgtCount, tgtStart, (int) N + 1, st));
@@ -336,14 +334,13 @@ void construct_on_device(DeviceConstruction& c, cudaStream_t st, const std::func
 		tmp = scratch.get<uint8_t>(tmpBytes);
 		CC_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmpBytes, key2, key2Sorted, plk, plkSorted, (int) P, 0, tBits,
 				st));
-		c.rcmSrc = static_cast<uint32_t*>(alloc(P * 4));
-		c.rcmFwd = static_cast<uint32_t*>(alloc(P * 4));
-		fill_reverse_kernel<<<blocks(P), THREADS, 0, st>>>(P, plkSorted, idxSorted, ls, c.syn, c.rcmSrc, c.rcmFwd);
+		fill_reverse_kernel<<<blocks(P), THREADS, 0, st>>>(P, plkSorted, idxSorted, ls, syn, c.synOff,
+				c.rcmSrc + c.plOff, c.rcmFwd + c.plOff);
 		CC_CUDA(cudaGetLastError());
 		std::vector<uint32_t> hs((size_t) N + 1);
 		CC_CUDA(cudaMemcpyAsync(hs.data(), tgtStart, ((size_t) N + 1) * 4, cudaMemcpyDeviceToHost, st));
 		CC_CUDA(cudaStreamSynchronize(st));
-		for(size_t i = 0; i <= N; ++i) c.hostRcmPtr[i] = hs[i];
+		for(size_t i = 0; i < N; ++i) c.hostRcmPtr[i] = c.plOff + hs[i];
 		c.plastic_count = P;
 	}
 

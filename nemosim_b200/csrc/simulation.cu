@@ -1574,10 +1574,9 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 	}
 	S.stdp = conf.stdp ? 1 : 0;
 
-	std::vector<uint32_t> g2lDense;
-	if(conf.deviceConstruction && !batch && !needAll && Sn < (1ull << 31) - 1 && (uint64_t) N * D < (1ull << 31) - 1 &&
-			denseIds(g2lDense)) {
-		buildOnDevice(*nets[0], g2lDense, deliver, outPtr, rcmPtr, dlvGroups);
+	std::vector<DevicePart> parts;
+	if(conf.deviceConstruction && !needAll && planDeviceBuild(nets, conf.stdp, parts)) {
+		buildOnDevice(nets, parts, deliver, outPtr, rcmPtr, dlvGroups);
 	} else {
 		// synapses of all networks, each mapped through its own network's ids
 		hvector<unsigned> lsrc(Sn), ltgt(Sn), sdelay(Sn);
@@ -2765,69 +2764,153 @@ void Simulation::setNeuronParameter(unsigned g, unsigned p, float v)
 	sync();
 }
 
-bool Simulation::denseIds(std::vector<uint32_t>& g2l) const
+bool Simulation::planDeviceBuild(const std::vector<const Network*>& nets, bool stdp,
+		std::vector<DevicePart>& parts) const
 {
-	uint32_t maxGid = 0;
-	for(unsigned g : m_l2g) maxGid = std::max(maxGid, g);
-	if((uint64_t) maxGid + 1 > 4ull * m_N + (1u << 20)) return false;
-	g2l.assign((size_t) maxGid + 1, ~0u);
-	for(unsigned l = 0; l < m_N; ++l) g2l[m_l2g[l]] = l;
+	const uint32_t D = m_dev.dStride;
+	parts.assign(nets.size(), DevicePart());
+	uint64_t total = 0;
+	for(size_t i = 0; i < nets.size(); ++i) {
+		const Network& net = *nets[i];
+		DevicePart& part = parts[i];
+		if(nets.size() == 1) {
+			part.srcBase = 0;
+			part.nLocal = m_N;
+		} else {
+			// one neuron type: the network's neurons are one contiguous run
+			int only = -1;
+			for(size_t t = 0; t < net.types.size(); ++t) {
+				if(net.types[t].size() == 0) continue;
+				if(only >= 0) return false;
+				only = (int) t;
+			}
+			if(only < 0) return false;
+			const NetTypeRange& r = m_netTypes[i][only];
+			part.srcBase = m_types[r.hostType].base + r.offset;
+			part.nLocal = r.count;
+		}
+		const size_t Si = net.src.size();
+		if(Si >= (1ull << 31) - 1 || (uint64_t) part.nLocal * D >= (1ull << 31) - 1) return false;
+		uint32_t maxGid = 0;
+		for(const auto& kv : m_g2l[i]) maxGid = std::max(maxGid, kv.first);
+		if((uint64_t) maxGid + 1 > 4ull * part.nLocal + (1u << 20)) return false;
+		part.g2l.assign((size_t) maxGid + 1, ~0u);
+		for(const auto& kv : m_g2l[i]) part.g2l[kv.first] = kv.second;
+		if(stdp) {
+			uint64_t p = 0;
+			for(size_t k = 0; k < Si; ++k) p += net.plastic[k] != 0;
+			part.plastic = p;
+		}
+		total += Si;
+	}
+	if(stdp && total > 0xffffffffull) return false;
+	// each network's rows and reverse rows follow the order of its neurons
+	std::vector<size_t> order(nets.size());
+	for(size_t i = 0; i < order.size(); ++i) order[i] = i;
+	std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return parts[a].srcBase < parts[b].srcBase; });
+	uint64_t so = 0, po = 0;
+	for(size_t i : order) {
+		parts[i].synOff = so;
+		parts[i].plOff = po;
+		so += nets[i]->src.size();
+		po += parts[i].plastic;
+	}
 	return true;
 }
 
-// The device build of one network's connectivity (construction.cu): the
-// same forward matrix, delay groups and reverse matrix as the host build,
-// and the same errors, in the same order, for synapses between
-// non-existing neurons and weights outside the fixed-point range.
-void Simulation::buildOnDevice(const Network& net, const std::vector<uint32_t>& g2l, bool deliver,
+// The device build of the connectivity (construction.cu), network by
+// network into the union arrays: the same forward matrix, delay groups and
+// reverse matrix as the host build, and the same errors, in the same order,
+// for synapses between non-existing neurons and weights outside the
+// fixed-point range.
+void Simulation::buildOnDevice(const std::vector<const Network*>& nets, std::vector<DevicePart>& parts, bool deliver,
 		std::vector<unsigned long long>& outPtr, std::vector<unsigned long long>& rcmPtr, uint64_t& dlvGroups)
 {
 	DevSim& S = m_dev;
 	const unsigned N = m_N;
-	DeviceConstruction c;
-	c.S = m_nsyn;
-	c.src = net.src.data();
-	c.tgt = net.tgt.data();
-	c.delay = net.delay.data();
-	c.weight = net.weight.data();
-	c.plastic = net.plastic.data();
-	c.g2l = g2l.data();
-	c.maxGid = (uint32_t) (g2l.size() - 1);
-	c.N = N;
-	c.D = S.dStride;
-	c.deliver = deliver;
-	c.stdp = S.stdp != 0;
-	c.keepQueries = !m_writeOnly;
-	try {
-		construct_on_device(c, m_stream, [this](size_t bytes) { return (void*) dalloc<uint8_t>(bytes); });
-	} catch(...) {
-		m_kept = KeptSynapses{ c.keptSrc, c.keptPos, c.keptTgt, c.keptDelay, c.keptPlastic };
-		freeKept();
-		throw;
+	const uint32_t D = S.dStride;
+	// the wide delay-group table when some row has 65,536 synapses or more
+	uint32_t maxOut = 0;
+	uint64_t P = 0;
+	for(size_t i = 0; i < nets.size(); ++i) {
+		for(const auto& kv : nets[i]->axonCount) maxOut = std::max(maxOut, kv.second);
+		P += parts[i].plastic;
 	}
-	m_kept = KeptSynapses{ c.keptSrc, c.keptPos, c.keptTgt, c.keptDelay, c.keptPlastic };
-	S.syn = c.syn;
-	S.outPtr = c.outPtr;
-	S.dEnd16 = c.dEnd16;
-	S.dEnd32 = c.dEnd32;
-	S.delayMask = c.delayMask;
-	S.allPtr = dalloc<unsigned long long>(N + 1);  // no reverse matrix of all synapses
-	outPtr = c.hostOutPtr;
+	uint2* syn = dalloc<uint2>(m_nsyn);
+	auto* dOut = dalloc<unsigned long long>((size_t) N + 1);
+	uint16_t* end16 = maxOut < 65536 ? dalloc<uint16_t>((size_t) N * D) : nullptr;
+	uint32_t* end32 = maxOut < 65536 ? nullptr : dalloc<uint32_t>((size_t) N * D);
+	auto* mask = dalloc<uint64_t>(N);
+	uint32_t* rsrc = S.stdp ? dalloc<uint32_t>(P) : nullptr;
+	uint32_t* rfwd = S.stdp ? dalloc<uint32_t>(P) : nullptr;
+	outPtr.assign((size_t) N + 1, 0);
+	rcmPtr.assign((size_t) N + 1, 0);
+	dlvGroups = 0;
+	for(size_t i = 0; i < nets.size(); ++i) {
+		const Network& net = *nets[i];
+		DevicePart& part = parts[i];
+		DeviceConstruction c;
+		c.S = net.src.size();
+		c.src = net.src.data();
+		c.tgt = net.tgt.data();
+		c.delay = net.delay.data();
+		c.weight = net.weight.data();
+		c.plastic = net.plastic.data();
+		c.g2l = part.g2l.data();
+		c.maxGid = (uint32_t) (part.g2l.size() - 1);
+		c.srcBase = part.srcBase;
+		c.nLocal = part.nLocal;
+		c.D = D;
+		c.deliver = deliver;
+		c.stdp = S.stdp != 0;
+		c.keepQueries = !m_writeOnly && nets.size() == 1;
+		c.synOff = part.synOff;
+		c.plOff = part.plOff;
+		c.syn = syn;
+		c.outPtr = dOut;
+		c.dEnd16 = end16;
+		c.dEnd32 = end32;
+		c.delayMask = mask;
+		c.rcmSrc = rsrc;
+		c.rcmFwd = rfwd;
+		try {
+			construct_on_device(c, m_stream);
+		} catch(...) {
+			m_kept = KeptSynapses{ c.keptSrc, c.keptPos, c.keptTgt, c.keptDelay, c.keptPlastic };
+			freeKept();
+			throw;
+		}
+		if(c.keepQueries) m_kept = KeptSynapses{ c.keptSrc, c.keptPos, c.keptTgt, c.keptDelay, c.keptPlastic };
+		for(uint32_t s = 0; s < part.nLocal; ++s) {
+			outPtr[part.srcBase + s] = c.hostOutPtr[s];
+			rcmPtr[part.srcBase + s] = c.hostRcmPtr[s];
+		}
+		dlvGroups += c.dlvGroups;
+		part.g2l.clear();
+		part.g2l.shrink_to_fit();
+	}
+	outPtr[N] = m_nsyn;
+	rcmPtr[N] = P;
+	NB_CUDA(cudaMemcpyAsync(dOut + N, &outPtr[N], 8, cudaMemcpyHostToDevice, m_stream));
+	S.syn = syn;
+	S.outPtr = dOut;
+	S.dEnd16 = end16;
+	S.dEnd32 = end32;
+	S.delayMask = mask;
+	S.allPtr = dalloc<unsigned long long>((size_t) N + 1);  // no reverse matrix of all synapses
 	m_outDegree.resize(N);
 	for(unsigned s = 0; s < N; ++s) {
 		m_outDegree[s] = (uint32_t) (outPtr[s + 1] - outPtr[s]);
 		m_maxOutDeg = std::max(m_maxOutDeg, m_outDegree[s]);
 	}
-	dlvGroups = c.dlvGroups;
-	if(c.stdp) {
-		rcmPtr = c.hostRcmPtr;
+	if(S.stdp) {
 		for(unsigned t = 0; t < N; ++t) {
 			m_maxPlasticInDeg = std::max(m_maxPlasticInDeg, (uint32_t) (rcmPtr[t + 1] - rcmPtr[t]));
 		}
-		S.rcmSrc = c.rcmSrc;
-		S.rcmFwd = c.rcmFwd;
-		S.rcmAcc = dalloc<int32_t>(c.plastic_count);
-		lastPlastic = c.plastic_count;
+		S.rcmSrc = rsrc;
+		S.rcmFwd = rfwd;
+		S.rcmAcc = dalloc<int32_t>(P);
+		lastPlastic = P;
 	}
 	m_builtOnDevice = true;
 	NB_CUDA(cudaStreamSynchronize(m_stream));

@@ -268,12 +268,19 @@ private:
 	bool findLocal(unsigned g, unsigned* l) const;  // localIdx without throwing (one network)
 	void locate(unsigned g, const HostType** t, unsigned* i) const;
 	size_t synapseKey(uint64_t id);
-	// the connectivity built on the device (one network whose global ids
-	// fit a dense table of at most 4 entries per neuron plus 2^20, fewer
-	// than 2^31 - 1 synapses and delay-group rows, no reverse matrix of all
-	// synapses)
-	bool denseIds(std::vector<uint32_t>& g2l) const;
-	void buildOnDevice(const Network& net, const std::vector<uint32_t>& g2l, bool deliver,
+	// the connectivity built on the device, one network at a time: each
+	// network's neurons contiguous in the simulation's local order (one
+	// network, or a batch of networks of one neuron type each), its global
+	// ids within a dense table of at most 4 entries per neuron plus 2^20,
+	// fewer than 2^31 - 1 synapses and delay-group rows per network, and
+	// no type that reads the reverse matrix of all synapses
+	struct DevicePart {
+		uint32_t srcBase = 0, nLocal = 0;
+		std::vector<uint32_t> g2l;  // global id -> local index
+		uint64_t synOff = 0, plOff = 0, plastic = 0;
+	};
+	bool planDeviceBuild(const std::vector<const Network*>& nets, bool stdp, std::vector<DevicePart>& parts) const;
+	void buildOnDevice(const std::vector<const Network*>& nets, std::vector<DevicePart>& parts, bool deliver,
 			std::vector<unsigned long long>& outPtr, std::vector<unsigned long long>& rcmPtr, uint64_t& dlvGroups);
 	bool m_builtOnDevice = false;
 	uint64_t m_dlvGroups = 0;

@@ -224,3 +224,58 @@ def test_c2_network_digests_and_build_time():
     print(f"C2 construction: device {t_dev:.2f} s, host {t_host:.2f} s")
     assert on_dev and not on_host
     assert dd == dh
+
+
+def batch_specs(seed, count, stdp):
+    rng = np.random.default_rng(seed)
+    return [dict(ncount=int(rng.integers(300, 2500)), scount=int(rng.integers(20, 200)), seed=100 + 7 * k,
+                 sigma=float(rng.uniform(2, 8)), stdp=stdp) for k in range(count)]
+
+
+def batch_net(s):
+    return nb.example_random(s["ncount"], s["scount"], 20, s["stdp"], seed=s["seed"],
+                             sigma_exc=s["sigma"], sigma_inh=s["sigma"])
+
+
+def both_batch(specs, make_conf, expect_device=True, extra=None):
+    out = []
+    for device in (True, False):
+        conf = make_conf()
+        conf.set_device_construction(device)
+        networks = [batch_net(s) for s in specs] + ([extra()] if extra else [])
+        out.append(nb.Batch(networks, conf))
+    (dd, on_dev), (dh, on_host) = out[0].connectivity_digest(), out[1].connectivity_digest()
+    assert on_dev == expect_device and not on_host
+    assert dd == dh
+    return out
+
+
+@pytest.mark.parametrize("stdp", [False, True])
+def test_batch_of_one_type_networks(stdp):
+    """A batch whose networks have one neuron type each is built on the
+    device network by network, into the same union arrays."""
+    bd, bh = both_batch(batch_specs(4, 7, stdp), (lambda: nets.standard_stdp(nb)) if stdp else nb.Configuration)
+    cd, _, idd = bd.run(300, 100 if stdp else 0, 1.0)
+    ch, _, idh = bh.run(300, 100 if stdp else 0, 1.0)
+    assert np.array_equal(cd, ch) and np.array_equal(idd, idh)
+    assert cd.sum() > 0
+
+
+def test_batch_with_a_mixed_type_network_falls_back():
+    bd, bh = both_batch(batch_specs(5, 3, False), nb.Configuration, expect_device=False,
+                        extra=lambda: nets.mixed_network(nb, n_if=200, n_iz=300, n_poisson=50, seed=1)[0])
+    cd, _, idd = bd.run(200)
+    ch, _, idh = bh.run(200)
+    assert np.array_equal(cd, ch) and np.array_equal(idd, idh)
+
+
+def test_batch_error_names_the_first_bad_synapse():
+    got = []
+    for device in (True, False):
+        conf = nb.Configuration()
+        conf.set_device_construction(device)
+        networks = [batch_net(s) for s in batch_specs(6, 3, False)] + [bad_network(bad_tgt_at=11, bad_w_at=30)]
+        with pytest.raises(nb.NemoError) as e:
+            nb.Batch(networks, conf)
+        got.append((e.value.code, str(e.value)))
+    assert got[0] == got[1]
