@@ -5,8 +5,7 @@
 // -- the host build's counting sort, which keeps insertion order within a
 // row -- and a stable radix sort of the plastic synapses, taken in forward
 // order, by target gives the reverse matrix in forward order within a
-// target.  The sorts are
-// CUB's (construction is not the step loop).
+// target.  The sorts are CUB's (construction is not the step loop).
 #include "construction.hpp"
 
 #include <cub/cub.cuh>
@@ -39,7 +38,8 @@ struct Scratch {
 		CC_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
 		ptrs.push_back(p);
 		return static_cast<T*>(p);
-	}	// hands one buffer over to the caller (no longer freed here)
+	}
+	// hands one buffer over to the caller (no longer freed here)
 	template<typename T> T* release(T* p)
 	{
 		ptrs.erase(std::find(ptrs.begin(), ptrs.end(), (void*) p));
