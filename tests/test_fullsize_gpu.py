@@ -14,6 +14,10 @@ configurations.
 
 Each side runs alone and is deleted before the other is built, so that the
 host holds one copy of the network at a time.
+
+- The 256-network batch of the batched configuration, 1000 ms: every
+  network's fire stream in the batch equals its own single-network run
+  (which the parity tests above pin to the oracle's arithmetic).
 """
 import gc
 
@@ -101,3 +105,40 @@ def test_c3_mixed_plugins_full_size_2000_ms():
     assert np.array_equal(ip, io), "fired ids: " + first_difference(ip, io)
     assert same_bits(sp[0], so[0]), "IF_curr_exp state differs"
     assert same_bits(sp[1], so[1]), "Izhikevich state differs"
+
+
+def test_c4_256_network_batch_matches_individual_runs():
+    """The batched configuration at full size: 256 networks of 1,000-32,000
+    Izhikevich neurons, fan-out 100-1000, delays 1-20, input-noise sigma
+    U(2, 8) and their own generator seeds (the benchmark's networks), 1000
+    ms.  Every network's fire stream in the batch equals its own
+    single-network run, bit for bit, and the batch is built on the device."""
+    rng = np.random.default_rng(0)
+    specs = [dict(n=int(rng.integers(1000, 32001)), f=int(rng.integers(100, 1001)), seed=1000 + 17 * k,
+                  sigma=float(rng.uniform(2.0, 8.0))) for k in range(256)]
+    MS = 1000
+
+    def make(sp):
+        return nb.example_random(sp["n"], sp["f"], 20, False, seed=sp["seed"], sigma_exc=sp["sigma"],
+                                 sigma_inh=sp["sigma"])
+
+    conf = nb.Configuration()
+    singles, networks = [], []
+    for sp in specs:
+        net = make(sp)
+        sim = nb.Simulation(net, conf)
+        c, _, ids = sim.run(MS, max_ids=sp["n"] * MS // 10)
+        singles.append((c, ids))
+        del sim
+        networks.append(net)
+    batch = nb.Batch(networks, conf)
+    del networks
+    gc.collect()
+    assert batch.connectivity_digest()[1]
+    neurons = sum(sp["n"] for sp in specs)
+    counts, _, ids = batch.run(MS, max_ids=neurons * MS // 20)
+    streams = batch.streams(counts, ids)
+    bad = [k for k, ((c1, i1), (c2, i2)) in enumerate(zip(streams, singles))
+           if not (np.array_equal(c1, c2) and np.array_equal(i1, i2))]
+    assert not bad, bad[:10]
+    assert sum(int(c.sum()) for c, _ in singles) > 0
