@@ -477,14 +477,28 @@ def run_b200(args, rank, world, local):
                        else "two launches per step" + ("" if args.no_graphs else ", CUDA graphs of 100 steps")},
             "spikes_per_neuron_s": st["fired"] / args.neurons / (args.steps * W / 1e3),
         }
-        print(json.dumps(line), flush=True)
     del sim
+    if rank == 0:
+        if world == 1 and not args.no_secondary:
+            # the batched and differentiable configurations, measured in the
+            # same run (their own lines: --workload batch256 / bptt)
+            b = run_batch(args, local, emit=False)
+            d = run_bptt(args, local, emit=False, reps=5)
+            line["secondary"] = {
+                "batch256": {k: b[k] for k in ("metric", "value", "unit", "batch_ms", "sequential_ms",
+                                               "bitexact_vs_individual_runs", "mismatched_networks",
+                                               "batch_events_per_s", "batch_build_s", "launch", "clocks")},
+                "bptt": {k: d[k] for k in ("metric", "value", "unit", "adjoint_ms", "state_dtype",
+                                           "adjoint_fp32_state_ms", "torch_autograd_ms", "torch_autograd_reps",
+                                           "steps", "clocks")},
+            }
+        print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
 
 
-def run_batch(args, local):
+def run_batch(args, local, emit=True):
     """The batched configuration: networks of uneven size, each with its own
     generator seed and input-noise sigma, advanced together by one Batch,
     against the same networks run one after another as plain Simulations
@@ -571,7 +585,10 @@ def run_batch(args, local):
         "launch": {"partition": launch[0], "threads": launch[1], "autotuned_us_per_step": tuned_us},
         "batch_build_s": build_s, "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
+    del batch
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def run_floor(args, local):
@@ -602,7 +619,7 @@ def torch_sms(local):
     return torch.cuda.get_device_properties(local).multi_processor_count
 
 
-def run_bptt(args, local):
+def run_bptt(args, local, emit=True, reps=None):
     """The differentiable configuration at full size: one gradient step
     (forward + hand-written adjoint) against PyTorch float32 autograd of
     the same unrolled dynamics on the same GPU (the baseline leg)."""
@@ -637,8 +654,9 @@ def run_bptt(args, local):
         return start.elapsed_time(end) / reps
 
     with ClockSampler(local) as clk:
-        ms32 = ours(torch.float32, args.steps)
-        ms64 = ours(torch.float64, args.steps)
+        nrep = reps if reps is not None else args.steps
+        ms32 = ours(torch.float32, nrep)
+        ms64 = ours(torch.float64, nrep)
     W, a, b = net.tensors(dev)
     c, d = net.constants(dev)
     st = baseline.Structure(net.source, net.target, net.delay, N, dev)
@@ -663,11 +681,13 @@ def run_bptt(args, local):
                    "ms": T, "substeps": 4 * T, "trials": B, "readout": R, "checkpoint_ms": CK,
                    "delays_ms": [1, 10], "noise_sigma": 5.0},
         "adjoint_ms": ms64, "state_dtype": "float64", "adjoint_fp32_state_ms": ms32, "torch_autograd_ms": torch_ms,
-        "speedup_fp32_state": torch_ms / ms32, "steps": args.steps, "warmup": args.warmup,
+        "speedup_fp32_state": torch_ms / ms32, "steps": nrep, "warmup": args.warmup,
         "torch_autograd_reps": torch_reps,
         "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
@@ -687,6 +707,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--no-persistent", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="leave out the batched and differentiable configurations of the default line")
     ap.add_argument("--host-construction", action="store_true",
                     help="build the connectivity on the host instead of the device")
     ap.add_argument("--workload", choices=["headline", "batch256", "bptt", "floor"], default="headline",
