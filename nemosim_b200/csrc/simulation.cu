@@ -1403,6 +1403,17 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 // RNG streams and fire stream are those of its own single-network run.
 Simulation::Simulation(const std::vector<const Network*>& nets, const Configuration& conf)
 {
+	// a constructor that throws runs no destructor: free what was made
+	try {
+		init(nets, conf);
+	} catch(...) {
+		releaseAll();
+		throw;
+	}
+}
+
+void Simulation::init(const std::vector<const Network*>& nets, const Configuration& conf)
+{
 	if(nets.empty()) NB_THROW(NEMO_INVALID_INPUT, "no network");
 	const bool batch = nets.size() > 1;
 	// checks in the order of nemo::simulationBackend (src/nemo/nemo.cpp:109-134)
@@ -1921,11 +1932,17 @@ Simulation::Simulation(const std::vector<const Network*>& nets, const Configurat
 
 Simulation::~Simulation()
 {
+	releaseAll();
+}
+
+void Simulation::releaseAll() noexcept
+{
 	cudaSetDevice(m_device);
 	stopServe();
 	freeKept();
 	if(m_stream) cudaStreamSynchronize(m_stream);
 	for(void* p : m_allocs) cudaFree(p);
+	m_allocs.clear();
 	if(m_graph) cudaGraphExecDestroy(m_graph);
 	if(m_hCycle) cudaFreeHost(m_hCycle);
 	if(m_hBarrierError) cudaFreeHost(m_hBarrierError);
@@ -1938,7 +1955,18 @@ Simulation::~Simulation()
 	if(m_ev0) cudaEventDestroy(m_ev0);
 	if(m_ev1) cudaEventDestroy(m_ev1);
 	for(cudaEvent_t e : m_evPool) cudaEventDestroy(e);
+	m_evPool.clear();
 	if(m_stream) cudaStreamDestroy(m_stream);
+	m_graph = nullptr;
+	m_hCycle = nullptr;
+	m_hBarrierError = nullptr;
+	m_hFired = nullptr;
+	m_hFiredMapped = nullptr;
+	m_hStim = nullptr;
+	m_hServe = nullptr;
+	m_hFiredIds = nullptr;
+	m_serveEnd = m_ev0 = m_ev1 = nullptr;
+	m_stream = nullptr;
 }
 
 void Simulation::sync()

@@ -263,6 +263,8 @@ private:
 		float* dState = nullptr;
 	};
 
+	void init(const std::vector<const Network*>& nets, const Configuration& conf);
+	void releaseAll() noexcept;  // every device and host resource made so far
 	float* currentState(const HostType& t) const;
 	unsigned localIdx(unsigned g) const;
 	bool findLocal(unsigned g, unsigned* l) const;  // localIdx without throwing (one network)

@@ -279,3 +279,26 @@ def test_batch_error_names_the_first_bad_synapse():
             nb.Batch(networks, conf)
         got.append((e.value.code, str(e.value)))
     assert got[0] == got[1]
+
+
+def test_failed_construction_frees_device_memory():
+    """A simulation whose construction fails (here at its last synapse,
+    after the device arrays were allocated) frees them: five failed
+    attempts at a 20M-synapse network leave the free device memory as it
+    was."""
+    import torch
+
+    def attempt():
+        net = nb.example_random(20_000, 1000, 20, True)
+        net.add_synapse(0, 1_000_000, 1, 1.0, False)
+        with pytest.raises(nb.NemoError) as e:
+            nb.Simulation(net, nets.standard_stdp(nb))
+        assert e.value.code == nb.NEMO_INVALID_INPUT
+
+    attempt()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for _ in range(5):
+        attempt()
+    free1 = torch.cuda.mem_get_info(0)[0]
+    assert free0 - free1 < (64 << 20), (free0, free1)
