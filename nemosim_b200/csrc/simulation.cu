@@ -486,10 +486,10 @@ constexpr uint32_t PHASE_RESET = 4;    // empty the lists the next update publis
 
 // Pre-phase of a step over the lists published by the update of the step
 // with parity `pub`.  When there are both deliveries and STDP entries, the
-// CTAs split into two groups in proportion to the work (an STDP entry, two
-// dependent loads, counted as two deliveries) so that the two lists' chains
-// of dependent loads run at the same time; each list's entries are spread
-// evenly over its group's warps.  Every thread of the grid calls this.
+// warps of every CTA split into two groups in proportion to the work, so
+// that the two lists' chains of dependent loads run at the same time on
+// every SM; each list's entries are spread evenly over its group's warps
+// across the grid.  Every thread of the grid calls this.
 __device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uint32_t what)
 {
 	const unsigned long long cd = (what & PHASE_DELIVER) ? S.dlvWork.count[pub] : 0ull;
@@ -501,44 +501,47 @@ __device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uin
 		S.stdpWork.count[pub ^ 1u] = 0;
 	}
 	const uint64_t* hist = S.hist + (size_t) pub * S.N;
-	// CTAs [0, gs) take the STDP list, [gs, gridDim.x) the deliveries, in
-	// proportion to their work: an STDP entry (a load, a dependent history
-	// load for a recently active source, a reduction where its change is
-	// nonzero) costs about 2.5 deliveries (at 100k x 1000 a period took
-	// 2.5% less than with 3 and 2.4% less than with 2)
-	constexpr unsigned long long STDP_ENTRY_COST_X2 = 5;  // twice the cost, for half steps
-	uint32_t gs = ns ? gridDim.x : 0u;
+	// In every CTA, warps [0, ws) take the STDP list and [ws, wpc) the
+	// deliveries, in proportion to their work, so that every SM runs the
+	// same mix: an STDP entry (a load, a dependent history load for a
+	// recently active source, a reduction where its change is nonzero)
+	// costs about 3.5 deliveries.  At 100k x 1000 (352 x 512) a launch of
+	// 100 steps took 2098 us, against 2134 us with 2.5, 2185 with 4.5 and
+	// 2172 us when whole CTAs took one list or the other.
+	constexpr unsigned long long STDP_ENTRY_COST_X2 = 7;  // twice the cost, for half steps
+	uint32_t ws = ns ? wpc : 0u;
 	if(nd && ns) {
-		gs = (uint32_t) ((unsigned long long) gridDim.x * STDP_ENTRY_COST_X2 * ns
+		ws = (uint32_t) (((unsigned long long) wpc * STDP_ENTRY_COST_X2 * ns + (2ull * nd + STDP_ENTRY_COST_X2 * ns) / 2)
 				/ (2ull * nd + STDP_ENTRY_COST_X2 * ns));
-		gs = max(1u, min(gridDim.x - 1u, gs));
-		if(gridDim.x == 1) gs = 0;  // one CTA: it does both, deliveries first
+		ws = max(1u, min(wpc - 1u, ws));
+		if(wpc == 1) ws = 0;  // one warp: it does both, deliveries first
 	}
-	const bool doStdp = ns && (blockIdx.x < gs || gridDim.x == 1);
-	const bool doDlv = nd && (blockIdx.x >= gs || gridDim.x == 1);
-	if(doDlv) {
-		const uint32_t first = gridDim.x == 1 ? 0u : gs;
-		process_list<0, 8>(S, S.dlvWork, (uint32_t) (cd >> 32), nd, hist, nullptr, (blockIdx.x - first) * wpc + lw,
-				(gridDim.x - first) * wpc);
+	const bool stdpWarp = ns && (lw < ws || wpc == 1);
+	const bool dlvWarp = nd && (lw >= ws || wpc == 1);
+	if(dlvWarp) {
+		const uint32_t dw = wpc == 1 ? 1u : wpc - ws, first = wpc == 1 ? 0u : ws;
+		process_list<0, 8>(S, S.dlvWork, (uint32_t) (cd >> 32), nd, hist, nullptr, blockIdx.x * dw + (lw - first),
+				gridDim.x * dw);
 	}
 	// the sources' "fired in the last 64 steps" bits, copied to shared
-	// memory with asynchronous 16-byte copies
+	// memory by the STDP warps with asynchronous 16-byte copies; they then
+	// wait for each other only (named barrier 1)
 	extern __shared__ __align__(16) uint32_t sRecent[];
-	const bool filter = doStdp && S.recentBytes;
-	if(filter) {
-		const uint32_t* g = S.recent + (size_t) pub * S.recentWords;
-		for(uint32_t q = threadIdx.x; q < S.recentWords / 4; q += blockDim.x) {
-			const uint32_t dst = (uint32_t) __cvta_generic_to_shared(sRecent + 4 * q);
-			asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(g + 4 * q) : "memory");
+	if(stdpWarp) {
+		const uint32_t sw = wpc == 1 ? 1u : ws;
+		const bool filter = S.recentBytes != 0;
+		if(filter) {
+			const uint32_t* g = S.recent + (size_t) pub * S.recentWords;
+			for(uint32_t q = threadIdx.x; q < S.recentWords / 4; q += sw * 32) {
+				const uint32_t dst = (uint32_t) __cvta_generic_to_shared(sRecent + 4 * q);
+				asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(g + 4 * q) : "memory");
+			}
+			asm volatile("cp.async.commit_group;" ::: "memory");
+			asm volatile("cp.async.wait_all;" ::: "memory");
+			asm volatile("bar.sync 1, %0;" :: "r"(sw * 32) : "memory");
 		}
-		asm volatile("cp.async.commit_group;" ::: "memory");
-		asm volatile("cp.async.wait_all;" ::: "memory");
-	}
-	__syncthreads();
-	if(doStdp) {
-		const uint32_t cstdp = gridDim.x == 1 ? 1u : gs;
 		process_list<1, 4>(S, S.stdpWork, (uint32_t) (cs >> 32), ns, hist, filter ? sRecent : nullptr,
-				blockIdx.x * wpc + lw, cstdp * wpc);
+				blockIdx.x * sw + lw, gridDim.x * sw);
 	}
 	__syncthreads();  // the shared copy is rewritten by the next call
 }
