@@ -329,9 +329,10 @@ NEMO_B200_API nemo_status_t nemo_b200_set_wait_limit(nemo_simulation_t, unsigned
 /* Where a simulation created with this configuration builds its
  * connectivity (the forward matrix sorted by source and delay, its delay
  * groups, the reverse matrix of plastic synapses): on = 1 (the default)
- * builds it on the device when the network allows it -- one network, global
+ * builds it on the device when the networks allow it -- one network, or a
+ * batch whose networks have one neuron type each; per network global
  * neuron ids below 4 per neuron plus 2^20, fewer than 2^31 - 1 synapses
- * and neurons x maximum delay, no neuron type that reads the reverse
+ * and neurons x maximum delay; no neuron type that reads the reverse
  * matrix of all synapses -- and on the host otherwise; on = 0 always builds
  * it on the host.  Both builds give the same bytes, the same errors and the
  * same results. */
