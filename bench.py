@@ -461,9 +461,8 @@ def run_b200(args, rank, world, local):
                     "sim_ms_per_s": ke * W / e2e_s, "fired_per_ms": fired_total / (ke * W),
                     "python_step_us": py_step_us},
             # per period: the persistent loop (or 100 update + deliver launches,
-            # plus the graph's cycle-counter kernel), then applyStdp's collect
-            # and apply kernels
-            "gpu_launches": args.steps * ((1 if persistent else 2 * W + (W // 100)) + 2),
+            # plus the graph's cycle-counter kernel), then applyStdp's kernel
+            "gpu_launches": args.steps * ((1 if persistent else 2 * W + (W // 100)) + 1),
             "clocks": clk.summary(),
             # network generation (the random example's own loop, on the host)
             # and the simulation's construction from it, both untimed

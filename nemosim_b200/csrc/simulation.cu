@@ -997,34 +997,16 @@ static const void* serve_kernel_for(uint32_t threads)
 			: (const void*) serve_kernel<RUN_THREADS, 1>;
 }
 
-// Compacts the targets touched since the last applyStdp (a bit-vector) into
-// a list and clears the bit-vector: one warp per word, one atomic per warp.
-__global__ void __launch_bounds__(STEP_THREADS)
-collect_touched_kernel(const DevSim S)
-{
-	const uint32_t stride = gridDim.x * blockDim.x;
-	const uint32_t lane = threadIdx.x & 31;
-	const uint32_t end = S.W * 32;  // whole warps: n >> 5 is the warp's word
-	for(uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < end; n += stride) {
-		const uint32_t word = S.touchedBits[n >> 5];
-		if(!word) continue;
-		uint32_t base = 0;
-		if(lane == 0) {
-			base = atomicAdd(S.touchedCount, (uint32_t) __popc(word));
-			S.touchedBits[n >> 5] = 0u;
-		}
-		base = __shfl_sync(0xffffffffu, base, 0);
-		if((word >> lane) & 1u) S.touchedList[base + __popc(word & ((1u << lane) - 1u))] = n;
-	}
-}
-
 // applyStdp (src/nemo/ConnectivityMatrix.cpp:241-294): w' =
 // updatedWeight(w, reward x acc) for every incoming plastic synapse of the
 // touched targets (the only ones whose accumulator can be nonzero), written
 // back to the forward matrix when it changed, and the accumulator cleared.
 // ALL: every target, whatever its accumulator -- the first call, which also
 // clamps weights that start outside their range.  Work items are (slice,
-// 32 targets), slice-major; a warp flattens its 32 runs with a scan and
+// 32 consecutive targets: one word of the touched bit-vector), slice-major;
+// lanes whose target is untouched take an empty run (walking the word
+// directly costs less than compacting the touched targets into a list
+// first).  A warp flattens its 32 runs with a scan and
 // finds each entry's run with a 5-step shuffle search.  The targets of the
 // warp's item after next and the runs of its next item are loaded while an
 // item is processed (at 5 CTAs of 256 threads per SM: 48 registers, no
@@ -1035,16 +1017,18 @@ apply_kernel(const DevSim S, int32_t reward)
 {
 	const uint32_t FULL = 0xffffffffu;
 	const uint32_t lane = threadIdx.x & 31;
-	const uint32_t nT = ALL ? S.N : *S.touchedCount;
-	const uint32_t batches = (nT + 31) >> 5;
+	const uint32_t batches = S.W;  // words of 32 targets
 	const unsigned long long items = (unsigned long long) batches * S.applySlices;
 	const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
 	// lane's target of item ii (N: none)
 	auto target_of = [&](unsigned long long ii) -> uint32_t {
 		if(ii >= items) return S.N;
 		const uint32_t kk = (uint32_t) (ii / batches);
-		const uint32_t jj = (uint32_t) (ii - (unsigned long long) kk * batches) * 32 + lane;
-		return jj < nT ? (ALL ? jj : S.touchedList[jj]) : S.N;
+		const uint32_t w = (uint32_t) (ii - (unsigned long long) kk * batches);
+		const uint32_t t = w * 32 + lane;
+		if(t >= S.N) return S.N;
+		if(ALL) return t;
+		return (S.touchedBits[w] >> lane) & 1u ? t : S.N;
 	};
 	// lane's run of item ii for target t
 	auto run_of = [&](unsigned long long ii, uint32_t t, unsigned long long& lo, uint32_t& len) {
@@ -1822,8 +1806,6 @@ void Simulation::init(const std::vector<const Network*>& nets, const Configurati
 		makeList(S.dlvWork, dlvGroups, Sn);
 		m_dlvGroups = dlvGroups;
 		makeList(S.stdpWork, N, plastic);
-		S.touchedList = dalloc<uint32_t>(N);
-		S.touchedCount = dalloc<uint32_t>(1);
 	}
 	// applyStdp's slices of the forward matrix and each target's run in each
 	if(conf.stdp) {
@@ -2394,14 +2376,10 @@ void Simulation::applyStdpDevice(int32_t R)
 {
 	stopServe();
 	flushStdp();
-	const bool fullPassDone = m_weightsClamped;
 	timedBegin(K_APPLY);
 	if(!m_weightsClamped) {
 		apply_kernel<true><<<m_applyGrid, STEP_THREADS, 0, m_stream>>>(m_dev, R);
 	} else {
-		const unsigned cgrid = std::max(1u, std::min<unsigned>((m_dev.W * 32 + STEP_THREADS - 1) / STEP_THREADS,
-				(unsigned) m_sms * 8));
-		collect_touched_kernel<<<cgrid, STEP_THREADS, 0, m_stream>>>(m_dev);
 		apply_kernel<false><<<m_applyGrid, STEP_THREADS, 0, m_stream>>>(m_dev, R);
 	}
 	timedEnd();
@@ -2409,8 +2387,7 @@ void Simulation::applyStdpDevice(int32_t R)
 	// class, so after one full pass every plastic weight does, and only the
 	// synapses of touched targets can change
 	m_weightsClamped = true;
-	NB_CUDA(cudaMemsetAsync(m_dev.touchedCount, 0, 4, m_stream));
-	if(!fullPassDone) NB_CUDA(cudaMemsetAsync(m_dev.touchedBits, 0, (size_t) m_dev.W * 4, m_stream));
+	NB_CUDA(cudaMemsetAsync(m_dev.touchedBits, 0, (size_t) m_dev.W * 4, m_stream));
 }
 
 /* ConnectivityMatrix::applyStdp argument checks (src/nemo/ConnectivityMatrix.cpp:241-259) */
@@ -2588,7 +2565,6 @@ float Simulation::autotune(unsigned trialSteps)
 		regions.emplace_back(L->count, 16);
 	}
 	if(m_dev.stdp) regions.emplace_back(m_dev.rcmAcc, (size_t) lastPlastic * 4);
-	regions.emplace_back(m_dev.touchedCount, 4);
 	regions.emplace_back(m_dev.touchedBits, (size_t) m_dev.W * 4);
 	std::vector<void*> backup;
 	for(auto& r : regions) {

@@ -147,8 +147,6 @@ struct DevSim {
 	// synapses of its STDP targets (ranges of the reverse matrix)
 	WorkList dlvWork, stdpWork;
 	uint32_t* touchedBits;    // [W] STDP targets since the last applyStdp
-	uint32_t* touchedList;    // [N] applyStdp's compacted touched targets
-	uint32_t* touchedCount;
 	unsigned long long* cycleDev; // step counter read by kernels replayed from a CUDA graph
 	StdpParams sp;
 	LibmCalib calib;
