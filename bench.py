@@ -217,6 +217,23 @@ def barrier(world: int):
         dist.barrier()
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (Linux), for the CPU-baseline records."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# what the CPU baseline parallelises: the reference's OpenMP loops (the
+# neuron updates); delivery and STDP accumulation are serial loops there
+CPU_THREADS_NOTE = "neuron updates on OpenMP threads; delivery and STDP accumulation serial, as in the reference"
+
+
 def cpu_sample(neurons: int, warm_ms: int, ms: int, stdp_period: int = WINDOW_MS) -> dict:
     """Time the oracle (the reference CPU backend restated, OpenMP on the
     neuron update as in the reference) on the same network."""
@@ -268,7 +285,8 @@ def run_reference(args, rank, world):
         "sim_ms_per_s": args.steps * window / el,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{args.steps} steps of {window} simulated ms (+applyStdp) after "
-                                   f"{args.warmup} warm-up steps; network build {build_s:.1f} s untimed"},
+                                   f"{args.warmup} warm-up steps; network build {build_s:.1f} s untimed",
+                         "cpu_model": cpu_model(), "threads": CPU_THREADS_NOTE},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -436,7 +454,7 @@ def run_b200(args, rank, world, local):
         cpu = {"value": c["events_per_s"], "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                "sample": f"{args.cpu_ms} simulated ms (after {args.cpu_warm_ms} warm-up ms) of the same "
                          f"network on the oracle; build {c['build_s']:.0f} s untimed",
-               "sim_ms_per_s": c["sim_ms_per_s"]}
+               "sim_ms_per_s": c["sim_ms_per_s"], "cpu_model": cpu_model(), "threads": CPU_THREADS_NOTE}
 
     if rank == 0:
         line = {
