@@ -97,14 +97,15 @@ __global__ void map_kernel(size_t S, const unsigned* src, const unsigned* tgt, c
 	}
 }
 
-// syn: the network's part of the union forward matrix; pos: each synapse's
+// synTgt, synW: the network's part of the union forward matrix; pos: each synapse's
 // place in it
 __global__ void fill_forward_kernel(size_t S, const uint32_t* sortedIdx, const uint32_t* lt, const unsigned* delay,
-		const int32_t* fx, uint2* syn, uint32_t* pos)
+		const int32_t* fx, uint32_t* synTgt, uint32_t* synW, uint32_t* pos)
 {
 	for(size_t p = blockIdx.x * (size_t) blockDim.x + threadIdx.x; p < S; p += (size_t) gridDim.x * blockDim.x) {
 		const uint32_t k = sortedIdx[p];
-		syn[p] = make_uint2(lt[k] | ((delay[k] - 1) << 26), (uint32_t) fx[k]);
+		synTgt[p] = lt[k] | ((delay[k] - 1) << 26);
+		synW[p] = (uint32_t) fx[k];
 		pos[k] = (uint32_t) p;
 	}
 }
@@ -156,11 +157,11 @@ __global__ void compact_kernel(size_t S, const uint32_t* flag, const uint32_t* a
 }
 
 // key2: the plastic entry's target relative to the network's first neuron
-__global__ void plastic_keys_kernel(size_t P, const uint32_t* plf, const uint2* syn, uint32_t srcBase,
+__global__ void plastic_keys_kernel(size_t P, const uint32_t* plf, const uint32_t* synTgt, uint32_t srcBase,
 		uint32_t* key2, uint32_t* tgtCount)
 {
 	for(size_t q = blockIdx.x * (size_t) blockDim.x + threadIdx.x; q < P; q += (size_t) gridDim.x * blockDim.x) {
-		const uint32_t t = (syn[plf[q]].x & TARGET_MASK) - srcBase;
+		const uint32_t t = (synTgt[plf[q]] & TARGET_MASK) - srcBase;
 		key2[q] = t;
 		atomicAdd(tgtCount + t, 1u);
 	}
@@ -168,11 +169,11 @@ __global__ void plastic_keys_kernel(size_t P, const uint32_t* plf, const uint2* 
 
 // rsrc, rfwd: the network's part of the union reverse matrix
 __global__ void fill_reverse_kernel(size_t P, const uint32_t* sortedPlf, const uint32_t* sortedIdx,
-		const uint32_t* ls, const uint2* syn, uint64_t synOff, uint32_t* rsrc, uint32_t* rfwd)
+		const uint32_t* ls, const uint32_t* synTgt, uint64_t synOff, uint32_t* rsrc, uint32_t* rfwd)
 {
 	for(size_t q = blockIdx.x * (size_t) blockDim.x + threadIdx.x; q < P; q += (size_t) gridDim.x * blockDim.x) {
 		const uint32_t p = sortedPlf[q];
-		rsrc[q] = ls[sortedIdx[p]] | (syn[p].x & ~TARGET_MASK);
+		rsrc[q] = ls[sortedIdx[p]] | (synTgt[p] & ~TARGET_MASK);
 		rfwd[q] = (uint32_t) (synOff + p);
 	}
 }
@@ -276,9 +277,10 @@ void construct_on_device(DeviceConstruction& c, cudaStream_t st)
 	tmp = scratch.get<uint8_t>(tmpBytes);
 	CC_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmpBytes, key, keySorted, idx, idxSorted, (int) S, 0, keyBits, st));
 
-	uint2* syn = c.syn + c.synOff;
+	uint32_t* synTgt = c.synTgt + c.synOff;
+	uint32_t* synW = c.synW + c.synOff;
 	uint32_t* pos = scratch.get<uint32_t>(S);
-	fill_forward_kernel<<<blocks(S), THREADS, 0, st>>>(S, idxSorted, lt, dly, fx, syn, pos);
+	fill_forward_kernel<<<blocks(S), THREADS, 0, st>>>(S, idxSorted, lt, dly, fx, synTgt, synW, pos);
 	CC_CUDA(cudaGetLastError());
 
 	// delay groups
@@ -318,7 +320,7 @@ void construct_on_device(DeviceConstruction& c, cudaStream_t st)
 		uint32_t* tgtCount = scratch.get<uint32_t>((size_t) N + 1);
 		uint32_t* tgtStart = scratch.get<uint32_t>((size_t) N + 1);
 		CC_CUDA(cudaMemsetAsync(tgtCount, 0, ((size_t) N + 1) * 4, st));
-		plastic_keys_kernel<<<blocks(P), THREADS, 0, st>>>(P, plk, syn, c.srcBase, key2, tgtCount);
+		plastic_keys_kernel<<<blocks(P), THREADS, 0, st>>>(P, plk, synTgt, c.srcBase, key2, tgtCount);
 		CC_CUDA(cudaGetLastError());
 		tmpBytes = 0;
 		CC_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmpBytes, tgtCount, tgtStart, (int) N + 1, st));
@@ -334,7 +336,7 @@ void construct_on_device(DeviceConstruction& c, cudaStream_t st)
 		tmp = scratch.get<uint8_t>(tmpBytes);
 		CC_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmpBytes, key2, key2Sorted, plk, plkSorted, (int) P, 0, tBits,
 				st));
-		fill_reverse_kernel<<<blocks(P), THREADS, 0, st>>>(P, plkSorted, idxSorted, ls, syn, c.synOff,
+		fill_reverse_kernel<<<blocks(P), THREADS, 0, st>>>(P, plkSorted, idxSorted, ls, synTgt, c.synOff,
 				c.rcmSrc + c.plOff, c.rcmFwd + c.plOff);
 		CC_CUDA(cudaGetLastError());
 		std::vector<uint32_t> hs((size_t) N + 1);

@@ -43,13 +43,14 @@ struct DeviceConstruction {
 	uint64_t plOff = 0;    // its first entry in the union reverse matrix
 
 	// the union arrays (device memory, allocated by the caller)
-	uint2* syn = nullptr;                  // {target | (delay - 1) << 26, weight}
+	uint32_t* synTgt = nullptr;            // target | (delay - 1) << 26
+	uint32_t* synW = nullptr;              // weight
 	unsigned long long* outPtr = nullptr;  // [N + 1] (the caller sets entry N)
 	uint16_t* dEnd16 = nullptr;            // [N][D] when every row is shorter than 65536
 	uint32_t* dEnd32 = nullptr;            // [N][D] otherwise
 	uint64_t* delayMask = nullptr;         // [N]
 	uint32_t* rcmSrc = nullptr;            // source | (delay - 1) << 26
-	uint32_t* rcmFwd = nullptr;            // index into syn
+	uint32_t* rcmFwd = nullptr;            // index into the forward matrix
 
 	// outputs: the network's row starts in the union arrays ([nLocal] each),
 	// its delay groups and plastic synapses
@@ -58,7 +59,7 @@ struct DeviceConstruction {
 	uint64_t plastic_count = 0;
 	// kept on the device for the synapse queries, which build their host
 	// tables from them on first use (cudaMalloc'd, freed by the caller):
-	// local source, position in syn, global target, delay and plasticity
+	// local source, position in the forward matrix, global target, delay and plasticity
 	// per synapse in insertion order
 	uint32_t* keptSrc = nullptr;
 	uint32_t* keptPos = nullptr;

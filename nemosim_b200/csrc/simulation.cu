@@ -425,7 +425,7 @@ __device__ __forceinline__ void process_list(const DevSim& S, const WorkList& L,
 		const uint32_t coverEnd = __shfl_sync(0xffffffffu, d.w + d.z, lastLane);
 		const uint32_t lo = max(E0, __shfl_sync(0xffffffffu, d.w, 0)), hi = min(E1, coverEnd);
 		for(uint32_t base = lo; base < hi; base += 32 * K) {
-			// entry indices into syn / the reverse matrix, both shorter than
+			// entry indices into the forward / the reverse matrix, both shorter than
 			// 2^32 entries (checked when the simulation is built)
 			uint32_t idx[K];
 #pragma unroll
@@ -439,14 +439,19 @@ __device__ __forceinline__ void process_list(const DevSim& S, const WorkList& L,
 				idx[j] = __shfl_sync(0xffffffffu, d.x, q) + (e - __shfl_sync(0xffffffffu, d.w, q));
 			}
 			if(KIND == 0) {
-				uint2 sy[K];
-#pragma unroll
-				for(int j = 0; j < K; ++j) if(base + lane + 32 * j < hi) sy[j] = __ldcs(S.syn + idx[j]);
+				uint32_t tg[K], wt[K];
 #pragma unroll
 				for(int j = 0; j < K; ++j) {
 					if(base + lane + 32 * j < hi) {
-						const int32_t w = (int32_t) sy[j].y;
-						unsigned long long* a = reinterpret_cast<unsigned long long*>(S.slot + (sy[j].x & (MAX_NEURONS - 1)));
+						tg[j] = __ldcs(S.synTgt + idx[j]);
+						wt[j] = __ldcs(S.synW + idx[j]);
+					}
+				}
+#pragma unroll
+				for(int j = 0; j < K; ++j) {
+					if(base + lane + 32 * j < hi) {
+						const int32_t w = (int32_t) wt[j];
+						unsigned long long* a = reinterpret_cast<unsigned long long*>(S.slot + (tg[j] & (MAX_NEURONS - 1)));
 						red_add_u64(a + (w >= 0 ? 0 : 1), (unsigned long long) (long long) w);
 					}
 				}
@@ -520,7 +525,10 @@ __device__ __forceinline__ void deliver_range(const DevSim& S, uint32_t pub, uin
 	const bool dlvWarp = nd && (lw >= ws || wpc == 1);
 	if(dlvWarp) {
 		const uint32_t dw = wpc == 1 ? 1u : wpc - ws, first = wpc == 1 ? 0u : ws;
-		process_list<0, 8>(S, S.dlvWork, (uint32_t) (cd >> 32), nd, hist, nullptr, blockIdx.x * dw + (lw - first),
+		// four entries a lane per round: eight loads (target and weight)
+		// in flight, and no spills in the 64-register instance of the
+		// persistent loop, which at eight entries spilled inside this loop
+		process_list<0, 4>(S, S.dlvWork, (uint32_t) (cd >> 32), nd, hist, nullptr, blockIdx.x * dw + (lw - first),
 				gridDim.x * dw);
 	}
 	// the sources' "fired in the last 64 steps" bits, copied to shared
@@ -1082,12 +1090,12 @@ apply_kernel(const DevSim S, int32_t reward)
 			for(uint32_t q = 0; q < APPLY_ILP; ++q) live[q] = off + lane + 32 * q < total && (ALL || acc[q] != 0);
 			int32_t w[APPLY_ILP];
 #pragma unroll
-			for(uint32_t q = 0; q < APPLY_ILP; ++q) w[q] = live[q] ? (int32_t) S.syn[fwd[q]].y : 0;
+			for(uint32_t q = 0; q < APPLY_ILP; ++q) w[q] = live[q] ? (int32_t) S.synW[fwd[q]] : 0;
 #pragma unroll
 			for(uint32_t q = 0; q < APPLY_ILP; ++q) {
 				if(!live[q]) continue;
 				const int32_t nw2 = stdp_updated_weight(S.sp, w[q], fx_mul_dev(reward, acc[q]));
-				if(nw2 != w[q]) S.syn[fwd[q]].y = (uint32_t) nw2;
+				if(nw2 != w[q]) S.synW[fwd[q]] = (uint32_t) nw2;
 				if(acc[q]) S.rcmAcc[e[q]] = 0;
 			}
 		}
@@ -1699,16 +1707,20 @@ void Simulation::init(const std::vector<const Network*>& nets, const Configurati
 			for(size_t k = 0; k < Sn; ++k) pos[k] = rowStart[(size_t) lsrc[k] * D + sdelay[k] - 1]++;
 		}
 		{
-			hvector<uint2> syn(Sn);
+			hvector<uint32_t> synTgt(Sn), synW(Sn);
 			for(size_t k = 0; k < Sn; ++k) {
-				syn[pos[k]] = make_uint2(ltgt[k] | ((sdelay[k] - 1) << 26), (uint32_t) fxw[k]);
+				synTgt[pos[k]] = ltgt[k] | ((sdelay[k] - 1) << 26);
+				synW[pos[k]] = (uint32_t) fxw[k];
 			}
 			auto* dOut = dalloc<unsigned long long>(N + 1);
-			auto* dSyn = dalloc<uint2>(Sn);
+			auto* dTgt = dalloc<uint32_t>(Sn);
+			auto* dW = dalloc<uint32_t>(Sn);
 			NB_CUDA(cudaMemcpyAsync(dOut, outPtr.data(), (N + 1) * 8, cudaMemcpyHostToDevice, m_stream));
-			NB_CUDA(cudaMemcpyAsync(dSyn, syn.data(), Sn * 8, cudaMemcpyHostToDevice, m_stream));
+			NB_CUDA(cudaMemcpyAsync(dTgt, synTgt.data(), Sn * 4, cudaMemcpyHostToDevice, m_stream));
+			NB_CUDA(cudaMemcpyAsync(dW, synW.data(), Sn * 4, cudaMemcpyHostToDevice, m_stream));
 			S.outPtr = dOut;
-			S.syn = dSyn;
+			S.synTgt = dTgt;
+			S.synW = dW;
 			NB_CUDA(cudaStreamSynchronize(m_stream));
 		}
 
@@ -2843,7 +2855,8 @@ void Simulation::buildOnDevice(const std::vector<const Network*>& nets, std::vec
 		for(const auto& kv : nets[i]->axonCount) maxOut = std::max(maxOut, kv.second);
 		P += parts[i].plastic;
 	}
-	uint2* syn = dalloc<uint2>(m_nsyn);
+	uint32_t* synTgt = dalloc<uint32_t>(m_nsyn);
+	uint32_t* synW = dalloc<uint32_t>(m_nsyn);
 	auto* dOut = dalloc<unsigned long long>((size_t) N + 1);
 	uint16_t* end16 = maxOut < 65536 ? dalloc<uint16_t>((size_t) N * D) : nullptr;
 	uint32_t* end32 = maxOut < 65536 ? nullptr : dalloc<uint32_t>((size_t) N * D);
@@ -2873,7 +2886,8 @@ void Simulation::buildOnDevice(const std::vector<const Network*>& nets, std::vec
 		c.keepQueries = !m_writeOnly && nets.size() == 1;
 		c.synOff = part.synOff;
 		c.plOff = part.plOff;
-		c.syn = syn;
+		c.synTgt = synTgt;
+		c.synW = synW;
 		c.outPtr = dOut;
 		c.dEnd16 = end16;
 		c.dEnd32 = end32;
@@ -2899,7 +2913,8 @@ void Simulation::buildOnDevice(const std::vector<const Network*>& nets, std::vec
 	outPtr[N] = m_nsyn;
 	rcmPtr[N] = P;
 	NB_CUDA(cudaMemcpyAsync(dOut + N, &outPtr[N], 8, cudaMemcpyHostToDevice, m_stream));
-	S.syn = syn;
+	S.synTgt = synTgt;
+	S.synW = synW;
 	S.outPtr = dOut;
 	S.dEnd16 = end16;
 	S.dEnd32 = end32;
@@ -2969,7 +2984,8 @@ void Simulation::connectivityDigest(uint64_t out[DIGESTS])
 	const DevSim& S = m_dev;
 	const size_t N = m_N, P = lastPlastic;
 	const size_t rows = N * S.dStride;
-	out[0] = device_digest(S.syn, m_nsyn * 8, m_stream);
+	out[0] = device_digest(S.synTgt, m_nsyn * 4, m_stream)
+			+ 0x9E3779B97F4A7C15ull * device_digest(S.synW, m_nsyn * 4, m_stream);
 	out[1] = device_digest(S.outPtr, (N + 1) * 8, m_stream);
 	out[2] = S.dEnd16 ? device_digest(S.dEnd16, rows * 2, m_stream) : device_digest(S.dEnd32, rows * 4, m_stream) ^ 1;
 	out[3] = device_digest(S.delayMask, N * 8, m_stream);
@@ -3017,11 +3033,11 @@ unsigned char Simulation::getSynapsePlastic(uint64_t id) { return m_synPlastic[s
 float Simulation::getSynapseWeight(uint64_t id)
 {
 	size_t k = synapseKey(id);
-	uint2 s;
+	uint32_t w = 0;
 	NB_CUDA(cudaSetDevice(m_device));
-	NB_CUDA(cudaMemcpyAsync(&s, m_dev.syn + m_pos[k], 8, cudaMemcpyDeviceToHost, m_stream));
+	NB_CUDA(cudaMemcpyAsync(&w, m_dev.synW + m_pos[k], 4, cudaMemcpyDeviceToHost, m_stream));
 	sync();
-	return fx_toFloat((int32_t) s.y);
+	return fx_toFloat((int32_t) w);
 }
 
 void Simulation::getWeightsFx(int32_t* out, size_t cap, size_t* len)
@@ -3029,9 +3045,9 @@ void Simulation::getWeightsFx(int32_t* out, size_t cap, size_t* len)
 	if(m_writeOnly) NB_THROW(NEMO_INVALID_INPUT, "Cannot read synapse state if simulation configured with write-only synapses");
 	if(cap < m_nsyn) NB_THROW(NEMO_BUFFER_OVERFLOW, "weight buffer too small");
 	ensureQueryTables();
-	std::vector<uint2> syn(m_nsyn);
+	std::vector<uint32_t> w(m_nsyn);
 	NB_CUDA(cudaSetDevice(m_device));
-	NB_CUDA(cudaMemcpyAsync(syn.data(), m_dev.syn, m_nsyn * 8, cudaMemcpyDeviceToHost, m_stream));
+	NB_CUDA(cudaMemcpyAsync(w.data(), m_dev.synW, m_nsyn * 4, cudaMemcpyDeviceToHost, m_stream));
 	sync();
 	// network iteration order: sources by ascending global id
 	std::vector<unsigned> sources(m_N);
@@ -3040,7 +3056,7 @@ void Simulation::getWeightsFx(int32_t* out, size_t cap, size_t* len)
 	size_t o = 0;
 	for(unsigned l : sources) {
 		for(uint64_t j = m_srcStart[l]; j < m_srcStart[l + 1]; ++j) {
-			out[o++] = (int32_t) syn[m_pos[m_srcOrder[j]]].y;
+			out[o++] = (int32_t) w[m_pos[m_srcOrder[j]]];
 		}
 	}
 	*len = o;

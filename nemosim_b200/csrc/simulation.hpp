@@ -110,7 +110,8 @@ struct DevSim {
 	float* curExt;            // [N] pending current stimulus
 	ulonglong2* slot;         // [N] int64 E and I fixed-point sums (two's complement) of this step's arrivals
 	const unsigned long long* outPtr; // [N+1] outgoing synapses per source, sorted by delay
-	uint2* syn;               // [S] {target | (delay - 1) << 26, weight}
+	uint32_t* synTgt;         // [S] target | (delay - 1) << 26
+	uint32_t* synW;           // [S] weight (Q11.20), apart from the targets: applyStdp moves 4 bytes a synapse
 	// delay groups: bit d - 1 of delayMask[n] is set when source n has
 	// synapses of delay d that deliverSpikes delivers; dEnd[n][d - 1] is the
 	// end of its delay-d group within its row (uint16 when every row is
@@ -129,7 +130,7 @@ struct DevSim {
 	// reverse matrix of plastic synapses: per target, sorted by forward index
 	const unsigned long long* rcmPtr; // [N+1] incoming plastic synapses per target
 	const uint32_t* rcmSrc;   // source | (delay - 1) << 26
-	const uint32_t* rcmFwd;   // index into syn
+	const uint32_t* rcmFwd;   // index into the forward matrix (synTgt, synW)
 	int32_t* rcmAcc;          // STDP accumulator per incoming plastic synapse
 	// applyStdp's slices of the forward matrix: rcmSlice[k][t] is the offset
 	// within target t's entries of the first one whose forward index is at
@@ -143,7 +144,7 @@ struct DevSim {
 	const uint32_t* allSrc;
 	const float* allW;
 	// work published by a step's update for the next pre-phase: the delay
-	// groups arriving next step (ranges of syn) and the incoming plastic
+	// groups arriving next step (ranges of the forward matrix) and the incoming plastic
 	// synapses of its STDP targets (ranges of the reverse matrix)
 	WorkList dlvWork, stdpWork;
 	uint32_t* touchedBits;    // [W] STDP targets since the last applyStdp
