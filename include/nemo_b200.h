@@ -338,9 +338,10 @@ NEMO_B200_API nemo_status_t nemo_b200_set_wait_limit(nemo_simulation_t, unsigned
  * same results. */
 NEMO_B200_API nemo_status_t nemo_b200_set_device_construction(nemo_configuration_t, int on);
 /* Digests of the simulation's connectivity as it sits in device memory:
- * out[0..7] hash the forward matrix, its row starts, the delay-group ends,
- * the per-source delay masks, and the reverse matrix of plastic synapses
- * (row starts, sources, forward indices, weights); out[8] is the number of
+ * out[0..7] hash the forward matrix (targets and weights), its row starts,
+ * the delay-group ends, the per-source delay masks, the reverse matrix of
+ * plastic synapses (row starts, sources, forward indices) and applyStdp's
+ * table of each target's runs per slice; out[8] is the number of
  * delay groups and out[9] is 1 when the device built it.  Two simulations
  * with equal out[0..8] hold the same bytes. */
 NEMO_B200_API nemo_status_t nemo_b200_connectivity_digest(nemo_simulation_t, uint64_t out[10]);
