@@ -468,10 +468,12 @@ def run_b200(args, rank, world, local):
                          "kernel": dominant, "alg_bytes_per_launch": alg_bytes,
                          "avg_launch_us": step_ms * 1e3, "kernels": per_kernel},
             "cpu_baseline": cpu,
-            # nemo_step through the resident loop: per ms a 4-byte stimulus and
-            # a 16-byte request in, the fired ids and a 16-byte reply out (two
-            # launches: the fired bit-vector out instead)
-            "e2e": {"value": e2e_events / e2e_s, "unit": UNIT, "h2d_bytes_per_step": (4 + 16) * W,
+            # nemo_step through the resident loop: per ms a 16-byte request
+            # and the one-neuron stimulus in its line (8 bytes) in, the fired
+            # ids and a 16-byte reply out (two launches: a 4-byte stimulus in
+            # and the fired bit-vector out instead)
+            "e2e": {"value": e2e_events / e2e_s, "unit": UNIT,
+                    "h2d_bytes_per_step": (8 + 16) * W if resident else (4 + 16) * W,
                     "d2h_bytes_per_step": (round(4 * fired_total / ke) + 16 * W) if resident else 4 * words * W,
                     "api": "nemo_step + nemo_apply_stdp (C ABI), loop in C (nemo_b200_bench_step_loop)",
                     "python_loop_value": py_loop_events / py_loop_s,

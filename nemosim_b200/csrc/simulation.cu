@@ -943,28 +943,52 @@ serve_kernel(const DevSim S, uint32_t P, unsigned long long cycle0, GridBarrier*
 		// other CTAs finished the last step at its final barrier)
 		uint32_t op;
 		if(blockIdx.x == 0) {
-			if(threadIdx.x == 0) {
+			if(threadIdx.x < 32) {
+				// warp 0 reads the request line -- the two request words and
+				// the inline stimulus -- in one 64-byte read per poll
+				const uint32_t FULL = 0xffffffffu, lane = threadIdx.x;
+				const unsigned long long* line = &ctl->req[0];
 				op = 0;
 				const unsigned long long t0 = global_ns();
 				for(uint32_t polls = 0; polls < SERVE_POLL_LIMIT; ++polls) {
-					// both words in one round trip
-					const unsigned long long a = ld_relaxed_sys_u64(&ctl->req[0]);
-					const unsigned long long b = ld_relaxed_sys_u64(&ctl->req[1]);
-					if((uint32_t) (a >> 32) == want && (uint32_t) (b >> 32) == want) {
+					const unsigned long long w = lane < 2 + SERVE_INLINE ? ld_relaxed_sys_u64(line + lane) : 0ull;
+					const unsigned long long a = __shfl_sync(FULL, w, 0);
+					const unsigned long long b = __shfl_sync(FULL, w, 1);
+					bool got = (uint32_t) (a >> 32) == want && (uint32_t) (b >> 32) == want;
+					const bool inl = got && ((uint32_t) a & SERVE_INLINE_FLAG) != 0u;
+					const uint32_t count = (uint32_t) a & ~SERVE_INLINE_FLAG;
+					const bool mine = inl && lane >= 2 && lane - 2 < count;
+					if(inl) got = __all_sync(FULL, !mine || (uint32_t) (w >> 32) == want);
+					if(got) {
 						// the stimulus the host wrote before the request
 						asm volatile("fence.acq_rel.sys;" ::: "memory");
-						gb->nf = (uint32_t) a;
-						gb->ni = (uint32_t) b;
-						S.eventCount[ring] = 0;
+						// an inline firing stimulus is applied here; the step's
+						// first grid barrier orders it before the update reads it
+						if(mine) {
+							const uint32_t l = (uint32_t) w;
+							atomicOr(&S.fstim[l >> 5], 1u << (l & 31));
+						}
+						if(lane == 0) {
+							gb->nf = inl ? 0u : (uint32_t) a;
+							gb->ni = (uint32_t) b;
+							S.eventCount[ring] = 0;
+						}
 						op = 1;
 						break;
 					}
-					if((uint32_t) (a >> 32) == (want | SERVE_STOP) || global_ns() - t0 > idleNs) break;
-					if((polls & 1023u) == 1023u && ld_acquire(&gb->error)) break;
+					uint32_t stop = 0;
+					if(lane == 0) {
+						stop = (uint32_t) (a >> 32) == (want | SERVE_STOP) || global_ns() - t0 > idleNs
+								|| ((polls & 1023u) == 1023u && ld_acquire(&gb->error));
+					}
+					if(__shfl_sync(FULL, stop, 0)) break;
 					__nanosleep(32);
 				}
-				st_release(&gb->cmd, op ? want : want | SERVE_STOP);
-				sOp = op;
+				__syncwarp();
+				if(lane == 0) {
+					st_release(&gb->cmd, op ? want : want | SERVE_STOP);
+					sOp = op;
+				}
 			}
 			__syncthreads();
 			op = sOp;
@@ -2260,10 +2284,15 @@ void Simulation::stepResident(uint32_t nf, uint32_t ni)
 {
 	volatile ServeCtl* c = reinterpret_cast<volatile ServeCtl*>(m_hServe);
 	const uint32_t want = m_serveSeq;
-	// the stimulus (m_hStim) is in place before the request
+	// a small firing stimulus goes in the request line itself
+	const bool inl = ni == 0 && nf <= SERVE_INLINE;
+	if(inl) {
+		for(uint32_t i = 0; i < nf; ++i) c->inl[i] = (unsigned long long) want << 32 | m_hStim[i];
+	}
+	// the stimulus (m_hStim or inline) is in place before the request
 	std::atomic_thread_fence(std::memory_order_seq_cst);
 	c->req[1] = (unsigned long long) want << 32 | ni;
-	c->req[0] = (unsigned long long) want << 32 | nf;
+	c->req[0] = (unsigned long long) want << 32 | (inl ? SERVE_INLINE_FLAG | nf : nf);
 	std::atomic_thread_fence(std::memory_order_seq_cst);
 	if(!m_serving) launchServe();
 	const auto t0 = std::chrono::steady_clock::now();

@@ -47,15 +47,24 @@ constexpr unsigned RESIDENT_REPLY_LIMIT_S = 20;
 // sequence number in the high half of both, the stimulus sizes (nf firing
 // indices, ni (index, current) pairs) in the low halves; it is complete
 // when both carry the same sequence number.  req[0] = (seq | stop flag)
-// << 32 ends the loop.
+// << 32 ends the loop.  A firing stimulus of at most SERVE_INLINE neurons
+// without currents travels in the request's own 64-byte line, so that the
+// poll that finds the request also reads it: inl[i] = seq << 32 | local
+// index, each word checked by its sequence number as the request words
+// are, and req[0]'s low half is then SERVE_INLINE_FLAG | count.
+constexpr uint32_t SERVE_INLINE = 6;
+constexpr uint32_t SERVE_INLINE_FLAG = 0x80000000u;
 struct ServeCtl {
 	unsigned long long req[2];
-	uint32_t pad0[28];
+	unsigned long long inl[SERVE_INLINE];
+	uint32_t pad0[16];
 	uint32_t done;     // sequence number of the last completed step
 	uint32_t fired;    // its fired neurons (global ids in the fired-id buffer)
 	unsigned long long events;  // its synaptic events
 	uint32_t pad1[28];
 };
+static_assert(offsetof(ServeCtl, inl) + 8 * SERVE_INLINE <= 64, "the request and its inline stimulus share one 64-byte line");
+static_assert(offsetof(ServeCtl, done) == 128, "the reply starts a line of its own");
 
 // STDP accumulation first tests a source against a shared-memory copy of the
 // "fired in the last 64 steps" bit-vector (W words), when it fits in this
