@@ -31,12 +31,16 @@ def same_state(a, b, n):
 
 def script(n, steps, seed):
     """Per step: a firing stimulus and a current stimulus (or None), with
-    some large ones that outgrow the staging buffer."""
+    some large ones that outgrow the staging buffer.  Firing stimuli of 1-8
+    neurons cover both sides of the six that travel inside the resident
+    loop's request line, and one repeats a neuron."""
     rng = np.random.default_rng(seed)
     out = []
     for t in range(steps):
-        f = rng.choice(n, int(rng.integers(1, 6)), replace=False).tolist() if t % 3 == 0 else None
+        f = rng.choice(n, int(rng.integers(1, 9)), replace=False).tolist() if t % 3 == 0 else None
         i = [(int(a), float(v)) for a, v in zip(rng.choice(n, 4), rng.normal(0, 15, 4))] if t % 7 == 0 else None
+        if t == 60:
+            f = [5, 17, 5]
         if t in (40, 41):
             f = rng.choice(n, n // 2, replace=False).tolist()       # beyond the initial buffer
             i = [(int(a), 3.0) for a in rng.choice(n, 700)]
